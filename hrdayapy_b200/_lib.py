@@ -1,0 +1,116 @@
+"""ctypes binding of libhrdaya_b200.so (declarations: include/hrdaya_b200.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+present, every entry point raises instead of falling back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libhrdaya_b200.so"
+
+HP_OK = 0
+_STATUS = {1: "HP_ERR_INVALID", 2: "HP_ERR_OOM", 3: "HP_ERR_CUDA", 4: "HP_ERR_NOT_CONVERGED",
+           5: "HP_ERR_STAGNATED", 6: "HP_ERR_NONFINITE", 7: "HP_ERR_TIMEOUT",
+           8: "HP_ERR_UNSUPPORTED"}
+
+HP_MAX_SITES = 8
+HP_MAX_VARIANTS = 64
+
+P = C.c_void_p
+
+
+class HpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class HpMonoDesc(C.Structure):
+    _fields_ = [
+        ("n_bricks", C.c_int32), ("bi", C.c_int32), ("bj", C.c_int32), ("bk", C.c_int32),
+        ("anisotropic", C.c_int32),
+        ("brick_nbr", P), ("tag", P), ("wface", P), ("doff", P), ("iso_coef", C.c_float),
+        ("brick_variant", P), ("n_variants", C.c_int32), ("variant_gks", P), ("variant_gkr", P),
+        ("n_pk", C.c_int32), ("pk_ptr", P), ("pk_idx", P), ("pk_coef", P), ("pk_stim", P),
+        ("pk_variant", P),
+        ("n_pmj_rows", C.c_int32), ("pmj_row", P), ("pmj_ptr", P), ("pmj_pk", P), ("pmj_coef", P),
+        ("dt", C.c_double), ("Cm", C.c_double), ("v0", C.c_float), ("n_steps", C.c_int64),
+        ("n_sites", C.c_int32), ("site_amp", P), ("site_on", P),
+        ("n_myo", C.c_int32), ("slot_of_node", P), ("vm_every", C.c_int64),
+        ("n_surf", C.c_int32), ("surf_of_slot", P), ("frame_every", C.c_int64),
+        ("act_threshold", C.c_float), ("deact_threshold", C.c_float), ("max_events", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m hrdayapy_b200.build "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(str(LIB_PATH))
+    L.hp_last_error.restype = C.c_char_p
+    L.hp_version.restype = C.c_char_p
+    L.hp_mono_create.argtypes = [C.POINTER(HpMonoDesc), C.POINTER(P), P]
+    L.hp_mono_run.argtypes = [P, C.c_int64, C.c_int32, P]
+    L.hp_mono_steps_done.argtypes = [P]
+    L.hp_mono_steps_done.restype = C.c_int64
+    L.hp_mono_copy_vm.argtypes = [P, C.c_int64, C.c_int64, P, C.c_int32, P]
+    L.hp_mono_copy_frames.argtypes = [P, C.c_int64, C.c_int64, P, P, C.c_int32, P]
+    L.hp_mono_copy_events.argtypes = [P, P, P, P, P, P]
+    L.hp_mono_copy_v.argtypes = [P, P, P, P]
+    L.hp_mono_copy_state.argtypes = [P, P, P, P]
+    L.hp_mono_destroy.argtypes = [P]
+    _lib = L
+    _declare_optional(L)
+    return L
+
+
+def _declare_optional(L):
+    """Signatures of the torso / preconditioner entry points (declared in
+    include/hrdaya_b200.h); set up lazily so older builds still load."""
+    try:
+        from . import _lib_torso
+        _lib_torso.declare(L)
+    except ImportError:
+        pass
+
+
+def check(status: int, what: str = ""):
+    if status != HP_OK:
+        msg = lib().hp_last_error().decode(errors="replace")
+        if status == 1:
+            raise ValueError(f"{what}: {msg}")
+        raise HpError(status, f"{what}: {msg}")
+
+
+def ptr(a) -> P | None:
+    """Host pointer of a C-contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    if not a.flags.c_contiguous:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(P)
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("hrdayapy_b200 needs a CUDA device (B200, sm_100a); "
+                           "there is no CPU fallback")
+    return torch
+
+
+def current_stream():
+    torch = require_cuda()
+    return P(torch.cuda.current_stream().cuda_stream)

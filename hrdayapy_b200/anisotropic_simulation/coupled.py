@@ -1,0 +1,76 @@
+"""compute_anisotropic_coupled / purkinje_myocardium_anisotropic_solver with
+the signatures of the reference's hrdayapy/anisotropic_simulation/coupled.py
+:35-154 and anisotropic_simulation/functions/
+purkinje_myocardium_anisotropic_solver.py:1308-1360.
+
+A_P is derived as 2 / R_P and passing it raises TypeError, as in the
+reference (:1519-1526).  Only theta = 0 is accepted (fused explicit step).
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+from .. import monodomain
+from .._spacing import resolve_voxel_size
+
+
+def purkinje_myocardium_anisotropic_solver(
+        nodes, elements, activation_times, S, Z, phi, fibre_dir, *, voxel_size=0.4, dx_p=0.2,
+        sigma_P=0.225, sigma_l=3.0 * 6.5625e-5, sigma_t=6.5625e-5, Cm=0.01, A_P=None,
+        A_M=140.0, R_P=0.015, dt=0.1, T=400.0, theta=0.5, stim_protocol=None,
+        ectopic_region=None, stim_regions=None, stim_len_mm=2.0, c_pmj=0.05, n_pmj=1,
+        cg_tol=1e-5, cg_max_iter=100, n_frames=100, frame_save_dt=None, anim_tmp_dir=None,
+        device=None, dtype=None, out_npz=None, phi_endo_max=0.35, phi_epi_min=0.65,
+        vm_save_dt=None, out_vm_npz=None, vm_tmp_dir=None, act_threshold=-40.0,
+        deact_threshold=-40.0, max_events=4, brick=None):
+    if A_P is not None:
+        raise TypeError("A_P is no longer a settable parameter -- it's mechanically determined "
+                        "by R_P (A_P = 2.0/R_P for a cylindrical fibre). Remove the A_P= "
+                        "argument; only set R_P.")
+    fibre_dir = np.asarray(fibre_dir)
+    if fibre_dir.shape != tuple(np.asarray(S).shape) + (3,):
+        raise ValueError(f"fibre_dir shape {fibre_dir.shape} must be S.shape + (3,)")
+    return monodomain.run(
+        nodes, elements, activation_times, S, Z, phi, fibre_dir=fibre_dir, anisotropic=True,
+        theta=theta, dtype=dtype, device=device, n_frames=n_frames,
+        frame_save_dt=frame_save_dt, out_npz=out_npz, out_vm_npz=out_vm_npz,
+        vm_save_dt=vm_save_dt, vm_tmp_dir=vm_tmp_dir, anim_tmp_dir=anim_tmp_dir, cg_tol=cg_tol,
+        cg_max_iter=cg_max_iter, voxel_size=voxel_size, dx_p=dx_p, sigma_P=sigma_P,
+        sigma_l=sigma_l, sigma_t=sigma_t, Cm=Cm, A_P=2.0 / R_P, A_M=A_M, R_P=R_P, dt=dt, T=T,
+        stim_protocol=stim_protocol, ectopic_region=ectopic_region, stim_regions=stim_regions,
+        stim_len_mm=stim_len_mm, c_pmj=c_pmj, n_pmj=n_pmj, phi_endo_max=phi_endo_max,
+        phi_epi_min=phi_epi_min, act_threshold=act_threshold, deact_threshold=deact_threshold,
+        max_events=max_events, brick=brick)
+
+
+def compute_anisotropic_coupled(
+        nodes, elements, act_times, S, Z, phi, fibre_dir, *, anatomy=None, stim_protocol=None,
+        ectopic_region=None, stim_regions=None, voxel_size=0.4, dx_p: float = 0.2,
+        sigma_P: float = 0.45, sigma_l: float = 3.0 * 1.31e-4, sigma_t: float = 1.31e-4,
+        Cm: float = 0.01, A_M: float = 140.0, R_P: float = 0.015, dt: float = 0.1,
+        T: float = 400.0, theta: float = 0.5, stim_len_mm: float = 2.0, c_pmj: float = 0.05,
+        n_pmj: int = 1, cg_tol: float = 1e-5, cg_max_iter: int = 500, n_frames: int = 100,
+        frame_save_dt=None, anim_tmp_dir=None, device=None, phi_endo_max: float = 0.35,
+        phi_epi_min: float = 0.65, save_path=None, vm_save_dt=None, vm_save_path=None,
+        vm_tmp_dir=None, **extra):
+    voxel_size = resolve_voxel_size(voxel_size, anatomy, param_name="voxel_size")
+    return purkinje_myocardium_anisotropic_solver(
+        nodes=nodes, elements=elements, activation_times=act_times, S=S, Z=Z, phi=phi,
+        fibre_dir=fibre_dir, voxel_size=voxel_size, dx_p=dx_p, sigma_P=sigma_P,
+        sigma_l=sigma_l, sigma_t=sigma_t, Cm=Cm, A_M=A_M, R_P=R_P, dt=dt, T=T, theta=theta,
+        stim_protocol=stim_protocol, ectopic_region=ectopic_region, stim_regions=stim_regions,
+        stim_len_mm=stim_len_mm, c_pmj=c_pmj, n_pmj=n_pmj, cg_tol=cg_tol,
+        cg_max_iter=cg_max_iter, n_frames=n_frames, frame_save_dt=frame_save_dt,
+        anim_tmp_dir=anim_tmp_dir, device=device, out_npz=save_path,
+        phi_endo_max=phi_endo_max, phi_epi_min=phi_epi_min, vm_save_dt=vm_save_dt,
+        out_vm_npz=vm_save_path, vm_tmp_dir=vm_tmp_dir, **extra)
+
+
+def load_anisotropic_coupled(path):
+    path = Path(path).with_suffix(".npz")
+    if not path.exists():
+        raise FileNotFoundError(f"No saved anisotropic coupled simulation at {path}")
+    z = np.load(path)
+    return {k: z[k] for k in z.files}

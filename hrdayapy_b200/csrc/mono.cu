@@ -1,0 +1,739 @@
+// Fused monodomain time step for sm_100a.
+//
+// One launch advances every myocardial voxel and every Purkinje node by one
+// step of the reference's Lie splitting at theta = 0
+// (simulation/functions/purkinje_myocardium_pipeline.py:1347-1420,
+//  anisotropic_simulation/functions/purkinje_myocardium_anisotropic_solver.py:1746-1820):
+//
+//   V*_i     = V_i + dt/Cm (-Iion(V_i) Cm + Istim_i)          (ionic half)
+//   V_{i+1}  = clamp(V*_i + dt/Cm * L V*_i, -150, 80)           (diffusion half)
+//
+// The kernel is skewed by half a step so that a single pass per voxel is
+// enough: launch i reads W_i = V*_i of the voxel and its 18 neighbours,
+// forms V_{i+1} (recording threshold crossings and snapshots on it), then
+// immediately runs the TTP06 update of step i+1 on V_{i+1} and stores
+// W_{i+1}.  A prologue launch (mode 1) produces W_0 from the resting state.
+// W is double-buffered (neighbours need the old value); V_{i+1} is kept in
+// Vpost for the crossing test of the next step and for snapshots.
+//
+// Data layout in HBM (see include/hrdaya_b200.h): voxels of the mask in
+// bricks of BI x BJ x BK with k fastest, only bricks that touch the mask are
+// stored; every per-voxel field is a separate SoA array over slots, so each
+// warp's loads and stores are contiguous 128-byte lines.  The stencil reads
+// W (and, for the 19-point operator, the face weights and off-diagonal
+// tensor components) of the brick plus a one-voxel halo into shared memory.
+#include "hp_common.cuh"
+#include "ttp06.cuh"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+
+#include <vector>
+
+namespace hp {
+
+struct MonoArgs {
+  int32_t n_bricks, n_pk;
+  int64_t n_slots;
+  const uint32_t* tag;
+  const float* wface;  // 3 x n_slots
+  const float* doff;   // 3 x n_slots
+  float iso_coef;
+  const int32_t* nbr;  // n_bricks x 27
+  const uint8_t* brick_variant;
+  float* state;        // 18 x n_slots
+  float* Vs0;                       // W double buffer (slots)
+  float* Vs1;
+  float* Vpost;
+  // Purkinje
+  const int32_t* pk_ptr;
+  const int32_t* pk_idx;
+  const float* pk_coef;
+  const uint8_t* pk_stim;
+  const uint8_t* pk_variant;
+  float* pk_state;     // 18 x n_pk
+  float* pk_Vs0;
+  float* pk_Vs1;
+  float* pk_Vpost;
+  // junctions, myocardial side
+  const int32_t* pmj_row;
+  const int32_t* pmj_ptr;
+  const int32_t* pmj_pk;
+  const float* pmj_coef;
+  // time stepping
+  double dt_d;
+  float dt, Cm, dt_over_Cm;
+  float site_amp[HP_MAX_SITES];
+  const uint8_t* site_on;
+  const float* var_gks;
+  const float* var_gkr;
+  // outputs
+  float* vm_snap;
+  const int32_t* node_of_slot;
+  int64_t vm_every, n_myo;
+  float* surf_frames;
+  const int32_t* surf_of_slot;
+  int64_t n_surf;
+  float* pk_frames;
+  int64_t frame_every;
+  float act_thr, deact_thr;
+  int32_t max_events;
+  float* act_t;
+  uint8_t* act_n;
+  float* deact_t;
+  uint8_t* deact_n;
+  const int64_t* d_step;
+};
+
+// TTP06 phenotype table (ttp06_phenotype_constants.py:54-61), index = pheno-1.
+__device__ __forceinline__ CellParams pheno_params(int ph, float gks_s, float gkr_s) {
+  CellParams p;
+  p.g_Kr = 0.153f * gkr_s;
+  if (ph == 1) {         // endo
+    p.g_Ks = 0.392f * gks_s; p.g_to = 0.073f; p.endo_s = 1;
+  } else if (ph == 2) {  // mid
+    p.g_Ks = 0.098f * gks_s; p.g_to = 0.294f; p.endo_s = 1;
+  } else {               // epi
+    p.g_Ks = 0.392f * gks_s; p.g_to = 0.294f; p.endo_s = 0;
+  }
+  return p;
+}
+
+__device__ __forceinline__ float stim_current(const MonoArgs& a, uint32_t bits, int64_t istep) {
+  uint32_t on = bits & (uint32_t)a.site_on[istep];
+  float I = 0.0f;
+  while (on) {
+    int s = __ffs(on) - 1;
+    I += a.site_amp[s];
+    on &= on - 1;
+  }
+  return I;
+}
+
+// One threshold crossing between snapshots (t0, v0) -> (t1, v1), linear
+// interpolation as activation_maps.py:63-89 (float32, frac clipped to [0,1]).
+__device__ __forceinline__ void record_event(float* tbl, uint8_t* cnt, int64_t slot,
+                                             int64_t n_slots, int max_events, float thr,
+                                             float v0, float v1, float t0, float t1) {
+  float den = v1 - v0;
+  if (den == 0.0f) den = 1e-9f;
+  float frac = __fdiv_rn(thr - v0, den);
+  frac = fminf(fmaxf(frac, 0.0f), 1.0f);
+  const float tc = __fadd_rn(t0, __fmul_rn(frac, __fsub_rn(t1, t0)));
+  const int n = cnt[slot];
+  if (n < max_events) tbl[(int64_t)n * n_slots + slot] = tc;
+  if (n < 255) cnt[slot] = (uint8_t)(n + 1);
+}
+
+template <int BI, int BJ, int BK>
+struct TileGeom {
+  static constexpr int TI = BI + 2, TJ = BJ + 2, TK = BK + 2;
+  static constexpr int N = TI * TJ * TK;
+  static constexpr int SI = TJ * TK, SJ = TK;
+  static constexpr int BV = BI * BJ * BK;
+};
+
+// Loads local region [I0,I1) x [J0,J1) x [K0,K1) (coordinates relative to the
+// brick, -1 and B* address the halo) of a slot array into a shared tile.
+template <int BI, int BJ, int BK, int I0, int I1, int J0, int J1, int K0, int K1>
+__device__ __forceinline__ void load_region(float* __restrict__ tile,
+                                            const float* __restrict__ src,
+                                            const int* nb27, int tid) {
+  using G = TileGeom<BI, BJ, BK>;
+  constexpr int NI = I1 - I0, NJ = J1 - J0, NK = K1 - K0, NT = NI * NJ * NK;
+#pragma unroll 4
+  for (int e = tid; e < NT; e += G::BV) {
+    const int ek = e % NK;
+    const int t = e / NK;
+    const int ej = t % NJ;
+    const int ei = t / NJ;
+    const int li = ei + I0, lj = ej + J0, lk = ek + K0;
+    const int di = li < 0 ? -1 : (li >= BI ? 1 : 0);
+    const int dj = lj < 0 ? -1 : (lj >= BJ ? 1 : 0);
+    const int dk = lk < 0 ? -1 : (lk >= BK ? 1 : 0);
+    const int nb = nb27[(di + 1) * 9 + (dj + 1) * 3 + (dk + 1)];
+    float v = 0.0f;
+    if (nb >= 0) {
+      const int gi = li - di * BI, gj = lj - dj * BJ, gk = lk - dk * BK;
+      v = __ldg(src + (int64_t)nb * G::BV + (gi * BJ + gj) * BK + gk);
+    }
+    tile[(li + 1) * G::SI + (lj + 1) * G::SJ + (lk + 1)] = v;
+  }
+}
+
+// Purkinje nodes: thread per node over the CSR adjacency (cable edges and
+// junction edges to myocardial slots), same skewed step as the voxels.
+__device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t step, int mode) {
+  const bool odd = step & 1;
+  const float* __restrict__ Win = odd ? a.pk_Vs1 : a.pk_Vs0;
+  float* __restrict__ Wout = odd ? a.pk_Vs0 : a.pk_Vs1;
+  const float* __restrict__ Wmyo = odd ? a.Vs1 : a.Vs0;
+  float Vn;
+  int64_t istep;
+  if (mode == 0) {
+    const float Vc = Win[p];
+    float acc = 0.0f;
+    for (int q = a.pk_ptr[p]; q < a.pk_ptr[p + 1]; ++q) {
+      const int j = a.pk_idx[q];
+      const float Vj = j >= 0 ? Win[j] : Wmyo[-(int64_t)j - 1];
+      acc += a.pk_coef[q] * (Vj - Vc);
+    }
+    Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
+    a.pk_Vpost[p] = Vn;
+    if (a.frame_every > 0 && step % a.frame_every == 0)
+      a.pk_frames[(step / a.frame_every) * (int64_t)a.n_pk + p] = Vn;
+    istep = step + 1;
+  } else {
+    Vn = a.pk_Vpost[p];
+    istep = 0;
+    Wout = a.pk_Vs0;
+  }
+  const int var = a.pk_variant ? a.pk_variant[p] : 0;
+  const CellParams cp = pheno_params(1, a.var_gks[var], a.var_gkr[var]);  // Purkinje -> endo
+  CellState c;
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) c.v[v] = a.pk_state[(int64_t)v * a.n_pk + p];
+  const float Iion = ttp06_step(Vn, c, a.dt, cp);
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p] = c.v[v];
+  const float Is = stim_current(a, a.pk_stim[p], istep);
+  Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
+template <int BI, int BJ, int BK, bool ANISO>
+__global__ void __launch_bounds__(BI * BJ * BK)
+mono_step_kernel(MonoArgs a, int step_off, int mode) {
+  using G = TileGeom<BI, BJ, BK>;
+  constexpr int BV = G::BV, SI = G::SI, SJ = G::SJ;
+  const int64_t step = *a.d_step + step_off;
+  const int tid = threadIdx.x;
+  if ((int)blockIdx.x >= a.n_bricks) {
+    const int p = ((int)blockIdx.x - a.n_bricks) * BV + tid;
+    if (p < a.n_pk) purkinje_part(a, p, step, mode);
+    return;
+  }
+  const int b = blockIdx.x;
+  const bool odd = step & 1;
+  const float* __restrict__ Win = odd ? a.Vs1 : a.Vs0;
+  float* __restrict__ Wout = odd ? a.Vs0 : a.Vs1;
+
+  __shared__ int nb27[27];
+  __shared__ float tV[G::N];
+  __shared__ float tW[ANISO ? 3 * G::N : 1];
+  __shared__ float tD[ANISO ? 3 * G::N : 1];
+  if (tid < 27) nb27[tid] = a.nbr[(int64_t)b * 27 + tid];
+  __syncthreads();
+  if (mode == 0) {
+    load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, -1, BK + 1>(tV, Win, nb27, tid);
+    if constexpr (ANISO) {
+      const int64_t ns = a.n_slots;
+      load_region<BI, BJ, BK, -1, BI, 0, BJ, 0, BK>(tW, a.wface, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, -1, BJ, 0, BK>(tW + G::N, a.wface + ns, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, 0, BJ, -1, BK>(tW + 2 * G::N, a.wface + 2 * ns, nb27, tid);
+      load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, 0, BK>(tD, a.doff, nb27, tid);
+      load_region<BI, BJ, BK, -1, BI + 1, 0, BJ, -1, BK + 1>(tD + G::N, a.doff + ns, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, -1, BJ + 1, -1, BK + 1>(tD + 2 * G::N, a.doff + 2 * ns, nb27, tid);
+    }
+  }
+  __syncthreads();
+
+  const int64_t slot = (int64_t)b * BV + tid;
+  const uint32_t tag = a.tag[slot];
+  const int ph = tag & HP_TAG_PHENO_MASK;
+  if (ph == 0) return;
+
+  float Vn;
+  int64_t istep;
+  if (mode == 0) {
+    const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
+    const int c = (li + 1) * SI + (lj + 1) * SJ + (lk + 1);
+    const float Vc = tV[c];
+    float acc = 0.0f;
+    const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
+    if constexpr (!ANISO) {
+      float s = 0.0f;
+      if (fb & 1u) s += tV[c + SI] - Vc;
+      if (fb & 2u) s += tV[c - SI] - Vc;
+      if (fb & 4u) s += tV[c + SJ] - Vc;
+      if (fb & 8u) s += tV[c - SJ] - Vc;
+      if (fb & 16u) s += tV[c + 1] - Vc;
+      if (fb & 32u) s += tV[c - 1] - Vc;
+      acc = a.iso_coef * s;
+    } else {
+      const float* tWx = tW;
+      const float* tWy = tW + G::N;
+      const float* tWz = tW + 2 * G::N;
+      if (fb & 1u) acc += tWx[c] * (tV[c + SI] - Vc);
+      if (fb & 2u) acc += tWx[c - SI] * (tV[c - SI] - Vc);
+      if (fb & 4u) acc += tWy[c] * (tV[c + SJ] - Vc);
+      if (fb & 8u) acc += tWy[c - SJ] * (tV[c - SJ] - Vc);
+      if (fb & 16u) acc += tWz[c] * (tV[c + 1] - Vc);
+      if (fb & 32u) acc += tWz[c - 1] * (tV[c - 1] - Vc);
+      const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
+      const float* t01 = tD;
+      const float* t02 = tD + G::N;
+      const float* t12 = tD + 2 * G::N;
+      // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
+#define HP_DIAG(bit, T, OFF, SGN)                                            \
+  if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
+                                 (tV[c + (OFF)] - Vc);
+      HP_DIAG(0, t01, SI + SJ, 1.0f)
+      HP_DIAG(1, t01, -SI - SJ, 1.0f)
+      HP_DIAG(2, t01, SI - SJ, -1.0f)
+      HP_DIAG(3, t01, -SI + SJ, -1.0f)
+      HP_DIAG(4, t02, SI + 1, 1.0f)
+      HP_DIAG(5, t02, -SI - 1, 1.0f)
+      HP_DIAG(6, t02, SI - 1, -1.0f)
+      HP_DIAG(7, t02, -SI + 1, -1.0f)
+      HP_DIAG(8, t12, SJ + 1, 1.0f)
+      HP_DIAG(9, t12, -SJ - 1, 1.0f)
+      HP_DIAG(10, t12, SJ - 1, -1.0f)
+      HP_DIAG(11, t12, -SJ + 1, -1.0f)
+#undef HP_DIAG
+    }
+    if (tag & HP_TAG_PMJ) {
+      const float* __restrict__ Wpk = odd ? a.pk_Vs1 : a.pk_Vs0;
+      const int r = a.pmj_row[slot];
+      for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
+        acc += a.pmj_coef[q] * (Wpk[a.pmj_pk[q]] - Vc);
+    }
+    Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
+
+    // threshold crossings between the snapshots labelled t_{i-1} and t_i
+    if (step >= 1) {
+      const float Vp = a.Vpost[slot];
+      const bool was_act = Vp >= a.act_thr, is_act = Vn >= a.act_thr;
+      const bool was_dea = Vp >= a.deact_thr, is_dea = Vn >= a.deact_thr;
+      if ((!was_act && is_act) || (was_dea && !is_dea)) {
+        const float t0 = (float)((double)(step - 1) * a.dt_d);
+        const float t1 = (float)((double)step * a.dt_d);
+        if (!was_act && is_act)
+          record_event(a.act_t, a.act_n, slot, a.n_slots, a.max_events, a.act_thr, Vp, Vn, t0, t1);
+        if (was_dea && !is_dea)
+          record_event(a.deact_t, a.deact_n, slot, a.n_slots, a.max_events, a.deact_thr, Vp, Vn,
+                       t0, t1);
+      }
+    }
+    a.Vpost[slot] = Vn;
+    if (a.vm_every > 0 && step % a.vm_every == 0)
+      a.vm_snap[(step / a.vm_every) * a.n_myo + a.node_of_slot[slot]] = Vn;
+    if ((tag & HP_TAG_SURF) && a.frame_every > 0 && step % a.frame_every == 0)
+      a.surf_frames[(step / a.frame_every) * a.n_surf + a.surf_of_slot[slot]] = Vn;
+    istep = step + 1;
+  } else {
+    Vn = a.Vpost[slot];
+    istep = 0;
+    Wout = a.Vs0;
+  }
+
+  // ionic half of step istep on V = Vn
+  const int var = a.brick_variant ? a.brick_variant[b] : 0;
+  const CellParams cp = pheno_params(ph, a.var_gks[var], a.var_gkr[var]);
+  CellState cs;
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * a.n_slots + slot];
+  const float Iion = ttp06_step(Vn, cs, a.dt, cp);
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
+  const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep);
+  Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
+__global__ void init_cells_kernel(float* state, float* Vpost, int64_t n, float v0) {
+  // resting state, gpu_ttp06.py:150-169
+  const float init[N_STATE] = {138.4f, 10.355f, 0.00013f, 0.00448f, 0.476f, 0.0087f,
+                               0.00155f, 0.7573f, 0.7225f, 3.164e-5f, 0.8009f, 0.9778f,
+                               0.9953f, 0.3212f, 2.235e-8f, 3.715f, 0.9068f, 0.00036f};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) state[v * n + i] = init[v];
+    Vpost[i] = v0;
+  }
+}
+
+__global__ void fill_kernel(float* p, int64_t n, float v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
+
+typedef void (*StepFn)(MonoArgs, int, int);
+
+struct ShapeEntry {
+  int bi, bj, bk;
+  StepFn iso, aniso;
+};
+
+static const ShapeEntry kShapes[] = {
+    {4, 4, 8, mono_step_kernel<4, 4, 8, false>, mono_step_kernel<4, 4, 8, true>},
+    {4, 8, 8, mono_step_kernel<4, 8, 8, false>, mono_step_kernel<4, 8, 8, true>},
+    {2, 4, 16, mono_step_kernel<2, 4, 16, false>, mono_step_kernel<2, 4, 16, true>},
+    {8, 8, 8, mono_step_kernel<8, 8, 8, false>, mono_step_kernel<8, 8, 8, true>},
+};
+
+}  // namespace hp
+
+using namespace hp;
+
+struct HpMono {
+  MonoArgs a;
+  StepFn fn;
+  int bv;
+  int64_t n_steps, steps_done;
+  int64_t n_vm_frames, n_anim_frames;
+  int anisotropic;
+  std::vector<int32_t> slot_of_node;
+  std::vector<void*> allocs;
+  cudaGraphExec_t graph;
+  int32_t graph_chunk;
+  cudaStream_t graph_stream;
+  int device;
+};
+
+template <typename T>
+static hp_status up(HpMono* h, T** dst, const T* src, size_t n, cudaStream_t s) {
+  hp_status st = dev_upload(dst, src, n, s);
+  if (st == HP_OK && *dst) h->allocs.push_back((void*)*dst);
+  return st;
+}
+template <typename T>
+static hp_status al(HpMono* h, T** dst, size_t n) {
+  hp_status st = dev_alloc(dst, n);
+  if (st == HP_OK && *dst) h->allocs.push_back((void*)*dst);
+  return st;
+}
+
+#define HP_TRY(x)                      \
+  do {                                 \
+    hp_status _s = (x);                \
+    if (_s != HP_OK) {                 \
+      hp_mono_destroy(h);              \
+      return _s;                       \
+    }                                  \
+  } while (0)
+
+static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) {
+  const int grid = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  if (grid == 0) return HP_OK;
+  h->fn<<<grid, h->bv, 0, s>>>(h->a, step_off, mode);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* stream) {
+  HP_REQUIRE(d && out, "hp_mono_create: null argument");
+  *out = nullptr;
+  const ShapeEntry* se = nullptr;
+  for (const auto& e : kShapes)
+    if (e.bi == d->bi && e.bj == d->bj && e.bk == d->bk) se = &e;
+  if (!se) {
+    hp::set_error("hp_mono_create: brick shape %dx%dx%d is not compiled", d->bi, d->bj, d->bk);
+    return HP_ERR_UNSUPPORTED;
+  }
+  HP_REQUIRE(d->n_bricks >= 0 && d->n_pk >= 0, "hp_mono_create: negative sizes");
+  HP_REQUIRE(d->n_sites >= 0 && d->n_sites <= HP_MAX_SITES, "hp_mono_create: n_sites must be 0..%d",
+             HP_MAX_SITES);
+  HP_REQUIRE(d->n_variants >= 1 && d->n_variants <= HP_MAX_VARIANTS,
+             "hp_mono_create: n_variants must be 1..%d", HP_MAX_VARIANTS);
+  HP_REQUIRE(d->max_events >= 1 && d->max_events <= 16, "hp_mono_create: max_events must be 1..16");
+  HP_REQUIRE(d->dt > 0.0 && d->Cm > 0.0, "hp_mono_create: dt and Cm must be positive");
+  HP_REQUIRE(d->n_steps >= 0, "hp_mono_create: n_steps must be >= 0");
+  HP_REQUIRE(d->n_bricks == 0 || (d->brick_nbr && d->tag), "hp_mono_create: missing brick arrays");
+  HP_REQUIRE(!d->anisotropic || d->n_bricks == 0 || (d->wface && d->doff),
+             "hp_mono_create: anisotropic needs wface and doff");
+  HP_REQUIRE(d->n_pk == 0 || (d->pk_ptr && d->pk_stim), "hp_mono_create: missing Purkinje arrays");
+  HP_REQUIRE(d->site_on, "hp_mono_create: missing site_on");
+  HP_REQUIRE(d->n_myo >= 0 && (d->n_myo == 0 || d->slot_of_node), "hp_mono_create: missing slot_of_node");
+
+  HpMono* h = new HpMono();
+  h->graph = nullptr;
+  h->graph_chunk = 0;
+  h->graph_stream = nullptr;
+  cudaGetDevice(&h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  MonoArgs& a = h->a;
+  memset(&a, 0, sizeof(a));
+  h->bv = d->bi * d->bj * d->bk;
+  h->fn = d->anisotropic ? se->aniso : se->iso;
+  h->anisotropic = d->anisotropic;
+  h->n_steps = d->n_steps;
+  h->steps_done = 0;
+  a.n_bricks = d->n_bricks;
+  a.n_pk = d->n_pk;
+  const int64_t ns = (int64_t)d->n_bricks * h->bv;
+  a.n_slots = ns;
+  HP_TRY(up(h, (uint32_t**)&a.tag, d->tag, ns, s));
+  if (d->anisotropic) {
+    HP_TRY(up(h, (float**)&a.wface, d->wface, 3 * ns, s));
+    HP_TRY(up(h, (float**)&a.doff, d->doff, 3 * ns, s));
+  }
+  a.iso_coef = d->iso_coef;
+  HP_TRY(up(h, (int32_t**)&a.nbr, d->brick_nbr, (size_t)27 * d->n_bricks, s));
+  if (d->brick_variant) HP_TRY(up(h, (uint8_t**)&a.brick_variant, d->brick_variant, d->n_bricks, s));
+  HP_TRY(al(h, &a.state, (size_t)N_STATE * ns));
+  HP_TRY(al(h, &a.Vs0, ns));
+  HP_TRY(al(h, &a.Vs1, ns));
+  HP_TRY(al(h, &a.Vpost, ns));
+  // Purkinje
+  if (d->n_pk > 0) {
+    HP_TRY(up(h, (int32_t**)&a.pk_ptr, d->pk_ptr, d->n_pk + 1, s));
+    const int32_t nnz = d->pk_ptr[d->n_pk];
+    HP_REQUIRE(nnz >= 0, "hp_mono_create: bad pk_ptr");
+    if (nnz > 0) {
+      HP_REQUIRE(d->pk_idx && d->pk_coef, "hp_mono_create: missing pk_idx/pk_coef");
+      for (int32_t q = 0; q < nnz; ++q) {
+        const int32_t j = d->pk_idx[q];
+        if (j >= d->n_pk || (j < 0 && -(int64_t)j - 1 >= ns)) {
+          hp::set_error("hp_mono_create: pk_idx[%d]=%d out of range", q, j);
+          hp_mono_destroy(h);
+          return HP_ERR_INVALID;
+        }
+      }
+      HP_TRY(up(h, (int32_t**)&a.pk_idx, d->pk_idx, nnz, s));
+      HP_TRY(up(h, (float**)&a.pk_coef, d->pk_coef, nnz, s));
+    }
+    HP_TRY(up(h, (uint8_t**)&a.pk_stim, d->pk_stim, d->n_pk, s));
+    if (d->pk_variant) HP_TRY(up(h, (uint8_t**)&a.pk_variant, d->pk_variant, d->n_pk, s));
+    HP_TRY(al(h, &a.pk_state, (size_t)N_STATE * d->n_pk));
+    HP_TRY(al(h, &a.pk_Vs0, d->n_pk));
+    HP_TRY(al(h, &a.pk_Vs1, d->n_pk));
+    HP_TRY(al(h, &a.pk_Vpost, d->n_pk));
+  }
+  if (d->n_pmj_rows > 0) {
+    HP_REQUIRE(d->pmj_row && d->pmj_ptr, "hp_mono_create: missing junction arrays");
+    const int32_t nnz = d->pmj_ptr[d->n_pmj_rows];
+    for (int32_t q = 0; q < nnz; ++q)
+      if (d->pmj_pk[q] < 0 || d->pmj_pk[q] >= d->n_pk) {
+        hp::set_error("hp_mono_create: pmj_pk[%d] out of range", q);
+        hp_mono_destroy(h);
+        return HP_ERR_INVALID;
+      }
+    HP_TRY(up(h, (int32_t**)&a.pmj_row, d->pmj_row, ns, s));
+    HP_TRY(up(h, (int32_t**)&a.pmj_ptr, d->pmj_ptr, d->n_pmj_rows + 1, s));
+    HP_TRY(up(h, (int32_t**)&a.pmj_pk, d->pmj_pk, nnz, s));
+    HP_TRY(up(h, (float**)&a.pmj_coef, d->pmj_coef, nnz, s));
+  }
+  // time stepping
+  a.dt_d = d->dt;
+  a.dt = (float)d->dt;
+  a.Cm = (float)d->Cm;
+  a.dt_over_Cm = (float)(d->dt / d->Cm);
+  for (int i = 0; i < d->n_sites; ++i) a.site_amp[i] = d->site_amp[i];
+  HP_TRY(up(h, (uint8_t**)&a.site_on, d->site_on, d->n_steps + 1, s));
+  HP_TRY(up(h, (float**)&a.var_gks, d->variant_gks, d->n_variants, s));
+  HP_TRY(up(h, (float**)&a.var_gkr, d->variant_gkr, d->n_variants, s));
+  // outputs
+  a.n_myo = d->n_myo;
+  h->slot_of_node.assign(d->slot_of_node, d->slot_of_node + d->n_myo);
+  {
+    std::vector<int32_t> node_of_slot(ns, -1);
+    for (int32_t i = 0; i < d->n_myo; ++i) {
+      const int32_t sl = d->slot_of_node[i];
+      if (sl < 0 || sl >= ns) {
+        hp::set_error("hp_mono_create: slot_of_node[%d]=%d out of range", i, sl);
+        hp_mono_destroy(h);
+        return HP_ERR_INVALID;
+      }
+      node_of_slot[sl] = i;
+    }
+    // every tissue slot must map to a node (snapshots scatter through it)
+    for (int64_t sl = 0; sl < ns; ++sl)
+      if ((d->tag[sl] & HP_TAG_PHENO_MASK) && node_of_slot[sl] < 0) {
+        hp::set_error("hp_mono_create: tissue slot %lld has no node", (long long)sl);
+        hp_mono_destroy(h);
+        return HP_ERR_INVALID;
+      }
+    HP_TRY(up(h, (int32_t**)&a.node_of_slot, node_of_slot.data(), ns, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));  // node_of_slot is a stack temporary
+  }
+  a.vm_every = d->vm_every;
+  h->n_vm_frames = d->vm_every > 0 ? (d->n_steps + d->vm_every - 1) / d->vm_every : 0;
+  HP_TRY(al(h, &a.vm_snap, (size_t)h->n_vm_frames * d->n_myo));
+  a.frame_every = d->frame_every;
+  h->n_anim_frames = d->frame_every > 0 ? (d->n_steps + d->frame_every - 1) / d->frame_every : 0;
+  a.n_surf = d->n_surf;
+  if (d->n_surf > 0) {
+    HP_REQUIRE(d->surf_of_slot, "hp_mono_create: missing surf_of_slot");
+    HP_TRY(up(h, (int32_t**)&a.surf_of_slot, d->surf_of_slot, ns, s));
+  }
+  HP_TRY(al(h, &a.surf_frames, (size_t)h->n_anim_frames * d->n_surf));
+  HP_TRY(al(h, &a.pk_frames, (size_t)h->n_anim_frames * d->n_pk));
+  a.act_thr = d->act_threshold;
+  a.deact_thr = d->deact_threshold;
+  a.max_events = d->max_events;
+  HP_TRY(al(h, &a.act_t, (size_t)d->max_events * ns));
+  HP_TRY(al(h, &a.deact_t, (size_t)d->max_events * ns));
+  HP_TRY(al(h, &a.act_n, ns));
+  HP_TRY(al(h, &a.deact_n, ns));
+  if (ns) {
+    HP_CUDA_TRY(cudaMemsetAsync(a.act_n, 0, ns, s));
+    HP_CUDA_TRY(cudaMemsetAsync(a.deact_n, 0, ns, s));
+    HP_CUDA_TRY(cudaMemsetAsync(a.Vs1, 0, ns * sizeof(float), s));
+  }
+  int64_t* dstep = nullptr;
+  HP_TRY(al(h, &dstep, 1));
+  HP_CUDA_TRY(cudaMemsetAsync(dstep, 0, sizeof(int64_t), s));
+  a.d_step = dstep;
+  const float nanv = nanf("");
+  if (ns) {
+    fill_kernel<<<1024, 256, 0, s>>>(a.act_t, (int64_t)d->max_events * ns, nanv);
+    fill_kernel<<<1024, 256, 0, s>>>(a.deact_t, (int64_t)d->max_events * ns, nanv);
+    init_cells_kernel<<<1024, 256, 0, s>>>(a.state, a.Vpost, ns, d->v0);
+  }
+  if (d->n_pk) {
+    init_cells_kernel<<<256, 256, 0, s>>>(a.pk_state, a.pk_Vpost, d->n_pk, d->v0);
+    HP_CUDA_TRY(cudaMemsetAsync(a.pk_Vs1, 0, d->n_pk * sizeof(float), s));
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  HP_TRY(launch_step(h, 0, 1, s));  // W_0 = ionic(V_0)
+  // the caller's host arrays may be released once this returns
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  *out = h;
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_run(HpMono* h, int64_t n, int32_t graph_chunk, void* stream) {
+  HP_REQUIRE(h, "hp_mono_run: null handle");
+  HP_REQUIRE(n >= 0 && h->steps_done + n <= h->n_steps,
+             "hp_mono_run: %lld steps requested, %lld remain", (long long)n,
+             (long long)(h->n_steps - h->steps_done));
+  cudaStream_t s = (cudaStream_t)stream;
+  int64_t left = n;
+  if (graph_chunk > 0 && left >= graph_chunk) {
+    if (!h->graph || h->graph_chunk != graph_chunk || h->graph_stream != s) {
+      if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+      }
+      cudaGraph_t g;
+      HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      hp_status st = HP_OK;
+      for (int o = 0; o < graph_chunk && st == HP_OK; ++o) st = launch_step(h, o, 0, s);
+      if (st == HP_OK) advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, graph_chunk);
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (st != HP_OK) return st;
+      HP_CUDA_TRY(ce);
+      HP_CUDA_TRY(cudaGraphInstantiate(&h->graph, g, 0));
+      cudaGraphDestroy(g);
+      h->graph_chunk = graph_chunk;
+      h->graph_stream = s;
+    }
+    while (left >= graph_chunk) {
+      HP_CUDA_TRY(cudaGraphLaunch(h->graph, s));
+      left -= graph_chunk;
+    }
+  }
+  if (left > 0) {
+    for (int64_t o = 0; o < left; ++o) {
+      hp_status st = launch_step(h, (int)o, 0, s);
+      if (st != HP_OK) return st;
+    }
+    advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, left);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  h->steps_done += n;
+  return HP_OK;
+}
+
+extern "C" int64_t hp_mono_steps_done(const HpMono* h) { return h ? h->steps_done : -1; }
+
+extern "C" hp_status hp_mono_copy_vm(HpMono* h, int64_t f0, int64_t nf, float* dst,
+                                     int32_t dst_on_device, void* stream) {
+  HP_REQUIRE(h && dst, "hp_mono_copy_vm: null argument");
+  HP_REQUIRE(f0 >= 0 && nf >= 0 && f0 + nf <= h->n_vm_frames,
+             "hp_mono_copy_vm: frames [%lld,%lld) outside [0,%lld)", (long long)f0,
+             (long long)(f0 + nf), (long long)h->n_vm_frames);
+  if (nf == 0 || h->a.n_myo == 0) return HP_OK;
+  HP_CUDA_TRY(cudaMemcpyAsync(dst, h->a.vm_snap + f0 * h->a.n_myo, nf * h->a.n_myo * sizeof(float),
+                              dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                              (cudaStream_t)stream));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_copy_frames(HpMono* h, int64_t f0, int64_t nf, float* dst_surf,
+                                         float* dst_pk, int32_t dst_on_device, void* stream) {
+  HP_REQUIRE(h, "hp_mono_copy_frames: null handle");
+  HP_REQUIRE(f0 >= 0 && nf >= 0 && f0 + nf <= h->n_anim_frames,
+             "hp_mono_copy_frames: frames out of range");
+  const cudaMemcpyKind k = dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dst_surf && h->a.n_surf && nf)
+    HP_CUDA_TRY(cudaMemcpyAsync(dst_surf, h->a.surf_frames + f0 * h->a.n_surf,
+                                nf * h->a.n_surf * sizeof(float), k, s));
+  if (dst_pk && h->a.n_pk && nf)
+    HP_CUDA_TRY(cudaMemcpyAsync(dst_pk, h->a.pk_frames + f0 * h->a.n_pk,
+                                nf * h->a.n_pk * sizeof(float), k, s));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_copy_events(HpMono* h, float* act, int32_t* n_act, float* deact,
+                                         int32_t* n_deact, void* stream) {
+  HP_REQUIRE(h, "hp_mono_copy_events: null handle");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t ns = h->a.n_slots, nm = h->a.n_myo;
+  const int me = h->a.max_events;
+  std::vector<float> t((size_t)me * ns);
+  std::vector<uint8_t> c(ns);
+  for (int pass = 0; pass < 2; ++pass) {
+    float* dt_ = pass ? deact : act;
+    int32_t* dn = pass ? n_deact : n_act;
+    if (!dt_ && !dn) continue;
+    if (ns) {
+      HP_CUDA_TRY(cudaMemcpyAsync(t.data(), pass ? h->a.deact_t : h->a.act_t,
+                                  t.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+      HP_CUDA_TRY(cudaMemcpyAsync(c.data(), pass ? h->a.deact_n : h->a.act_n, ns,
+                                  cudaMemcpyDeviceToHost, s));
+      HP_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    for (int64_t i = 0; i < nm; ++i) {
+      const int32_t sl = h->slot_of_node[i];
+      if (dn) dn[i] = c[sl];
+      if (dt_)
+        for (int e = 0; e < me; ++e) dt_[(int64_t)e * nm + i] = t[(size_t)e * ns + sl];
+    }
+  }
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_copy_v(HpMono* h, float* v_myo, float* v_pk, void* stream) {
+  HP_REQUIRE(h, "hp_mono_copy_v: null handle");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (v_myo && h->a.n_myo) {
+    std::vector<float> v(h->a.n_slots);
+    HP_CUDA_TRY(cudaMemcpyAsync(v.data(), h->a.Vpost, v.size() * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < h->a.n_myo; ++i) v_myo[i] = v[h->slot_of_node[i]];
+  }
+  if (v_pk && h->a.n_pk) {
+    HP_CUDA_TRY(cudaMemcpyAsync(v_pk, h->a.pk_Vpost, h->a.n_pk * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_copy_state(HpMono* h, float* st_slots, float* st_pk, void* stream) {
+  HP_REQUIRE(h, "hp_mono_copy_state: null handle");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st_slots && h->a.n_slots)
+    HP_CUDA_TRY(cudaMemcpyAsync(st_slots, h->a.state, (size_t)N_STATE * h->a.n_slots * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+  if (st_pk && h->a.n_pk)
+    HP_CUDA_TRY(cudaMemcpyAsync(st_pk, h->a.pk_state, (size_t)N_STATE * h->a.n_pk * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_destroy(HpMono* h) {
+  if (!h) return HP_OK;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (void* p : h->allocs) cudaFree(p);
+  delete h;
+  return HP_OK;
+}

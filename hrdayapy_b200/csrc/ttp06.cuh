@@ -1,0 +1,255 @@
+// TTP06 (ten Tusscher & Panfilov 2006) single-cell update in FP32, one
+// thread per cell.  Same kinetics as HrdayaPy's
+// simulation/functions/ionic_models/gpu_ttp06.py:198-412 (_currents_and_gates):
+// Rush-Larsen for the 12 gates, forward Euler for Rprime and the five
+// concentrations with the reference's clamps, phenotype conductances from
+// ttp06_phenotype_constants.py:54-61.
+//
+// Differences from the reference are arithmetic only:
+//   * FP32 instead of FP64;
+//   * constant divisors are folded into multipliers, and exponentials that
+//     the reference evaluates twice are shared (exp((V+30)/10) in tau_f and
+//     tau_f2, exp((-45-V)/10) etc. are separate in the reference but the
+//     values are identical);
+//   * exp2V - 1 in I_CaL is evaluated with expm1f, which is the same
+//     quantity with less cancellation near V = 15 mV (the reference's FP64
+//     has the digits to spare; FP32 does not).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hp {
+
+// state variable order (gpu_ttp06.py:172-176)
+enum StateVar : int {
+  S_KI = 0, S_NAI, S_CAI, S_XR1, S_XR2, S_XS, S_M, S_H, S_J, S_D, S_F, S_F2,
+  S_FCASS, S_S, S_R, S_CASR, S_RPRIME, S_CASS, N_STATE
+};
+
+struct CellParams {
+  float g_Ks;
+  float g_to;
+  float g_Kr;
+  int endo_s;  // 1 = endo/M-cell s-gate, 0 = epi s-gate
+};
+
+// All 18 state variables of one cell, in registers.
+struct CellState {
+  float v[N_STATE];
+};
+
+// Exponential / logarithm used by the kinetics.  HP_FAST_EXP selects the
+// SFU intrinsics (__expf/__logf); otherwise the accurate libdevice versions.
+#ifdef HP_FAST_EXP
+__device__ __forceinline__ float hexp(float x) { return __expf(x); }
+__device__ __forceinline__ float hlog(float x) { return __logf(x); }
+#else
+__device__ __forceinline__ float hexp(float x) { return expf(x); }
+__device__ __forceinline__ float hlog(float x) { return logf(x); }
+#endif
+
+__device__ __forceinline__ float rl_gate(float x, float xinf, float tau, float dt) {
+  return xinf - (xinf - x) * hexp(-dt / tau);
+}
+
+__device__ __forceinline__ float sig(float x) {  // 1 / (1 + exp(x))
+  return 1.0f / (1.0f + hexp(x));
+}
+
+// Advances `c` by dt at membrane voltage V; returns I_ion [mV/ms].
+__device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
+                                            const CellParams p) {
+  // physical constants (gpu_ttp06.py:95-147)
+  constexpr double Rg = 8314.472, Tk = 310.0, Fc = 96485.3415;
+  constexpr float RTF = (float)(Rg * Tk / Fc);
+  constexpr float FRT = (float)(Fc / (Rg * Tk));
+  constexpr float Ko = 5.4f, Nao = 140.0f, Cao = 2.0f;
+  constexpr float g_Na = 14.838f, g_K1 = 5.405f, g_bna = 0.00029f, g_bca = 0.000592f;
+  constexpr float g_pCa = 0.1238f, g_pK = 0.0146f, P_NaK = 2.724f, K_mk = 1.0f;
+  constexpr float K_mNa = 40.0f, K_NaCa = 1000.0f, K_sat = 0.1f, alpha_ = 2.5f;
+  constexpr float gamma_ = 0.35f, Km_Ca = 1.38f, Km_Nai = 87.5f, P_kna = 0.03f;
+  constexpr float K_pCa = 0.0005f;
+  constexpr float k1p = 0.15f, k2p = 0.045f, k3 = 0.06f, k4 = 0.005f, EC = 1.5f;
+  constexpr float max_sr = 2.5f, min_sr = 1.0f, V_rel = 0.102f, V_xfer = 0.0038f;
+  constexpr float K_up = 0.00025f, V_leak = 0.00036f, Vmax_up = 0.006375f;
+  constexpr float Buf_c = 0.2f, K_buf_c = 0.001f, Buf_sr = 10.0f, K_buf_sr = 0.3f;
+  constexpr float Buf_ss = 0.4f, K_buf_ss = 0.00025f;
+  constexpr double V_c = 0.016404, V_sr = 0.001094, V_ss = 0.00005468;
+  constexpr float g_CaL = 3.98e-5f;
+  // derived constants
+  constexpr float inv_VcF = (float)(1.0 / (V_c * Fc));
+  constexpr float inv_2VcF = (float)(1.0 / (2.0 * V_c * Fc));
+  constexpr float inv_2VssF = (float)(1.0 / (2.0 * V_ss * Fc));
+  constexpr float Vsr_Vc = (float)(V_sr / V_c);
+  constexpr float Vsr_Vss = (float)(V_sr / V_ss);
+  constexpr float Vc_Vss = (float)(V_c / V_ss);
+  constexpr float CaL_k = (float)(4.0 * Fc * Fc / (Rg * Tk));
+  constexpr float NaCa_den =
+      (float)((87.5 * 87.5 * 87.5 + 140.0 * 140.0 * 140.0) * (1.38 + 2.0));
+  constexpr float Nao3 = 140.0f * 140.0f * 140.0f;
+  constexpr float NaK_k = P_NaK * Ko / (Ko + K_mk);
+  constexpr float E_Ks_num = Ko + P_kna * Nao;
+  // sqrt(Ko / 5.4) == 1 for Ko = 5.4
+  constexpr float sqko = 1.0f;
+
+  const float Ki = c.v[S_KI], Nai = c.v[S_NAI], Cai = c.v[S_CAI], Cass = c.v[S_CASS];
+  const float CaSR = c.v[S_CASR], Xr1 = c.v[S_XR1], Xr2 = c.v[S_XR2], Xs = c.v[S_XS];
+  const float m = c.v[S_M], h = c.v[S_H], j = c.v[S_J], d = c.v[S_D], f = c.v[S_F];
+  const float f2 = c.v[S_F2], fCass = c.v[S_FCASS], s = c.v[S_S], r = c.v[S_R];
+  const float Rp = c.v[S_RPRIME];
+
+  // reversal potentials
+  const float E_Na = RTF * hlog(Nao / Nai);
+  const float E_K = RTF * hlog(Ko / Ki);
+  const float E_Ks = RTF * hlog(E_Ks_num / (Ki + P_kna * Nai));
+  const float E_Ca = (0.5f * RTF) * hlog(Cao / Cai);
+
+  // INa
+  float t1 = sig((-56.86f - V) * (1.0f / 9.03f));
+  const float m_inf = t1 * t1;
+  const float alpha_m = sig((-60.0f - V) * 0.2f);
+  const float beta_m = 0.1f * sig((V + 35.0f) * 0.2f) + 0.1f * sig((V - 50.0f) * 0.005f);
+  const float tau_m = alpha_m * beta_m;
+  t1 = sig((V + 71.55f) * (1.0f / 7.43f));
+  const float h_inf = t1 * t1;
+  float alpha_h, beta_h, alpha_j, beta_j;
+  if (V < -40.0f) {
+    alpha_h = 0.057f * hexp(-(V + 80.0f) * (1.0f / 6.8f));
+    beta_h = 2.7f * hexp(0.079f * V) + 3.1e5f * hexp(0.3485f * V);
+    alpha_j = ((-25428.0f * hexp(0.2444f * V) - 6.948e-6f * hexp(-0.04391f * V)) *
+               (V + 37.78f)) * sig(0.311f * (V + 79.23f));
+    beta_j = 0.02424f * hexp(-0.01052f * V) * sig(-0.1378f * (V + 40.14f));
+  } else {
+    alpha_h = 0.0f;
+    beta_h = 0.77f / (0.13f * (1.0f + hexp((V + 10.66f) * (-1.0f / 11.1f))));
+    alpha_j = 0.0f;
+    beta_j = 0.6f * hexp(0.057f * V) * sig(-0.1f * (V + 32.0f));
+  }
+  const float tau_h = 1.0f / (alpha_h + beta_h + 1e-30f);
+  const float tau_j = 1.0f / (alpha_j + beta_j + 1e-30f);
+  const float i_Na = g_Na * m * m * m * h * j * (V - E_Na);
+
+  // IKr
+  const float xr1_inf = sig((-26.0f - V) * (1.0f / 7.0f));
+  const float e_m45 = hexp((-45.0f - V) * 0.1f);
+  const float e_p30_10 = hexp((V + 30.0f) * 0.1f);  // shared by tau_f, tau_f2
+  const float tau_xr1 = 450.0f / (1.0f + e_m45) * 6.0f * sig((V + 30.0f) * (1.0f / 11.5f));
+  const float xr2_inf = sig((V + 88.0f) * (1.0f / 24.0f));
+  const float tau_xr2 = 3.0f * sig((-60.0f - V) * 0.05f) * 1.12f * sig((V - 60.0f) * 0.05f);
+  const float i_Kr = p.g_Kr * sqko * Xr1 * Xr2 * (V - E_K);
+
+  // IKs
+  const float xs_inf = sig((-5.0f - V) * (1.0f / 14.0f));
+  const float axs = 1400.0f * rsqrtf(1.0f + hexp((5.0f - V) * (1.0f / 6.0f)));
+  const float bxs = sig((V - 35.0f) * (1.0f / 15.0f));
+  const float tau_xs = axs * bxs + 80.0f;
+  const float i_Ks = p.g_Ks * Xs * Xs * (V - E_Ks);
+
+  // IK1
+  const float VmEK = V - E_K;
+  const float ak1 = 0.1f * sig(0.06f * (VmEK - 200.0f));
+  const float bk1 = (3.0f * hexp(2e-4f * (VmEK + 100.0f)) + hexp(0.1f * (VmEK - 10.0f))) *
+                    sig(-0.5f * VmEK);
+  const float xk1_inf = ak1 / (ak1 + bk1);
+  const float i_K1 = g_K1 * sqko * xk1_inf * VmEK;
+
+  // Ito
+  float s_inf, tau_s;
+  if (p.endo_s) {
+    s_inf = sig((V + 28.0f) * 0.2f);
+    const float a = V + 67.0f;
+    tau_s = 1000.0f * hexp(-a * a * 0.001f) + 8.0f;
+  } else {
+    s_inf = sig((V + 20.0f) * 0.2f);
+    const float a = V + 45.0f;
+    tau_s = 85.0f * hexp(-a * a * (1.0f / 320.0f)) + 5.0f * sig((V - 20.0f) * 0.2f) + 3.0f;
+  }
+  const float r_inf = sig((20.0f - V) * (1.0f / 6.0f));
+  const float a40 = V + 40.0f;
+  const float tau_r = 9.5f * hexp(-a40 * a40 * (1.0f / 1800.0f)) + 0.8f;
+  const float i_to = p.g_to * r * s * VmEK;
+
+  // ICaL
+  const float d_inf = sig((-8.0f - V) * (1.0f / 7.5f));
+  const float tau_d = (1.4f * sig((-35.0f - V) * (1.0f / 13.0f)) + 0.25f) * 1.4f *
+                          sig((V + 5.0f) * 0.2f) +
+                      sig((50.0f - V) * 0.05f);
+  const float f_inf = sig((V + 20.0f) * (1.0f / 7.0f));
+  const float a27 = V + 27.0f;
+  const float tau_f = 1102.5f * hexp(-a27 * a27 * (1.0f / 225.0f)) +
+                      200.0f * sig((13.0f - V) * 0.1f) + 180.0f / (1.0f + e_p30_10) + 20.0f;
+  const float f2_inf = 0.67f * sig((V + 35.0f) * (1.0f / 7.0f)) + 0.33f;
+  const float tau_f2 = 562.0f * hexp(-a27 * a27 * (1.0f / 240.0f)) +
+                       31.0f * sig((25.0f - V) * 0.1f) + 80.0f / (1.0f + e_p30_10);
+  const float cq = (Cass * 20.0f) * (Cass * 20.0f);
+  const float inv_cq = 1.0f / (1.0f + cq);
+  const float fCass_inf = 0.6f * inv_cq + 0.4f;
+  const float tau_fCass = 80.0f * inv_cq + 2.0f;
+
+  const float x2v = 2.0f * (V - 15.0f) * FRT;
+  const float exp2V = hexp(x2v);
+  float denom = expm1f(x2v);
+  if (fabsf(denom) < 1e-10f) denom = 1e-10f;
+  const float i_CaL = g_CaL * d * f * f2 * fCass * CaL_k * (V - 15.0f) *
+                      (0.25f * Cass * exp2V - Cao) / denom;
+
+  // background, pump, exchanger
+  const float i_bNa = g_bna * (V - E_Na);
+  const float i_bCa = g_bca * (V - E_Ca);
+  const float i_pCa = g_pCa * Cai / (Cai + K_pCa);
+  const float i_pK = g_pK * VmEK * sig((25.0f - V) * (1.0f / 5.98f));
+  const float VF = V * FRT;
+  const float i_NaK = NaK_k * Nai / (Nai + K_mNa) /
+                      (1.0f + 0.1245f * hexp(-0.1f * VF) + 0.0353f * hexp(-VF));
+  const float eVg = hexp(gamma_ * VF);
+  const float eVgm1 = hexp((gamma_ - 1.0f) * VF);
+  const float i_NaCa = K_NaCa * (eVg * Nai * Nai * Nai * Cao - eVgm1 * Nao3 * Cai * alpha_) /
+                       (NaCa_den * (1.0f + K_sat * eVgm1));
+
+  const float I_ion = i_K1 + i_to + i_Kr + i_Ks + i_CaL + i_NaK + i_Na + i_bNa + i_NaCa +
+                      i_bCa + i_pCa + i_pK;
+
+  // SR calcium
+  const float ecs = EC / CaSR;
+  const float kcasr = max_sr - (max_sr - min_sr) / (1.0f + ecs * ecs);
+  const float k1 = k1p / kcasr, k2 = k2p * kcasr;
+  const float Cass2 = Cass * Cass;
+  const float O = k1 * Cass2 * Rp / (k3 + k1 * Cass2 + 1e-30f);
+  const float i_rel = V_rel * O * (CaSR - Cass);
+  const float i_up = Vmax_up / (1.0f + K_up * K_up / (Cai * Cai + 1e-30f));
+  const float i_leak = V_leak * (CaSR - Cai);
+  const float i_xfer = V_xfer * (Cass - Cai);
+  const float bc = Cai + K_buf_c, bsr = CaSR + K_buf_sr, bss = Cass + K_buf_ss;
+  const float bufc = 1.0f / (1.0f + Buf_c * K_buf_c / (bc * bc));
+  const float bufsr = 1.0f / (1.0f + Buf_sr * K_buf_sr / (bsr * bsr));
+  const float bufss = 1.0f / (1.0f + Buf_ss * K_buf_ss / (bss * bss));
+
+  const float dNai = -(i_Na + i_bNa + 3.0f * i_NaK + 3.0f * i_NaCa) * inv_VcF;
+  const float dKi = -(i_K1 + i_to + i_Kr + i_Ks + i_pK - 2.0f * i_NaK) * inv_VcF;
+  const float dCai = bufc * ((i_leak - i_up) * Vsr_Vc + i_xfer -
+                             (i_bCa + i_pCa - 2.0f * i_NaCa) * inv_2VcF);
+  const float dCaSR = bufsr * (i_up - i_rel - i_leak);
+  const float dCass = bufss * (-i_CaL * inv_2VssF + i_rel * Vsr_Vss - i_xfer * Vc_Vss);
+
+  c.v[S_M] = rl_gate(m, m_inf, tau_m, dt);
+  c.v[S_H] = rl_gate(h, h_inf, tau_h, dt);
+  c.v[S_J] = rl_gate(j, h_inf, tau_j, dt);
+  c.v[S_XR1] = rl_gate(Xr1, xr1_inf, tau_xr1, dt);
+  c.v[S_XR2] = rl_gate(Xr2, xr2_inf, tau_xr2, dt);
+  c.v[S_XS] = rl_gate(Xs, xs_inf, tau_xs, dt);
+  c.v[S_D] = rl_gate(d, d_inf, tau_d, dt);
+  c.v[S_F] = rl_gate(f, f_inf, tau_f, dt);
+  c.v[S_F2] = rl_gate(f2, f2_inf, tau_f2, dt);
+  c.v[S_FCASS] = rl_gate(fCass, fCass_inf, tau_fCass, dt);
+  c.v[S_S] = rl_gate(s, s_inf, tau_s, dt);
+  c.v[S_R] = rl_gate(r, r_inf, tau_r, dt);
+  c.v[S_RPRIME] = Rp + dt * (-k2 * Cass * Rp + k4 * (1.0f - Rp));
+  c.v[S_NAI] = fmaxf(Nai + dt * dNai, 1e-3f);
+  c.v[S_KI] = fmaxf(Ki + dt * dKi, 1e-3f);
+  c.v[S_CAI] = fmaxf(Cai + dt * dCai, 1e-7f);
+  c.v[S_CASR] = fmaxf(CaSR + dt * dCaSR, 1e-7f);
+  c.v[S_CASS] = fmaxf(Cass + dt * dCass, 1e-7f);
+  return I_ion;
+}
+
+}  // namespace hp

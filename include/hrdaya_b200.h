@@ -1,0 +1,174 @@
+/*
+ * hrdaya_b200.h -- C ABI of the B200-native HrdayaPy hot path.
+ *
+ * One shared library (libhrdaya_b200.so) exports these entry points.  They
+ * take plain pointers and sizes; device buffers are owned by the handles
+ * (allocated at create, freed at destroy) and results are copied out to
+ * caller-owned memory, host or device.  Every call returns an hp_status;
+ * hp_last_error() gives the message of the last failure on this thread.
+ * Handles are not thread-safe (same contract as the reference's solvers,
+ * which are single-threaded Python).  `stream` arguments are cudaStream_t
+ * passed as void* (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the HrdayaPy project):
+ *   hp_mono_*   -- the time loop of run_coupled
+ *                  (simulation/functions/purkinje_myocardium_pipeline.py:1030-1463)
+ *                  and purkinje_myocardium_anisotropic_solver
+ *                  (anisotropic_simulation/functions/
+ *                   purkinje_myocardium_anisotropic_solver.py:1308-1881):
+ *                  HeteroIonicSolver.step (ionic_models/hetero_solver.py:141-194),
+ *                  the V update (pipeline.py:1379-1382), the global
+ *                  Laplacian mat-vec and solve (pipeline.py:578-754), the clamp,
+ *                  the Vm snapshot / animation frame writers (pipeline.py:1395-1412)
+ *                  and the activation-time extraction of
+ *                  compute_activation_maps (activation_maps.py:295-350).
+ *   hp_torso_*  -- make_gpu_solver / solve_frame / _pcg_gpu
+ *                  (ecg/functions/compute_bspm.py:164-436) over the stiffness
+ *                  operator of _assemble_stiffness (ecg/functions/build_torso_grid.py:276-397).
+ */
+#ifndef HRDAYA_B200_H
+#define HRDAYA_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HP_OK = 0,
+  HP_ERR_INVALID = 1,       /* bad argument (maps to ValueError) */
+  HP_ERR_OOM = 2,           /* device allocation failed */
+  HP_ERR_CUDA = 3,          /* CUDA runtime error */
+  HP_ERR_NOT_CONVERGED = 4, /* iteration limit reached */
+  HP_ERR_STAGNATED = 5,     /* Krylov stagnation / breakdown */
+  HP_ERR_NONFINITE = 6,     /* NaN / Inf detected */
+  HP_ERR_TIMEOUT = 7,       /* bounded device wait expired */
+  HP_ERR_UNSUPPORTED = 8    /* configuration not built into this library */
+} hp_status;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *hp_last_error(void);
+/* Library version string. */
+const char *hp_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Monodomain (fused TTP06 + 19-point stencil + activation recording)  */
+/* ------------------------------------------------------------------ */
+
+/* Voxel tag bits (uint32 per voxel slot). */
+#define HP_TAG_PHENO_MASK 0x3u        /* 0 = not tissue, 1 endo, 2 mid, 3 epi */
+#define HP_TAG_FACE_SHIFT 2           /* 6 bits: +i -i +j -j +k -k neighbour in mask */
+#define HP_TAG_DIAG_SHIFT 8           /* 12 bits: edge-diagonal neighbours in mask */
+#define HP_TAG_STIM_SHIFT 20          /* 8 bits: stimulus-site membership */
+#define HP_TAG_PMJ (1u << 28)         /* voxel coupled to Purkinje junction(s) */
+#define HP_TAG_SURF (1u << 29)        /* voxel is an animation-surface node */
+#define HP_MAX_SITES 8
+#define HP_MAX_VARIANTS 64
+
+/*
+ * Geometry and parameters of one monodomain problem (or of a batched
+ * ensemble of independent variants, concatenated brick by brick).
+ * All pointers are HOST pointers; hp_mono_create copies them to the device.
+ *
+ * Voxels live in bricks of bi x bj x bk (k fastest); slot = brick * bv +
+ * (li * bj + lj) * bk + lk.  brick_nbr holds, per brick, the 27 neighbouring
+ * brick ids in (di, dj, dk) order with di slowest, -1 where absent (index 13
+ * is the brick itself).
+ *
+ * Diffusion coefficients are pre-scaled by dt / (Cm * Ai) so that one
+ * explicit step is V += sum_j coef_ij (V_j - V_i):
+ *   isotropic:   coef = iso_coef for every face neighbour in the mask;
+ *   anisotropic: face coef to +i/+j/+k stored per voxel (wface, 3 x n_slots,
+ *                zero where the edge does not exist), edge-diagonal coef
+ *                = +/-(doff_a + doff_b) / 4 from the per-voxel off-diagonal
+ *                tensor components doff (3 x n_slots: D01, D02, D12 scaled).
+ */
+typedef struct {
+  int32_t n_bricks;
+  int32_t bi, bj, bk;           /* brick shape; must be a compiled shape */
+  int32_t anisotropic;          /* 0: 7-point, 1: 19-point */
+  const int32_t *brick_nbr;     /* n_bricks x 27 */
+  const uint32_t *tag;          /* n_slots */
+  const float *wface;           /* 3 x n_slots (anisotropic) */
+  const float *doff;            /* 3 x n_slots (anisotropic) */
+  float iso_coef;               /* isotropic face coefficient */
+  const uint8_t *brick_variant; /* n_bricks, or NULL (all variant 0) */
+  int32_t n_variants;
+  const float *variant_gks;     /* n_variants multipliers of g_Ks */
+  const float *variant_gkr;     /* n_variants multipliers of g_Kr */
+
+  /* Purkinje network: n_pk nodes, CSR neighbours; a neighbour index
+   * j >= 0 is a Purkinje node, j < 0 is myocardial slot (-j - 1). */
+  int32_t n_pk;
+  const int32_t *pk_ptr;        /* n_pk + 1 */
+  const int32_t *pk_idx;
+  const float *pk_coef;
+  const uint8_t *pk_stim;       /* n_pk stimulus-site bits */
+  const uint8_t *pk_variant;    /* n_pk, or NULL */
+  /* myocardial side of the junctions: for voxels tagged HP_TAG_PMJ,
+   * pmj_row[slot] indexes the CSR (pmj_ptr, pmj_pk, pmj_coef). */
+  int32_t n_pmj_rows;
+  const int32_t *pmj_row;       /* n_slots (only read where tagged) */
+  const int32_t *pmj_ptr;       /* n_pmj_rows + 1 */
+  const int32_t *pmj_pk;
+  const float *pmj_coef;
+
+  /* time stepping and stimulus */
+  double dt;                    /* ms */
+  double Cm;                    /* uF/mm^2 */
+  float v0;                     /* initial membrane potential, mV */
+  int64_t n_steps;              /* total steps of the run */
+  int32_t n_sites;
+  const float *site_amp;        /* n_sites, uA/mm^2 */
+  const uint8_t *site_on;       /* n_steps + 1 bitmasks: sites firing at t = step * dt */
+
+  /* outputs */
+  int32_t n_myo;                /* myocardial nodes in reference order */
+  const int32_t *slot_of_node;  /* n_myo */
+  int64_t vm_every;             /* Vm snapshot every vm_every steps (0 = off) */
+  int32_t n_surf;               /* animation surface nodes */
+  const int32_t *surf_of_slot;  /* n_slots (read where HP_TAG_SURF) */
+  int64_t frame_every;          /* animation frame every frame_every steps (0 = off) */
+  float act_threshold;          /* mV, upstroke crossing */
+  float deact_threshold;        /* mV, downstroke crossing */
+  int32_t max_events;           /* activation events kept per voxel (1..16) */
+} HpMonoDesc;
+
+typedef struct HpMono HpMono;
+
+/* Allocates device state, uploads the description, initialises every cell to
+ * the TTP06 resting state at v0 and runs the ionic half-step of step 0.  The
+ * returned handle is bound to the current device. */
+hp_status hp_mono_create(const HpMonoDesc *desc, HpMono **out, void *stream);
+/* Advances n steps (n <= remaining).  Kernels are enqueued on `stream`; time
+ * loops of `graph_chunk` > 0 steps are replayed from a CUDA graph. */
+hp_status hp_mono_run(HpMono *h, int64_t n, int32_t graph_chunk, void *stream);
+/* Steps done so far. */
+int64_t hp_mono_steps_done(const HpMono *h);
+/* Copies snapshots [f0, f0 + nf) (each n_myo floats, reference node order)
+ * to dst; dst_on_device selects cudaMemcpyDeviceToDevice. */
+hp_status hp_mono_copy_vm(HpMono *h, int64_t f0, int64_t nf, float *dst,
+                          int32_t dst_on_device, void *stream);
+/* Animation frames [f0, f0 + nf): surface part (n_surf floats each) and
+ * Purkinje part (n_pk floats each); either destination may be NULL. */
+hp_status hp_mono_copy_frames(HpMono *h, int64_t f0, int64_t nf, float *dst_surf,
+                              float *dst_pk, int32_t dst_on_device, void *stream);
+/* Activation / deactivation events in reference node order:
+ * act (max_events x n_myo, NaN = none), n_act (n_myo); same for deact.
+ * Host destinations. */
+hp_status hp_mono_copy_events(HpMono *h, float *act, int32_t *n_act, float *deact,
+                              int32_t *n_deact, void *stream);
+/* Current membrane potential after the last step: myocardium (n_myo, node
+ * order) and Purkinje (n_pk).  Host destinations, either may be NULL. */
+hp_status hp_mono_copy_v(HpMono *h, float *v_myo, float *v_pk, void *stream);
+/* Raw state access for checkpointing: the 18 TTP06 variables of every slot
+ * (18 x n_slots) and Purkinje node (18 x n_pk) as last written. */
+hp_status hp_mono_copy_state(HpMono *h, float *state_slots, float *state_pk, void *stream);
+hp_status hp_mono_destroy(HpMono *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HRDAYA_B200_H */
