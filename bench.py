@@ -194,11 +194,10 @@ def e2e_run(prob, args, fs):
     """hp_mono_create from host arrays + K frames + D2H of each frame."""
     import torch
     from hrdayapy_b200 import monodomain as M
+    import dataclasses
     k = max(1, min(args.steps, 10))
-    p2 = M.MonoProblem(**{**prob.__dict__})
-    p2.n_steps = k * fs
-    p2.site_on = prob.site_on[: k * fs + 1].copy()
-    p2.vm_every = fs
+    p2 = dataclasses.replace(prob, n_steps=k * fs, site_on=prob.site_on[: k * fs + 1].copy(),
+                             vm_every=fs)
     h2d = (p2.tag.nbytes + (p2.wface.nbytes + p2.doff.nbytes if p2.anisotropic else 0) +
            p2.layout.brick_nbr.nbytes + p2.pk_ptr.nbytes + p2.pk_idx.nbytes +
            p2.pk_coef.nbytes + p2.pmj_row.nbytes + p2.surf_of_slot.nbytes +
@@ -225,21 +224,19 @@ def cpu_baseline(prob, info, args, budget_s=15.0):
     from hrdayapy_b200 import synthetic
     g = synthetic.last_inputs()
     nthreads = orc.lib().orc_num_threads()
+    ctx = orc.setup(*g["args"], vm_save_dt=None, **g["kw"])
     t0 = time.perf_counter()
-    r = None
-    n = 2
-    elapsed = 0.0
-    while True:
-        t0 = time.perf_counter()
-        r = orc.run(*g["args"], vm_save_dt=None, **{**g["kw"], "T": n * g["kw"]["dt"]})
-        elapsed = time.perf_counter() - t0
-        if elapsed > budget_s / 4 or n >= 64:
-            break
-        n *= 4
-    N = len(r["V"])
+    orc.advance(ctx, 2, snapshots=False)
+    per_step = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(500, budget_s / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    orc.advance(ctx, n, snapshots=False)
+    elapsed = time.perf_counter() - t0
+    N = ctx["N"]
     return {"value": N * n / elapsed, "unit": "voxel-steps/s", "cores": int(nthreads),
             "kind": "port",
-            "sample": f"{n} time steps of the full workload ({N} nodes), FP64, set-up excluded"}
+            "sample": f"{n} time steps of the full workload ({N} nodes incl. Purkinje), "
+                      f"FP64, set-up excluded"}
 
 
 def run_reference(args):
@@ -251,13 +248,15 @@ def run_reference(args):
     prob, info = build_workload(args.workload)
     g = synthetic.last_inputs()
     n_per = 2 if args.workload == "biv_shell" else 50
+    kw = dict(g["kw"])
+    kw["T"] = (args.warmup + args.steps) * n_per * kw["dt"] + kw["dt"]
+    ctx = orc.setup(*g["args"], vm_save_dt=None, **kw)
+    N = ctx["N"]
     times = []
-    N = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        r = orc.run(*g["args"], vm_save_dt=None, **{**g["kw"], "T": n_per * g["kw"]["dt"]})
+        orc.advance(ctx, n_per, snapshots=False)
         dt_s = time.perf_counter() - t0
-        N = len(r["V"])
         if i >= args.warmup:
             times.append(dt_s)
     tot = sum(times)

@@ -280,19 +280,16 @@ def phenotypes(Np, phi_myo, phi_endo_max, phi_epi_min):
 # Full run
 # --------------------------------------------------------------------------
 
-def run(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
-        dx_p=0.2, sigma_P=0.225, sigma_M=6.5625e-5, sigma_l=None, sigma_t=None,
-        Cm=0.01, A_P=133.33, A_M=140.0, R_P=0.015, dt=0.02, T=10.0,
-        stim_protocol=None, ectopic_region=None, stim_regions=None,
-        stim_len_mm=2.0, c_pmj=0.05, n_pmj=1, phi_endo_max=0.35, phi_epi_min=0.65,
-        vm_save_dt=None, gks_scale=1.0, gkr_scale=1.0, anisotropic=False):
-    """theta = 0 FP64 run of the reference method.
-
-    ``anisotropic=True`` follows the anisotropic solver (A_P = 2/R_P, fibre
-    tensor, 18-connected mesh); otherwise run_coupled (A_P argument,
-    uniform sigma_M).  Returns a dict with ``Vm`` (n_snap, N_myo) float32,
-    ``time_vm`` float32, ``Vp`` Purkinje snapshots, final ``V``/``state``.
-    """
+def setup(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
+          dx_p=0.2, sigma_P=0.225, sigma_M=6.5625e-5, sigma_l=None, sigma_t=None,
+          Cm=0.01, A_P=133.33, A_M=140.0, R_P=0.015, dt=0.02, T=10.0,
+          stim_protocol=None, ectopic_region=None, stim_regions=None,
+          stim_len_mm=2.0, c_pmj=0.05, n_pmj=1, phi_endo_max=0.35, phi_epi_min=0.65,
+          vm_save_dt=None, gks_scale=1.0, gkr_scale=1.0, anisotropic=False):
+    """Set-up of the reference method (theta = 0): assembled L, phenotypes,
+    stimulus schedule, resting state.  ``anisotropic=True`` follows the
+    anisotropic solver (A_P = 2/R_P, fibre tensor, 18-connected mesh);
+    otherwise run_coupled (A_P argument, uniform sigma_M)."""
     h = float(voxel_size)
     nodes_mm = np.asarray(nodes, np.float32) * h
     elements = np.asarray(elements, np.int64)
@@ -335,7 +332,24 @@ def run(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
     if stim_protocol is None:
         stim_protocol = [dict(name="av_node", target="root", amp=12.0, dur=2.0, onset=0.0)]
     sites = resolve_stim_sites(stim_protocol, root_mask, ectopic_region, vox, Np, stim_regions)
+    snap_every = max(1, int(round(vm_save_dt / dt))) if vm_save_dt else 1
+    Lc = L.tocsr()
+    Lc.sort_indices()
+    return dict(L=L, ptr=Lc.indptr.astype(np.int64), idx=Lc.indices.astype(np.int32),
+                val=Lc.data.astype(np.float64), N=N, Np=Np, pheno=pheno, sites=sites,
+                dt=float(dt), Cm=float(Cm), n_steps=n_steps, snap_every=snap_every,
+                V=np.full(N, V0), state=np.tile(TTP06_INIT, (N, 1)),
+                gks=np.full(N, float(gks_scale)), gkr=np.full(N, float(gkr_scale)),
+                step=0, vox_idx=vox, comp_nodes=comp, comp_edges=cedges, branch_map=bmaps,
+                pmj_ids=pmj_ids, pmj_patches=patches)
+
+
+def advance(ctx, n_steps, snapshots=True):
+    """Runs n_steps more time steps (C time loop); returns (Vm, Vp, times)
+    snapshots taken in this call (float32), labelled t = step * dt."""
+    sites = ctx["sites"]
     nS = len(sites)
+    dt, k0 = ctx["dt"], ctx["step"]
     site_ptr = np.zeros(nS + 1, np.int64)
     site_ptr[1:] = np.cumsum([len(s[0]) for s in sites])
     site_nodes = (np.concatenate([s[0] for s in sites]).astype(np.int32)
@@ -343,30 +357,39 @@ def run(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
     site_amp = np.array([s[1]["amp"] for s in sites], np.float64)
     on = np.zeros((max(n_steps, 1), max(nS, 1)), np.uint8)
     for k in range(n_steps):
-        t = k * dt
+        t = (k0 + k) * dt
         for s, (_, st) in enumerate(sites):
             on[k, s] = stim_active(t, st["onset"], st["dur"], st["period"], st["n_pulses"])
-    snap_every = max(1, int(round(vm_save_dt / dt))) if vm_save_dt else 1
-    n_snap = (n_steps + snap_every - 1) // snap_every
-    snaps = np.zeros((n_snap, N_myo), np.float32)
-    psnaps = np.zeros((n_snap, Np), np.float32)
-    V = np.full(N, V0)
-    state = np.tile(TTP06_INIT, (N, 1))
-    gks = np.full(N, float(gks_scale)); gkr = np.full(N, float(gkr_scale))
-    Lc = L.tocsr()
-    Lc.sort_indices()
-    ptr = Lc.indptr.astype(np.int64); idx = Lc.indices.astype(np.int32)
-    val = Lc.data.astype(np.float64)
-    rc = lib().orc_mono_run(N, Np, _p(ptr), _p(idx), _p(val), _p(pheno), _p(gks), _p(gkr),
-                            float(dt), float(Cm), n_steps, nS, _p(site_ptr), _p(site_nodes),
-                            _p(site_amp), _p(on), _p(V), _p(state), snap_every,
+    se = ctx["snap_every"]
+    N, Np = ctx["N"], ctx["Np"]
+    # snapshot steps of this call, in global step numbering
+    first = (-k0) % se
+    n_snap = len(range(first, n_steps, se)) if snapshots else 0
+    snaps = np.zeros((max(n_snap, 1), N - Np), np.float32)
+    psnaps = np.zeros((max(n_snap, 1), Np), np.float32)
+    if snapshots and k0 % se != 0 and n_snap:
+        raise ValueError("advance() must start on a snapshot boundary when snapshots are on")
+    rc = lib().orc_mono_run(N, Np, _p(ctx["ptr"]), _p(ctx["idx"]), _p(ctx["val"]),
+                            _p(ctx["pheno"]), _p(ctx["gks"]), _p(ctx["gkr"]), dt, ctx["Cm"],
+                            n_steps, nS, _p(site_ptr), _p(site_nodes), _p(site_amp), _p(on),
+                            _p(ctx["V"]), _p(ctx["state"]), se if snapshots else 0,
                             _p(snaps), _p(psnaps))
     if rc != 0:
         raise RuntimeError(f"orc_mono_run failed ({rc})")
-    times = np.array([k * dt for k in range(0, n_steps, snap_every)], np.float32)
-    return dict(Vm=snaps, Vp=psnaps, time_vm=times, V=V, state=state, vox_idx=vox,
-                Np=Np, comp_nodes=comp, comp_edges=cedges, branch_map=bmaps,
-                pmj_ids=pmj_ids, pmj_patches=patches, L=L, pheno=pheno)
+    ctx["step"] = k0 + n_steps
+    times = np.array([(k0 + k) * dt for k in range(first, n_steps, se)], np.float32)
+    return snaps[:n_snap], psnaps[:n_snap], times
+
+
+def run(nodes, elements, act_times, S, phi, **kw):
+    """Full theta = 0 FP64 run of the reference method from rest.  Returns
+    ``Vm`` (n_snap, N_myo) float32, ``time_vm``, ``Vp`` Purkinje snapshots,
+    final ``V``/``state`` and the set-up bookkeeping."""
+    ctx = setup(nodes, elements, act_times, S, phi, **kw)
+    Vm, Vp, t = advance(ctx, ctx["n_steps"])
+    out = dict(ctx)
+    out.update(Vm=Vm, Vp=Vp, time_vm=t)
+    return out
 
 
 def activation_maps(Vm, t, act_threshold=-40.0, deact_threshold=-40.0):
