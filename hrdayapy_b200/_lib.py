@@ -76,14 +76,31 @@ def lib():
     return L
 
 
+class HpTorsoDesc(C.Structure):
+    _fields_ = [
+        ("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("h_m", C.c_double),
+        ("label", P), ("n_materials", C.c_int32), ("sigma", P), ("pin_row", C.c_int64),
+        ("n_heart", C.c_int32), ("heart_nbr", P), ("proj", P), ("coeff", C.c_double),
+        ("n_expected", C.c_double), ("n_read", C.c_int32), ("read_rows", P),
+    ]
+
+
+class HpSolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32),
+                ("rel_residual", C.c_double), ("stat", C.c_double), ("restarts", C.c_int32)]
+
+
 def _declare_optional(L):
-    """Signatures of the torso / preconditioner entry points (declared in
-    include/hrdaya_b200.h); set up lazily so older builds still load."""
-    try:
-        from . import _lib_torso
-        _lib_torso.declare(L)
-    except ImportError:
-        pass
+    """Signatures of the torso entry points (include/hrdaya_b200.h)."""
+    L.hp_torso_create.argtypes = [C.POINTER(HpTorsoDesc), C.POINTER(P), P]
+    L.hp_torso_rows.argtypes = [P]
+    L.hp_torso_rows.restype = C.c_int64
+    L.hp_torso_solve_frame.argtypes = [P, P, C.c_int32, P, C.c_int32, C.c_double, C.c_int32,
+                                       C.c_int32, C.POINTER(HpSolveStats), P]
+    L.hp_torso_copy_solution.argtypes = [P, P, P]
+    L.hp_torso_copy_rhs.argtypes = [P, P, P]
+    L.hp_torso_reset.argtypes = [P]
+    L.hp_torso_destroy.argtypes = [P]
 
 
 def check(status: int, what: str = ""):

@@ -603,7 +603,8 @@ extern "C" hp_status hp_mono_run(HpMono* h, int64_t n, int32_t graph_chunk, void
              (long long)(h->n_steps - h->steps_done));
   cudaStream_t s = (cudaStream_t)stream;
   int64_t left = n;
-  if (graph_chunk > 0 && left >= graph_chunk) {
+  // the legacy default stream cannot be captured: launch directly there
+  if (graph_chunk > 0 && left >= graph_chunk && s != nullptr) {
     if (!h->graph || h->graph_chunk != graph_chunk || h->graph_stream != s) {
       if (h->graph) {
         cudaGraphExecDestroy(h->graph);

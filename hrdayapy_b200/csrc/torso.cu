@@ -1,0 +1,780 @@
+// Per-frame torso Poisson solve (ECG forward problem) for sm_100a.
+//
+// Replaces make_gpu_solver / solve_frame / _pcg_gpu of the reference
+// (ecg/functions/compute_bspm.py:164-436) over the sharp-boundary 7-point
+// operator of _assemble_stiffness (ecg/functions/build_torso_grid.py:276-397):
+//   A_kk = sum_faces g_f,  A_kn = -g_f,  g_f = harm(sigma_k, sigma_n) / h^2,
+// air faces skipped (Neumann), one pinned row fixed to 0.
+//
+// The operator is never assembled.  Conductivity is piecewise constant by
+// material label, so a face conductance is a lookup in an M x M table; the
+// solver keeps one byte per voxel of operator data instead of 7 CSR entries.
+// Grid arrays are dense over the torso box padded by one air voxel on every
+// side (no bounds tests in the stencil); k is the fastest axis, so a warp's
+// accesses and its +/-k neighbours are contiguous and the +/-j, +/-i
+// neighbours are rows / planes that the previous warps just brought into L2.
+//
+// Precision: vectors r, p, Ap and the SpMV run in FP32; the solution x and
+// every dot product / norm are FP64; the convergence decision for the
+// relative rule is taken on the FP64 true residual b - A x evaluated with the
+// FP64 conductance table (the reference operator's own coefficients).  If the
+// recursive FP32 residual claims convergence but the true residual does not,
+// r is replaced by the true residual and CG restarts (residual replacement).
+//
+// Reductions are deterministic: each block writes its partial, the last block
+// to arrive (atomic ticket after __threadfence) sums the partials in block
+// order and updates the scalars.  No kernel ever waits on another block.
+#include "hp_common.cuh"
+
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+namespace hp {
+
+constexpr int TB = 256;            // threads per block
+constexpr int NPART = 4;           // partial sums per block
+
+enum Scal : int {
+  SC_RZ = 0, SC_PAP, SC_ALPHA, SC_BETA, SC_ALPHA_PREV, SC_ZZ, SC_ZMAX, SC_RR, SC_BB,
+  SC_TRUE_RR, SC_SRC_MEAN, SC_STAT, SC_TOL, N_SCAL
+};
+enum IScal : int { IS_DONE = 0, IS_ITER, IS_RULE, IS_MAXIT, IS_BREAKDOWN, IS_NONFINITE, N_ISCAL };
+
+struct TorsoArgs {
+  int64_t ng;          // padded grid cells
+  int32_t pj, pk;      // padded dims j, k (i stride = pj * pk)
+  const uint8_t* label;
+  const float* invd;
+  float* r;
+  float* p0;
+  float* p1;
+  float* Ap;
+  double* x;
+  float* b;
+  int64_t pin;         // padded grid index of the pinned voxel
+  int64_t n_rows;
+  double* scal;
+  int32_t* iscal;
+  double* part;        // gridDim x NPART
+  unsigned int* ticket;
+};
+
+__constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
+__constant__ double c_T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-reduces NV sums (and optionally one max stored as v[NV-1] when
+// last_is_max) into part[blockIdx], then returns true in the one block that
+// arrived last, after which `tot` holds the grid totals in every thread of
+// that block.
+template <int NV>
+__device__ bool block_reduce_last(double (&v)[NV], bool last_is_max, double* part,
+                                  unsigned int* ticket, double (&tot)[NV]) {
+  __shared__ double sh[TB / 32][NV];
+  __shared__ bool am_last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double w = (last_is_max && q == NV - 1) ? (double)warp_max((float)v[q]) : warp_sum(v[q]);
+    if (lane == 0) sh[wid][q] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = sh[0][q];
+      for (int w = 1; w < TB / 32; ++w)
+        s = (last_is_max && q == NV - 1) ? fmax(s, sh[w][q]) : s + sh[w][q];
+      part[(int64_t)blockIdx.x * NPART + q] = s;
+    }
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  // the last block sums all partials in block order (deterministic)
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = (last_is_max && q == NV - 1) ? 0.0 : 0.0;
+  for (int blk = threadIdx.x; blk < (int)gridDim.x; blk += TB) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      const double pv = ((volatile double*)part)[(int64_t)blk * NPART + q];
+      v[q] = (last_is_max && q == NV - 1) ? fmax(v[q], pv) : v[q] + pv;
+    }
+  }
+  // fixed-order tree over the block
+  __shared__ double sh2[TB][NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sh2[threadIdx.x][q] = v[q];
+  __syncthreads();
+  for (int s = TB / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        sh2[threadIdx.x][q] = (last_is_max && q == NV - 1)
+                                  ? fmax(sh2[threadIdx.x][q], sh2[threadIdx.x + s][q])
+                                  : sh2[threadIdx.x][q] + sh2[threadIdx.x + s][q];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < NV; ++q) tot[q] = sh2[0][q];
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+__device__ __forceinline__ bool is_row(const TorsoArgs& a, int64_t g) {
+  return a.label[g] != 0 && g != a.pin;
+}
+
+// Iteration part 1: pending x update, p <- z + beta p (z = M^-1 r), Ap = A p,
+// partial p.Ap.
+__global__ void __launch_bounds__(TB) pcg_k1(TorsoArgs a, int parity) {
+  if (a.iscal[IS_DONE]) return;
+  const double beta = a.scal[SC_BETA];
+  const double alpha_prev = a.scal[SC_ALPHA_PREV];
+  const float betaf = (float)beta;
+  const float* __restrict__ pin_ = parity ? a.p1 : a.p0;
+  float* __restrict__ pout = parity ? a.p0 : a.p1;
+  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  double acc[1] = {0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * TB) {
+    const int l = a.label[g];
+    if (l == 0 || g == a.pin) continue;
+    const float pold = pin_[g];
+    if (alpha_prev != 0.0) a.x[g] += alpha_prev * (double)pold;
+    const float pn = a.invd[g] * a.r[g] + betaf * pold;
+    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+    float diag = 0.0f, off = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int64_t n = nb[f];
+      const float t = c_T32[l * HP_MAX_MATERIALS + a.label[n]];
+      diag += t;
+      const float pnn = a.invd[n] * a.r[n] + betaf * pin_[n];
+      off += t * pnn;
+    }
+    const float ap = diag * pn - off;
+    pout[g] = pn;
+    a.Ap[g] = ap;
+    acc[0] += (double)pn * (double)ap;
+  }
+  double tot[1];
+  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+    const double pAp = tot[0];
+    a.scal[SC_PAP] = pAp;
+    a.scal[SC_ALPHA_PREV] = 0.0;   // every block applied the pending x update
+    if (!(fabs(pAp) >= 1e-30) || !isfinite(pAp)) {   // breakdown, as the reference's |pAp| < 1e-30
+      a.iscal[IS_BREAKDOWN] = isfinite(pAp) ? 1 : 0;
+      a.iscal[IS_NONFINITE] = isfinite(pAp) ? 0 : 1;
+      a.iscal[IS_DONE] = 1;
+      a.scal[SC_ALPHA] = 0.0;
+    } else {
+      a.scal[SC_ALPHA] = a.scal[SC_RZ] / pAp;
+    }
+  }
+}
+
+// Iteration part 2: r -= alpha Ap, z = M^-1 r, partial r.z, z.z, r.r, max|z|;
+// the last block forms beta and tests the stopping rule.
+__global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
+  if (a.iscal[IS_DONE]) return;
+  const double alpha = a.scal[SC_ALPHA];
+  const float alphaf = (float)alpha;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * TB) {
+    if (!is_row(a, g)) continue;
+    const float r = a.r[g] - alphaf * a.Ap[g];
+    a.r[g] = r;
+    const float z = a.invd[g] * r;
+    acc[0] += (double)r * z;
+    acc[1] += (double)z * z;
+    acc[2] += (double)r * r;
+    acc[3] = fmax(acc[3], (double)fabsf(z));
+  }
+  double tot[4];
+  if (block_reduce_last<4>(acc, true, a.part, a.ticket, tot) && threadIdx.x == 0) {
+    const double rz_new = tot[0];
+    a.scal[SC_BETA] = rz_new / a.scal[SC_RZ];
+    a.scal[SC_RZ] = rz_new;
+    a.scal[SC_ALPHA_PREV] = alpha;
+    a.scal[SC_ZZ] = tot[1];
+    a.scal[SC_RR] = tot[2];
+    a.scal[SC_ZMAX] = tot[3];
+    const int it = ++a.iscal[IS_ITER];
+    const int rule = a.iscal[IS_RULE];
+    double stat;
+    if (rule == HP_STOP_RMS) stat = sqrt(tot[1] / (double)a.n_rows);
+    else if (rule == HP_STOP_LINF) stat = tot[3];
+    else stat = sqrt(tot[2] / fmax(a.scal[SC_BB], 1e-300));  // recursive estimate
+    a.scal[SC_STAT] = stat;
+    // REL: stop the recursion a little below tol; the true residual decides
+    const double lim = rule == HP_STOP_REL ? 0.5 * a.scal[SC_TOL] : a.scal[SC_TOL];
+    if (!isfinite(rz_new)) { a.iscal[IS_NONFINITE] = 1; a.iscal[IS_DONE] = 1; }
+    else if (stat < lim || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
+  }
+}
+
+// x += alpha_prev * p (the pending update of the last iteration).
+__global__ void __launch_bounds__(TB) pcg_finish_x(TorsoArgs a, int parity) {
+  const double alpha = a.scal[SC_ALPHA_PREV];
+  const float* __restrict__ p = parity ? a.p1 : a.p0;
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * TB)
+    if (is_row(a, g)) a.x[g] += alpha * (double)p[g];
+}
+
+// FP64 true residual r = b - A x (written to r in FP32), and ||r||^2,
+// ||b||^2, r.M^-1 r.  Resets the CG recursion (beta = 0, no pending x).
+__global__ void __launch_bounds__(TB) true_residual(TorsoArgs a, int reset) {
+  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * TB) {
+    if (!is_row(a, g)) continue;
+    const int l = a.label[g];
+    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+    double diag = 0.0, off = 0.0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const double t = c_T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
+      diag += t;
+      off += t * a.x[nb[f]];   // x is 0 on air and at the pinned voxel
+    }
+    const double bb = (double)a.b[g];
+    const double rr = bb - (diag * a.x[g] - off);
+    const float rf = (float)rr;
+    if (reset) a.r[g] = rf;
+    acc[0] += rr * rr;
+    acc[1] += bb * bb;
+    acc[2] += (double)rf * ((double)a.invd[g] * rf);
+  }
+  double tot[3];
+  if (block_reduce_last<3>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+    a.scal[SC_TRUE_RR] = tot[0];
+    a.scal[SC_BB] = tot[1];
+    if (reset) {
+      a.scal[SC_RZ] = tot[2];
+      a.scal[SC_BETA] = 0.0;
+      a.scal[SC_ALPHA_PREV] = 0.0;
+      a.iscal[IS_DONE] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- sources
+
+struct SrcArgs {
+  int32_t n_heart;
+  const int32_t* nbr;      // n_heart x 6
+  const int32_t* proj;     // n_heart (coarse row or -1)
+  const float* vm;         // n_heart, mV
+  float* iv;               // n_heart: (sigma_i/h^2) K Vm (V) on projected voxels
+  double coeff;
+  double* part;
+  unsigned int* ticket;
+  double* scal;
+  int64_t* mean_count;     // [1] number of projected voxels
+};
+
+// iv_i = coeff * sum_n (V_n - V_i) with V = Vm * 1e-3 (compute_bspm.py:381-387)
+__global__ void __launch_bounds__(TB) src_laplacian(SrcArgs s) {
+  double acc[1] = {0.0};
+  for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < s.n_heart;
+       i += (int64_t)gridDim.x * TB) {
+    if (s.proj[i] < 0) continue;
+    const float vi = s.vm[i] * 1e-3f;
+    float lap = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int32_t n = s.nbr[i * 6 + f];
+      if (n >= 0) lap += s.vm[n] * 1e-3f - vi;
+    }
+    const float iv = lap * (float)s.coeff;
+    s.iv[i] = iv;
+    acc[0] += (double)iv;
+  }
+  double tot[1];
+  if (block_reduce_last<1>(acc, false, s.part, s.ticket, tot) && threadIdx.x == 0)
+    s.scal[SC_SRC_MEAN] = tot[0] / (double)fmax(1.0, (double)*s.mean_count);
+}
+
+// b[row] = (sum of iv over the heart voxels of row - count * mean) / n_expected,
+// one thread per receiving row (rows listed in seg order, deterministic).
+__global__ void __launch_bounds__(TB) src_scatter(const float* iv, const int32_t* seg_ptr,
+                                                  const int32_t* seg_vox, const int64_t* seg_grid,
+                                                  int32_t n_seg, const double* scal,
+                                                  double inv_nexp, float* b, int64_t pin) {
+  const int q = blockIdx.x * TB + threadIdx.x;
+  if (q >= n_seg) return;
+  const float mean = (float)scal[SC_SRC_MEAN];
+  float s = 0.0f;
+  for (int t = seg_ptr[q]; t < seg_ptr[q + 1]; ++t) s += iv[seg_vox[t]] - mean;
+  const int64_t g = seg_grid[q];
+  b[g] = g == pin ? 0.0f : (float)(s * inv_nexp);
+}
+
+__global__ void gather_out(const double* x, const int64_t* grid_of_read, int32_t n, float* out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) out[q] = (float)(x[grid_of_read[q]] * 1e3);
+}
+
+__global__ void gather_rows(const double* x, const int64_t* grid_of_row, int64_t n, double* out) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < n) out[q] = x[grid_of_row[q]];
+}
+
+__global__ void gather_rows_f(const float* b, const int64_t* grid_of_row, int64_t n, float* out) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < n) out[q] = b[grid_of_row[q]];
+}
+
+}  // namespace hp
+
+using namespace hp;
+
+struct HpTorso {
+  TorsoArgs a;
+  SrcArgs s;
+  int nblk;
+  int ni, nj, nk;
+  int64_t n_rows;
+  std::vector<void*> allocs;
+  int32_t n_read;
+  int64_t* grid_of_read;
+  int64_t* grid_of_row;
+  int32_t* seg_ptr;
+  int32_t* seg_vox;
+  int64_t* seg_grid;
+  int32_t n_seg;
+  double inv_nexp;
+  float* vm_dev;
+  float* out_dev;
+  double* h_scal;   // pinned host mirrors
+  int32_t* h_iscal;
+  int parity;
+  bool have_x;
+  cudaGraphExec_t graph[2];
+  int graph_chunk;
+  cudaStream_t graph_stream;
+};
+
+template <typename T>
+static hp_status tup(HpTorso* h, T** dst, const T* src, size_t n, cudaStream_t s) {
+  hp_status st = dev_upload(dst, src, n, s);
+  if (st == HP_OK && *dst) h->allocs.push_back((void*)*dst);
+  return st;
+}
+template <typename T>
+static hp_status tal(HpTorso* h, T** dst, size_t n) {
+  hp_status st = dev_alloc(dst, n);
+  if (st == HP_OK && *dst) h->allocs.push_back((void*)*dst);
+  return st;
+}
+
+#define TT_TRY(x)                \
+  do {                           \
+    hp_status _s = (x);          \
+    if (_s != HP_OK) {           \
+      hp_torso_destroy(h);       \
+      return _s;                 \
+    }                            \
+  } while (0)
+
+extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* stream) {
+  HP_REQUIRE(d && out, "hp_torso_create: null argument");
+  *out = nullptr;
+  HP_REQUIRE(d->ni > 0 && d->nj > 0 && d->nk > 0 && d->label, "hp_torso_create: empty grid");
+  HP_REQUIRE(d->n_materials >= 1 && d->n_materials <= HP_MAX_MATERIALS && d->sigma,
+             "hp_torso_create: n_materials must be 1..%d", HP_MAX_MATERIALS);
+  HP_REQUIRE(d->h_m > 0.0, "hp_torso_create: h_m must be positive");
+  HP_REQUIRE(d->n_heart >= 0 && (d->n_heart == 0 || (d->heart_nbr && d->proj)),
+             "hp_torso_create: missing heart arrays");
+  HP_REQUIRE(d->n_read >= 0 && (d->n_read == 0 || d->read_rows), "hp_torso_create: missing read_rows");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ni = d->ni, nj = d->nj, nk = d->nk;
+  const int PI = ni + 2, PJ = nj + 2, PK = nk + 2;
+  const int64_t ng = (int64_t)PI * PJ * PK;
+  // padded labels, row <-> grid maps (rows in flat active order)
+  std::vector<uint8_t> lab(ng, 0);
+  std::vector<int64_t> grid_of_row;
+  grid_of_row.reserve((size_t)ni * nj * nk);
+  for (int i = 0; i < ni; ++i)
+    for (int j = 0; j < nj; ++j)
+      for (int k = 0; k < nk; ++k) {
+        const uint8_t l = d->label[((int64_t)i * nj + j) * nk + k];
+        if (l >= d->n_materials) {
+          hp::set_error("hp_torso_create: label %d at (%d,%d,%d) >= n_materials", l, i, j, k);
+          return HP_ERR_INVALID;
+        }
+        const int64_t g = ((int64_t)(i + 1) * PJ + (j + 1)) * PK + (k + 1);
+        lab[g] = l;
+        if (l != 0) grid_of_row.push_back(g);
+      }
+  const int64_t n_rows = (int64_t)grid_of_row.size();
+  HP_REQUIRE(d->pin_row >= 0 && d->pin_row < n_rows, "hp_torso_create: pin_row out of range");
+  for (int m = 0; m < d->n_read; ++m)
+    HP_REQUIRE(d->read_rows[m] >= 0 && d->read_rows[m] < n_rows,
+               "hp_torso_create: read_rows[%d] out of range", m);
+  // conductance tables (harmonic mean / h^2; both-zero pairs -> 0)
+  float T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS] = {0};
+  double T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS] = {0};
+  const double h2 = d->h_m * d->h_m;
+  for (int u = 0; u < d->n_materials; ++u)
+    for (int v = 0; v < d->n_materials; ++v) {
+      const double su = d->sigma[u], sv = d->sigma[v];
+      if (u == 0 || v == 0 || su + sv < 1e-30) continue;   // air never couples
+      const double g = (2.0 * su * sv) / (su + sv) / h2;
+      T64[u * HP_MAX_MATERIALS + v] = g;
+      T32[u * HP_MAX_MATERIALS + v] = (float)g;
+    }
+  // Jacobi inverse diagonal (FP32 of the FP64 diagonal), 0 on the pin
+  const int64_t SJ = PK, SI = (int64_t)PJ * PK;
+  std::vector<float> invd(ng, 0.0f);
+  const int64_t pin_g = grid_of_row[d->pin_row];
+  for (int64_t r = 0; r < n_rows; ++r) {
+    const int64_t g = grid_of_row[r];
+    if (g == pin_g) continue;
+    const int l = lab[g];
+    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+    double dg = 0.0;
+    for (int f = 0; f < 6; ++f) dg += T64[l * HP_MAX_MATERIALS + lab[nb[f]]];
+    invd[g] = dg > 1e-30 ? (float)(1.0 / dg) : 1.0f;
+  }
+  HpTorso* h = new HpTorso();
+  memset(&h->a, 0, sizeof(h->a));
+  memset(&h->s, 0, sizeof(h->s));
+  h->graph[0] = h->graph[1] = nullptr;
+  h->graph_chunk = 0;
+  h->graph_stream = nullptr;
+  h->ni = ni; h->nj = nj; h->nk = nk;
+  h->n_rows = n_rows;
+  h->parity = 0;
+  h->have_x = false;
+  HP_CUDA_TRY(cudaMemcpyToSymbolAsync(c_T32, T32, sizeof(T32), 0, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyToSymbolAsync(c_T64, T64, sizeof(T64), 0, cudaMemcpyHostToDevice, s));
+  TorsoArgs& a = h->a;
+  a.ng = ng; a.pj = PJ; a.pk = PK; a.pin = pin_g; a.n_rows = n_rows;
+  TT_TRY(tup(h, (uint8_t**)&a.label, lab.data(), ng, s));
+  TT_TRY(tup(h, (float**)&a.invd, invd.data(), ng, s));
+  TT_TRY(tal(h, &a.r, ng));
+  TT_TRY(tal(h, &a.p0, ng));
+  TT_TRY(tal(h, &a.p1, ng));
+  TT_TRY(tal(h, &a.Ap, ng));
+  TT_TRY(tal(h, &a.x, ng));
+  TT_TRY(tal(h, &a.b, ng));
+  HP_CUDA_TRY(cudaMemsetAsync(a.r, 0, ng * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.p0, 0, ng * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.p1, 0, ng * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.Ap, 0, ng * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, ng * 8, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.b, 0, ng * 4, s));
+  int nsm = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  h->nblk = nsm * 8;
+  TT_TRY(tal(h, &a.scal, N_SCAL));
+  TT_TRY(tal(h, &a.iscal, N_ISCAL));
+  TT_TRY(tal(h, &a.part, (size_t)h->nblk * NPART));
+  TT_TRY(tal(h, &a.ticket, 1));
+  HP_CUDA_TRY(cudaMemsetAsync(a.scal, 0, N_SCAL * 8, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.iscal, 0, N_ISCAL * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.ticket, 0, 4, s));
+  TT_TRY(tup(h, &h->grid_of_row, grid_of_row.data(), n_rows, s));
+  // heart sources: segments of heart voxels per receiving row
+  SrcArgs& sa = h->s;
+  sa.n_heart = d->n_heart;
+  sa.coeff = d->coeff;
+  sa.part = a.part;
+  sa.ticket = a.ticket;
+  sa.scal = a.scal;
+  h->inv_nexp = 1.0 / d->n_expected;
+  std::vector<int32_t> order;
+  int64_t n_valid = 0;
+  for (int32_t i = 0; i < d->n_heart; ++i) {
+    if (d->proj[i] >= n_rows) {
+      hp::set_error("hp_torso_create: proj[%d]=%d out of range", i, d->proj[i]);
+      hp_torso_destroy(h);
+      return HP_ERR_INVALID;
+    }
+    for (int f = 0; f < 6; ++f) {
+      const int32_t nbv = d->heart_nbr[(int64_t)i * 6 + f];
+      if (nbv >= d->n_heart) {
+        hp::set_error("hp_torso_create: heart_nbr out of range at %d", i);
+        hp_torso_destroy(h);
+        return HP_ERR_INVALID;
+      }
+    }
+    if (d->proj[i] >= 0) { order.push_back(i); ++n_valid; }
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t u, int32_t v) { return d->proj[u] < d->proj[v]; });
+  std::vector<int32_t> seg_ptr(1, 0), seg_vox;
+  std::vector<int64_t> seg_grid;
+  for (size_t t = 0; t < order.size(); ++t) {
+    if (t > 0 && d->proj[order[t]] != d->proj[order[t - 1]]) {
+      seg_ptr.push_back((int32_t)t);
+    }
+    if (t == 0 || d->proj[order[t]] != d->proj[order[t - 1]])
+      seg_grid.push_back(grid_of_row[d->proj[order[t]]]);
+    seg_vox.push_back(order[t]);
+  }
+  seg_ptr.push_back((int32_t)order.size());
+  if (order.empty()) seg_ptr.assign(1, 0);
+  h->n_seg = (int32_t)seg_grid.size();
+  TT_TRY(tup(h, &h->seg_ptr, seg_ptr.data(), seg_ptr.size(), s));
+  TT_TRY(tup(h, &h->seg_vox, seg_vox.data(), seg_vox.size(), s));
+  TT_TRY(tup(h, &h->seg_grid, seg_grid.data(), seg_grid.size(), s));
+  TT_TRY(tup(h, (int32_t**)&sa.nbr, d->heart_nbr, (size_t)d->n_heart * 6, s));
+  TT_TRY(tup(h, (int32_t**)&sa.proj, d->proj, d->n_heart, s));
+  TT_TRY(tal(h, &h->vm_dev, d->n_heart));
+  TT_TRY(tal(h, &sa.iv, d->n_heart));
+  if (d->n_heart) HP_CUDA_TRY(cudaMemsetAsync(sa.iv, 0, d->n_heart * 4, s));
+  TT_TRY(tup(h, &sa.mean_count, &n_valid, 1, s));
+  sa.vm = h->vm_dev;
+  // read-out rows
+  h->n_read = d->n_read;
+  std::vector<int64_t> gr(d->n_read);
+  for (int m = 0; m < d->n_read; ++m) gr[m] = grid_of_row[d->read_rows[m]];
+  TT_TRY(tup(h, &h->grid_of_read, gr.data(), gr.size(), s));
+  TT_TRY(tal(h, &h->out_dev, d->n_read));
+  HP_CUDA_TRY(cudaMallocHost((void**)&h->h_scal, N_SCAL * sizeof(double)));
+  HP_CUDA_TRY(cudaMallocHost((void**)&h->h_iscal, N_ISCAL * sizeof(int32_t)));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  *out = h;
+  return HP_OK;
+}
+
+extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; }
+
+static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
+  for (int q = 0; q < n; ++q) {
+    pcg_k1<<<h->nblk, TB, 0, s>>>(h->a, h->parity);
+    pcg_k2<<<h->nblk, TB, 0, s>>>(h->a);
+    h->parity ^= 1;
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// CG iterations in chunks of `chunk` (a CUDA graph per parity), with the
+// host reading the done flag once per chunk.  Kernels after convergence
+// inside a chunk return immediately.
+static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
+  const int chunk = 8;   // even, so the p-buffer parity is the same after every chunk
+  if (s == nullptr) {    // the legacy default stream cannot be captured
+    for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
+      hp_status st = iter_launch(h, chunk, s);
+      if (st != HP_OK) return st;
+      HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
+      HP_CUDA_TRY(cudaStreamSynchronize(s));
+      if (h->h_iscal[IS_DONE]) break;
+    }
+    return HP_OK;
+  }
+  if (!h->graph[0] || h->graph_stream != s) {
+    for (int par = 0; par < 2; ++par) {
+      if (h->graph[par]) cudaGraphExecDestroy(h->graph[par]);
+      h->graph[par] = nullptr;
+      const int save = h->parity;
+      h->parity = par;
+      cudaGraph_t g;
+      HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      hp_status st = iter_launch(h, chunk, s);
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      h->parity = save;
+      if (st != HP_OK) return st;
+      HP_CUDA_TRY(ce);
+      HP_CUDA_TRY(cudaGraphInstantiate(&h->graph[par], g, 0));
+      cudaGraphDestroy(g);
+    }
+    h->graph_chunk = chunk;
+    h->graph_stream = s;
+  }
+  for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
+    HP_CUDA_TRY(cudaGraphLaunch(h->graph[h->parity], s));
+    HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h->h_iscal[IS_DONE]) break;
+  }
+  return HP_OK;
+}
+
+extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t vm_on_device,
+                                          float* out, int32_t out_on_device, double tol,
+                                          int32_t rule, int32_t max_iter, HpSolveStats* stats,
+                                          void* stream) {
+  HP_REQUIRE(h, "hp_torso_solve_frame: null handle");
+  HP_REQUIRE(rule >= 0 && rule <= 2, "hp_torso_solve_frame: unknown rule %d", rule);
+  HP_REQUIRE(max_iter >= 1, "hp_torso_solve_frame: max_iter must be >= 1");
+  HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame: tol must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  TorsoArgs& a = h->a;
+  SrcArgs& sa = h->s;
+  // 1. sources -> b
+  if (sa.n_heart > 0) {
+    HP_REQUIRE(vm, "hp_torso_solve_frame: vm is null");
+    HP_CUDA_TRY(cudaMemcpyAsync(h->vm_dev, vm, (size_t)sa.n_heart * 4,
+                                vm_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(a.b, 0, a.ng * 4, s));
+  if (sa.n_heart > 0) {
+    src_laplacian<<<h->nblk, TB, 0, s>>>(sa);
+    if (h->n_seg > 0)
+      src_scatter<<<(h->n_seg + TB - 1) / TB, TB, 0, s>>>(sa.iv, h->seg_ptr, h->seg_vox,
+                                                           h->seg_grid, h->n_seg, a.scal,
+                                                           h->inv_nexp, a.b, a.pin);
+  }
+  // 2. scalars: rule, tolerance (stat units: volts for RMS/LINF), limits
+  double tol_dev = rule == HP_STOP_REL ? tol : tol * 1e-3;   // mV -> V for the mV rules
+  HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol_dev, 8, cudaMemcpyHostToDevice, s));
+  int32_t is_init[N_ISCAL] = {0, 0, rule, max_iter, 0, 0};
+  HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_init, sizeof(is_init), cudaMemcpyHostToDevice, s));
+  // 3. r = b - A x0 (warm start; x = 0 for the first frame), beta = 0
+  true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+  HP_CUDA_TRY(cudaGetLastError());
+  int restarts = 0;
+  int total_it = 0;
+  hp_status result = HP_OK;
+  double rel = 0.0;
+  for (;;) {
+    HP_CUDA_TRY(cudaMemcpyAsync(h->h_scal, a.scal, N_SCAL * 8, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    const double bb = h->h_scal[SC_BB];
+    rel = bb > 0.0 ? sqrt(h->h_scal[SC_TRUE_RR] / bb) : 0.0;
+    if (bb == 0.0 && rule == HP_STOP_REL) {   // zero source: the pinned solution is 0
+      HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, a.ng * 8, s));
+      rel = 0.0;
+      break;
+    }
+    if (rule == HP_STOP_REL && rel <= tol) break;
+    if (total_it >= max_iter) { result = HP_ERR_NOT_CONVERGED; break; }
+    // iterate
+    int32_t is_run[N_ISCAL] = {0, 0, rule, max_iter - total_it, 0, 0};
+    HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_run, sizeof(is_run), cudaMemcpyHostToDevice, s));
+    const int par0 = h->parity;
+    hp_status st = run_iterations(h, max_iter - total_it, s);
+    if (st != HP_OK) return st;
+    HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(h->h_scal, a.scal, N_SCAL * 8, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    const int its = h->h_iscal[IS_ITER];
+    total_it += its;
+    // p of the last iteration lives in buffer (par0 ^ its) ^ ... : iteration q
+    // (0-based) reads parity par0^(q&1) and writes the other one
+    const int last_out = (par0 ^ ((its - 1) & 1)) ^ 1;
+    h->parity = (par0 ^ (its & 1));
+    if (its > 0) {
+      pcg_finish_x<<<h->nblk, TB, 0, s>>>(a, last_out);
+      HP_CUDA_TRY(cudaGetLastError());
+    }
+    if (h->h_iscal[IS_NONFINITE]) { result = HP_ERR_NONFINITE; break; }
+    if (rule != HP_STOP_REL) {
+      // reference mV rules: the recursive statistic decides
+      true_residual<<<h->nblk, TB, 0, s>>>(a, 0);
+      HP_CUDA_TRY(cudaMemcpyAsync(h->h_scal, a.scal, N_SCAL * 8, cudaMemcpyDeviceToHost, s));
+      HP_CUDA_TRY(cudaStreamSynchronize(s));
+      rel = h->h_scal[SC_BB] > 0 ? sqrt(h->h_scal[SC_TRUE_RR] / h->h_scal[SC_BB]) : 0.0;
+      if (!(h->h_scal[SC_STAT] < tol_dev)) result = HP_ERR_NOT_CONVERGED;
+      if (h->h_iscal[IS_BREAKDOWN]) result = HP_OK;   // reference: break, return x
+      break;
+    }
+    if (h->h_iscal[IS_BREAKDOWN] && total_it < max_iter) {
+      // Krylov breakdown: restart from the true residual
+      ++restarts;
+    }
+    // relative rule: true residual decides; replace r and restart if needed
+    true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+    HP_CUDA_TRY(cudaGetLastError());
+    ++restarts;
+    if (restarts > 50) { result = HP_ERR_STAGNATED; break; }
+  }
+  if (rule == HP_STOP_REL && restarts > 0) --restarts;   // the final check is not a restart
+  // read-out
+  if (h->n_read > 0 && out) {
+    gather_out<<<(h->n_read + 255) / 256, 256, 0, s>>>(a.x, h->grid_of_read, h->n_read,
+                                                        out_on_device ? out : h->out_dev);
+    if (!out_on_device)
+      HP_CUDA_TRY(cudaMemcpyAsync(out, h->out_dev, h->n_read * 4, cudaMemcpyDeviceToHost, s));
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (stats) {
+    stats->iterations = total_it;
+    stats->status = result;
+    stats->rel_residual = rel;
+    stats->stat = h->h_scal[SC_STAT];
+    stats->restarts = restarts;
+  }
+  h->have_x = true;
+  if (result == HP_ERR_NOT_CONVERGED || result == HP_ERR_STAGNATED) return HP_OK;  // reported in stats
+  if (result != HP_OK) {
+    hp::set_error("hp_torso_solve_frame: non-finite values in the solve");
+    return result;
+  }
+  return HP_OK;
+}
+
+extern "C" hp_status hp_torso_copy_solution(HpTorso* h, double* x_rows, void* stream) {
+  HP_REQUIRE(h && x_rows, "hp_torso_copy_solution: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  double* tmp = nullptr;
+  HP_CUDA_TRY(cudaMalloc((void**)&tmp, h->n_rows * 8));
+  gather_rows<<<(unsigned)((h->n_rows + 255) / 256), 256, 0, s>>>(h->a.x, h->grid_of_row,
+                                                                  h->n_rows, tmp);
+  HP_CUDA_TRY(cudaMemcpyAsync(x_rows, tmp, h->n_rows * 8, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  HP_CUDA_TRY(cudaFree(tmp));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_torso_copy_rhs(HpTorso* h, float* b_rows, void* stream) {
+  HP_REQUIRE(h && b_rows, "hp_torso_copy_rhs: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  float* tmp = nullptr;
+  HP_CUDA_TRY(cudaMalloc((void**)&tmp, h->n_rows * 4));
+  gather_rows_f<<<(unsigned)((h->n_rows + 255) / 256), 256, 0, s>>>(h->a.b, h->grid_of_row,
+                                                                    h->n_rows, tmp);
+  HP_CUDA_TRY(cudaMemcpyAsync(b_rows, tmp, h->n_rows * 4, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  HP_CUDA_TRY(cudaFree(tmp));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_torso_reset(HpTorso* h) {
+  HP_REQUIRE(h, "hp_torso_reset: null handle");
+  HP_CUDA_TRY(cudaMemset(h->a.x, 0, h->a.ng * 8));
+  h->have_x = false;
+  return HP_OK;
+}
+
+extern "C" hp_status hp_torso_destroy(HpTorso* h) {
+  if (!h) return HP_OK;
+  for (int q = 0; q < 2; ++q)
+    if (h->graph[q]) cudaGraphExecDestroy(h->graph[q]);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->h_scal) cudaFreeHost(h->h_scal);
+  if (h->h_iscal) cudaFreeHost(h->h_iscal);
+  delete h;
+  return HP_OK;
+}

@@ -195,7 +195,11 @@ class MonoHandle:
         d.deact_threshold = float(prob.deact_threshold)
         d.max_events = int(prob.max_events)
         self._desc = d
-        self.stream = stream if stream is not None else _lib.current_stream()
+        if stream is None:
+            # a dedicated stream: CUDA graphs cannot capture the legacy stream
+            self._torch_stream = torch.cuda.Stream()
+            stream = C.c_void_p(self._torch_stream.cuda_stream)
+        self.stream = stream
         h = C.c_void_p()
         _lib.check(L.hp_mono_create(C.byref(d), C.byref(h), self.stream), "hp_mono_create")
         self.h = h
@@ -264,8 +268,7 @@ class MonoHandle:
 
     def sync(self):
         import torch
-        torch.cuda.current_stream().synchronize() if self.stream is None else \
-            torch.cuda.synchronize()
+        torch.cuda.synchronize()
 
     def close(self):
         if getattr(self, "h", None):

@@ -168,6 +168,81 @@ hp_status hp_mono_copy_v(HpMono *h, float *v_myo, float *v_pk, void *stream);
 hp_status hp_mono_copy_state(HpMono *h, float *state_slots, float *state_pk, void *stream);
 hp_status hp_mono_destroy(HpMono *h);
 
+/* ------------------------------------------------------------------ */
+/* Torso forward solve (per-frame Poisson, Jacobi-PCG)                 */
+/* ------------------------------------------------------------------ */
+
+#define HP_MAX_MATERIALS 16
+
+/* Stopping rule of a frame solve. */
+typedef enum {
+  HP_STOP_REL = 0,   /* FP64 true residual ||b - A x|| / ||b|| <= tol */
+  HP_STOP_RMS = 1,   /* sqrt(mean(z^2)) < tol (z = M^-1 r, volts), reference 'rms' */
+  HP_STOP_LINF = 2   /* max |z| < tol, reference 'linf' */
+} hp_stop_rule;
+
+/*
+ * Torso grid and heart source geometry.  HOST pointers, copied at create.
+ *
+ * The torso is a dense grid ni x nj x nk (k fastest) of material labels;
+ * conductivity sigma[label] in S/m (label 0 = air, sigma 0).  A voxel is an
+ * unknown when its label is not 0 ("active"); rows are numbered in flat
+ * (i, j, k) order of the active voxels, as the reference's active_ids.  Face
+ * conductance = harmonic mean of the two sigmas / h^2, air faces Neumann.
+ * pin_row is fixed to 0 (reference potential).
+ *
+ * Heart: n_heart fine voxels with their 6 face neighbours (heart_nbr,
+ * n_heart x 6, -1 = none) for the source Laplacian, and the coarse row each
+ * voxel projects to (proj, -1 = outside the torso).  Per frame:
+ *   src_i = coeff * (K Vm * 1e-3)_i - mean over projected voxels,
+ *   b_row = sum_{i -> row} src_i / n_expected,  b[pin_row] = 0.
+ */
+typedef struct {
+  int32_t ni, nj, nk;
+  double h_m;                   /* torso voxel size, metres */
+  const uint8_t *label;         /* ni * nj * nk */
+  int32_t n_materials;
+  const double *sigma;          /* n_materials, S/m */
+  int64_t pin_row;              /* row index of the pinned node */
+  int32_t n_heart;
+  const int32_t *heart_nbr;     /* n_heart x 6 */
+  const int32_t *proj;          /* n_heart, coarse row or -1 */
+  double coeff;                 /* sigma_i / h_fine^2 */
+  double n_expected;            /* fine voxels per coarse voxel */
+  int32_t n_read;               /* read-out rows (surface nodes, electrodes) */
+  const int64_t *read_rows;     /* n_read */
+} HpTorsoDesc;
+
+typedef struct {
+  int32_t iterations;           /* CG iterations of the last frame */
+  int32_t status;               /* hp_status of the last frame */
+  double rel_residual;          /* FP64 true ||b - A x|| / ||b|| at exit */
+  double stat;                  /* value of the chosen stopping statistic */
+  int32_t restarts;             /* residual replacements */
+} HpSolveStats;
+
+typedef struct HpTorso HpTorso;
+
+hp_status hp_torso_create(const HpTorsoDesc *desc, HpTorso **out, void *stream);
+/* Number of active rows (unknowns). */
+int64_t hp_torso_rows(const HpTorso *h);
+/* Solves one frame: vm (n_heart floats, mV) is read from host or device
+ * memory (vm_on_device); warm start from the previous frame's solution
+ * (zero for the first).  Writes the read-out potentials (n_read floats, mV)
+ * to out (host or device, out_on_device).  tol/rule select the stopping
+ * rule; max_iter bounds the iterations. */
+hp_status hp_torso_solve_frame(HpTorso *h, const float *vm, int32_t vm_on_device, float *out,
+                               int32_t out_on_device, double tol, int32_t rule,
+                               int32_t max_iter, HpSolveStats *stats, void *stream);
+/* Copies the full potential field (rows, FP64 volts) of the last frame to
+ * host memory. */
+hp_status hp_torso_copy_solution(HpTorso *h, double *x_rows, void *stream);
+/* Copies the right-hand side (rows, FP32) of the last frame to host memory. */
+hp_status hp_torso_copy_rhs(HpTorso *h, float *b_rows, void *stream);
+/* Forgets the warm start (next frame starts from zero). */
+hp_status hp_torso_reset(HpTorso *h);
+hp_status hp_torso_destroy(HpTorso *h);
+
 #ifdef __cplusplus
 }
 #endif
