@@ -101,6 +101,8 @@ def _declare_optional(L):
     L.hp_torso_copy_rhs.argtypes = [P, P, P]
     L.hp_torso_reset.argtypes = [P]
     L.hp_torso_destroy.argtypes = [P]
+    L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_int32, C.c_int32, P, P]
 
 
 def check(status: int, what: str = ""):

@@ -1,0 +1,275 @@
+// tcgen05 3x3x3 convolution kernels (see tc_conv.cuh for the design) and
+// their C entry points.
+#include "hp_common.cuh"
+#include "tc_conv.cuh"
+
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace hp {
+namespace tc {
+
+enum Epi : int {
+  EPI_RELU = 0,     // y = relu(acc + bias)                 (bf16)
+  EPI_LINEAR = 1,   // y = acc + bias                        (bf16)
+  EPI_MASK = 2,     // y = acc * (mask > 0)                  (bf16)  ReLU backward
+  EPI_F32_C0 = 3    // y = acc[:, 0] + bias[0]               (fp32, one channel)
+};
+
+template <int CIN, int COUT>
+struct ConvCfg {
+  static constexpr int G = CIN / 8;
+  static constexpr int A_BYTES = G * CHUNK;
+  static constexpr int A_TX = G * LINE * 16;
+  static constexpr int B_BYTES = 3 * CIN * COUT * 2;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int SMEM = 2 * STAGE + 128;
+  static constexpr uint32_t COLS = TmemCols<COUT>::value;
+  static constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
+  static_assert(B_BYTES % 128 == 0, "stage alignment");
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128)
+conv3_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat16* __restrict__ Wp,
+                const float* __restrict__ bias, void* __restrict__ Yv,
+                const __nv_bfloat16* __restrict__ mask, int D, int H, int W, int epi, int* err) {
+  using C = ConvCfg<CIN, COUT>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ __align__(8) uint64_t empty[2];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int failed;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int w0 = blockIdx.x * TILE_M, h = blockIdx.y, d = blockIdx.z;
+
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(&done, 1);
+    failed = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(&tmem_base, C::COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+
+  if (tid == 0) {
+    auto issue = [&](int s, int buf) {
+      const int dz = s / 3 - 1, dy = s % 3 - 1;
+      uint8_t* A = smem + buf * C::STAGE;
+      uint8_t* B = A + C::A_BYTES;
+      mbar_expect_tx(&full[buf], C::A_TX + C::B_BYTES);
+#pragma unroll
+      for (int g = 0; g < C::G; ++g)
+        tma_load_4d(A + g * CHUNK, &tmX, g * 8, w0 - 1, h + dy, d + dz, &full[buf]);
+      const int tap0 = 9 * (dz + 1) + 3 * (dy + 1);
+      bulk_load(B, Wp + (size_t)tap0 * CIN * COUT, C::B_BYTES, &full[buf]);
+    };
+    int issued = 0;
+    issue(0, 0);
+    issue(1, 1);
+    issued = 2;
+    int consumed = 0;
+    for (int s = 0; s < 9; ++s) {
+      const int buf = s & 1;
+      const uint32_t par = (s >> 1) & 1;
+      if (!mbar_wait(&full[buf], par)) {
+        atomicOr(err, 1);
+        failed = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(smem + buf * C::STAGE);
+      const uint32_t b0 = a0 + C::A_BYTES;
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+        for (int k = 0; k < CIN / 16; ++k) {
+          const uint64_t ad = smem_desc(a0 + 2 * k * CHUNK + dx * 16, CHUNK, 128);
+          const uint64_t bd = smem_desc(b0 + (dx * C::G + 2 * k) * COUT * 16, COUT * 16, 128);
+          mma_bf16(tmem, ad, bd, C::IDESC, (s | dx | k) != 0);
+        }
+      }
+      mma_commit(&empty[buf]);
+      consumed = s + 1;
+      if (s + 2 < 9) {
+        if (!mbar_wait(&empty[buf], par)) {
+          atomicOr(err, 2);
+          failed = 1;
+          break;
+        }
+        issue(s + 2, buf);
+        ++issued;
+      }
+    }
+    if (failed) {
+      // let the copies already issued land before the CTA releases smem
+      for (int s = consumed; s < issued; ++s) (void)mbar_wait(&full[s & 1], (s >> 1) & 1);
+    }
+    mma_commit(&done);
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(&done, 0) && !failed;
+  if (!ok && tid == 0) atomicOr(err, 4);
+  tc_fence_after();
+  if (ok) {
+    // epilogue: this thread owns output voxel w0 + tid, TMEM lane tid
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const int64_t vox = ((int64_t)d * H + h) * W + w0 + tid;
+    if (epi == EPI_F32_C0) {
+      float v[16];
+      tmem_ld16(trow, v);
+      ((float*)Yv)[vox] = v[0] + bias[0];
+    } else {
+      __nv_bfloat16* Y = (__nv_bfloat16*)Yv;
+#pragma unroll
+      for (int c0 = 0; c0 < COUT; c0 += 16) {
+        float v[16];
+        tmem_ld16(trow + c0, v);
+        __align__(16) __nv_bfloat16 o[16];
+        if (epi == EPI_MASK) {
+          const uint4* mp = (const uint4*)(mask + vox * COUT + c0);
+          __align__(16) __nv_bfloat16 m[16];
+          *(uint4*)&m[0] = mp[0];
+          *(uint4*)&m[8] = mp[1];
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            o[q] = __float2bfloat16(__bfloat162float(m[q]) > 0.0f ? v[q] : 0.0f);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            float y = v[q] + bias[c0 + q];
+            if (epi == EPI_RELU) y = fmaxf(y, 0.0f);
+            o[q] = __float2bfloat16(y);
+          }
+        }
+        uint4* yp = (uint4*)(Y + vox * COUT + c0);
+        yp[0] = *(uint4*)&o[0];
+        yp[1] = *(uint4*)&o[8];
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, C::COLS);
+}
+
+// -------------------------------------------------------------------------
+// host side: tensor maps and dispatch
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static hp_status get_encode() {
+  static std::once_flag once;
+  static cudaError_t st = cudaSuccess;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    st = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (st == cudaSuccess && q == cudaDriverEntryPointSuccess) g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  });
+  if (!g_encode) {
+    hp::set_error("cuTensorMapEncodeTiled is not available");
+    return HP_ERR_CUDA;
+  }
+  return HP_OK;
+}
+
+// Tensor map over X[D][H][W][C] (bf16) with box (8 ch, 130 voxels, 1, 1).
+hp_status make_line_map(CUtensorMap* map, const void* X, int D, int H, int W, int Cch) {
+  hp_status s = get_encode();
+  if (s != HP_OK) return s;
+  if (((uintptr_t)X & 15) != 0) {
+    hp::set_error("conv input must be 16-byte aligned");
+    return HP_ERR_INVALID;
+  }
+  cuuint64_t dims[4] = {(cuuint64_t)Cch, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D};
+  cuuint64_t strides[3] = {(cuuint64_t)Cch * 2, (cuuint64_t)W * Cch * 2,
+                           (cuuint64_t)H * W * Cch * 2};
+  cuuint32_t box[4] = {8, (cuuint32_t)LINE, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)X, dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    hp::set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return HP_ERR_CUDA;
+  }
+  return HP_OK;
+}
+
+typedef void (*ConvFn)(CUtensorMap, const __nv_bfloat16*, const float*, void*,
+                       const __nv_bfloat16*, int, int, int, int, int*);
+
+struct ConvEntry {
+  int cin, cout, smem;
+  ConvFn fn;
+};
+
+#define HP_CONV(ci, co) {ci, co, ConvCfg<ci, co>::SMEM, conv3_tc_kernel<ci, co>}
+static const ConvEntry kConv[] = {
+    HP_CONV(16, 16), HP_CONV(16, 32), HP_CONV(32, 16), HP_CONV(32, 32), HP_CONV(32, 64),
+    HP_CONV(64, 32), HP_CONV(64, 64), HP_CONV(48, 16), HP_CONV(96, 32), HP_CONV(16, 48),
+    HP_CONV(32, 96),
+};
+#undef HP_CONV
+
+hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y,
+                       const void* mask, int D, int H, int W, int cin, int cout, int epi,
+                       int* err, cudaStream_t s) {
+  const ConvEntry* e = nullptr;
+  for (const auto& c : kConv)
+    if (c.cin == cin && c.cout == cout) e = &c;
+  if (!e) {
+    hp::set_error("conv %d->%d is not compiled", cin, cout);
+    return HP_ERR_UNSUPPORTED;
+  }
+  if (W % TILE_M != 0 || D < 1 || H < 1) {
+    hp::set_error("conv grid W=%d must be a multiple of %d", W, TILE_M);
+    return HP_ERR_INVALID;
+  }
+  if (((uintptr_t)Wp & 15) || ((uintptr_t)Y & 15) || (mask && ((uintptr_t)mask & 15))) {
+    hp::set_error("conv buffers must be 16-byte aligned");
+    return HP_ERR_INVALID;
+  }
+  CUtensorMap map;
+  hp_status st = make_line_map(&map, X, D, H, W, cin);
+  if (st != HP_OK) return st;
+  static bool attr_set[sizeof(kConv) / sizeof(kConv[0])] = {false};
+  const int idx = (int)(e - kConv);
+  if (!attr_set[idx]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute((const void*)e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     e->smem));
+    attr_set[idx] = true;
+  }
+  dim3 grid(W / TILE_M, H, D);
+  e->fn<<<grid, 128, e->smem, s>>>(map, (const __nv_bfloat16*)Wp, bias, Y,
+                                   (const __nv_bfloat16*)mask, D, H, W, epi, err);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+}  // namespace tc
+}  // namespace hp
+
+// Test / building-block entry point: one 3x3x3 convolution (zero padding 1).
+extern "C" hp_status hp_conv3_forward(const void* X, const void* Wp, const float* bias, void* Y,
+                                      const void* mask, int32_t D, int32_t H, int32_t W,
+                                      int32_t cin, int32_t cout, int32_t epi, int32_t* err,
+                                      void* stream) {
+  HP_REQUIRE(X && Wp && Y && err && (bias || epi == hp::tc::EPI_MASK),
+             "hp_conv3_forward: null argument");
+  HP_REQUIRE(epi >= 0 && epi <= 3, "hp_conv3_forward: bad epilogue %d", epi);
+  HP_REQUIRE(epi != hp::tc::EPI_MASK || mask, "hp_conv3_forward: mask epilogue needs mask");
+  return hp::tc::conv3_launch(X, Wp, bias, Y, mask, D, H, W, cin, cout, epi, err,
+                              (cudaStream_t)stream);
+}

@@ -316,3 +316,84 @@ def biv_shell_problem(seed=0, **kw_over):
                            vm_save_dt=None, save_every=None, **kwp)
     prob.frame_steps = 50
     return prob, info
+
+
+# --------------------------------------------------------------------------
+# torso (ECG forward problem)
+# --------------------------------------------------------------------------
+
+TORSO_SIGMA = {1: 0.2, 2: 0.05, 3: 0.7, 4: 0.2}   # bulk, lung, blood, heart (S/m)
+
+
+def torso_for_heart(geo, shape=(192, 160, 256), dx=1.5, heart_center_mm=None):
+    """Elliptic-cylinder torso with two ellipsoidal lungs and the heart of
+    `geo` (a biv_geometry dict) embedded by nearest sampling at the torso
+    voxel centres: myocardium -> label 4, LV/RV cavities -> blood (label 3).
+
+    Heart node coordinates follow the solver convention (x, y, z) = (col,
+    row, depth) * h; the registration {R = I, scale = 1, t} maps them to
+    torso millimetres with the torso's own (axis0, axis1, axis2) order.
+    Returns (labels int32, sigma_map, registration dict)."""
+    ni, nj, nk = shape
+    L0, L1, L2 = ni * dx, nj * dx, nk * dx
+    c = ((np.arange(ni) + 0.5) * dx, (np.arange(nj) + 0.5) * dx, (np.arange(nk) + 0.5) * dx)
+    A, B, Cz = np.meshgrid(*c, indexing="ij")
+    lab = np.zeros(shape, np.int32)
+    body = ((A - L0 / 2) / (0.49 * L0)) ** 2 + ((B - L1 / 2) / (0.49 * L1)) ** 2 <= 1.0
+    body &= (Cz > 2 * dx) & (Cz < L2 - 2 * dx)
+    lab[body] = 1
+    for s in (-1.0, 1.0):
+        lung = (((A - L0 / 2 - s * 0.27 * L0) / (0.17 * L0)) ** 2 +
+                ((B - L1 / 2 - 0.03 * L1) / (0.3 * L1)) ** 2 +
+                ((Cz - 0.6 * L2) / (0.28 * L2)) ** 2) <= 1.0
+        lab[lung & body] = 2
+    h = geo["h"]
+    n = geo["n"]
+    if heart_center_mm is None:
+        heart_center_mm = np.array([L0 / 2 + 0.06 * L0, L1 / 2 - 0.12 * L1, 0.6 * L2])
+    t = np.asarray(heart_center_mm, np.float64) - 0.5 * n * h
+    # torso voxel centre -> heart (x, y, z) -> heart array (row=y, col=x, depth=z)
+    x = A - t[0]; y = B - t[1]; z = Cz - t[2]
+    hi = np.floor(y / h).astype(np.int64)
+    hj = np.floor(x / h).astype(np.int64)
+    hk = np.floor(z / h).astype(np.int64)
+    inside = (hi >= 0) & (hi < n) & (hj >= 0) & (hj < n) & (hk >= 0) & (hk < n) & body
+    ii, jj, kk = hi[inside], hj[inside], hk[inside]
+    myo = geo["S"][ii, jj, kk] == 1
+    cav = geo["lv_cav"][ii, jj, kk] | geo["rv_cav"][ii, jj, kk]
+    sub = lab[inside]
+    sub[cav] = 3
+    sub[myo] = 4
+    lab[inside] = sub
+    reg = dict(R=np.eye(3), t=t, scale=1.0, dice=1.0)
+    return lab, dict(TORSO_SIGMA), reg
+
+
+def twelve_lead_electrodes(grid, reg, heart_n=256, heart_h=0.4):
+    """Approximate standard electrode sites on the torso surface (mm):
+    limb electrodes at the shoulders / lower flanks, V1-V6 on a chest arc at
+    heart level.  Order: RA, LA, RL, LL, V1..V6."""
+    surf = np.asarray(grid["surface_xyz"], np.float64)
+    lo, hi = surf.min(0), surf.max(0)
+    mid = 0.5 * (lo + hi)
+    zc = float(reg["t"][2] + 0.5 * heart_n * heart_h)
+    ext = hi - lo
+    front = lo[1]                         # anterior = low axis-1
+    pts = [(mid[0] - 0.4 * ext[0], mid[1], hi[2] - 0.12 * ext[2]),    # RA
+           (mid[0] + 0.4 * ext[0], mid[1], hi[2] - 0.12 * ext[2]),    # LA
+           (mid[0] - 0.4 * ext[0], mid[1], lo[2] + 0.12 * ext[2]),    # RL
+           (mid[0] + 0.4 * ext[0], mid[1], lo[2] + 0.12 * ext[2])]    # LL
+    for k, frac in enumerate((-0.08, 0.02, 0.1, 0.18, 0.28, 0.38)):  # V1..V6
+        pts.append((mid[0] + frac * ext[0], front + (0.05 + 0.12 * max(frac, 0)) * ext[1], zc))
+    return np.array(pts)
+
+
+def body_surface_grid(grid, reg, n=16, heart_n=256, heart_h=0.4):
+    """n x n electrode grid on the anterior torso surface around heart level."""
+    surf = np.asarray(grid["surface_xyz"], np.float64)
+    lo, hi = surf.min(0), surf.max(0)
+    zc = float(reg["t"][2] + 0.5 * heart_n * heart_h)
+    a = np.linspace(lo[0] + 0.15 * (hi[0] - lo[0]), hi[0] - 0.15 * (hi[0] - lo[0]), n)
+    z = np.linspace(zc - 0.2 * (hi[2] - lo[2]), zc + 0.2 * (hi[2] - lo[2]), n)
+    A, Z = np.meshgrid(a, z, indexing="ij")
+    return np.stack([A.ravel(), np.full(A.size, lo[1]), Z.ravel()], 1)

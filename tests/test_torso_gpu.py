@@ -1,0 +1,124 @@
+"""GPU torso solve against the FP64 oracle.
+
+Claims checked: the relative rule meets ||b - A x|| / ||b|| <= tol in FP64
+with the reference's own FP64 operator (evaluated here on the CPU); the
+potentials match the FP64 direct solve; per-lead ECG relative L2 <= 1e-3;
+the reference's absolute-mV rules stop where the FP64 restatement of
+_pcg_gpu stops."""
+import numpy as np
+import pytest
+
+from tests import torso_cases
+
+pytestmark = pytest.mark.gpu
+LEAD_TOL = 1e-3
+
+
+def _setup(case, electrodes=None):
+    from hrdayapy_b200.ecg import torso as T
+    from hrdayapy_b200.ecg.torso_grid import torso_grid_from_labels
+    lab, sigma_map, dx, vox, coords, reg, h, frames = case
+    grid = torso_grid_from_labels(lab, sigma_map, dx)
+    labels, table = T.labels_from_grid(grid)
+    proj, valid = T.projection_map(coords, reg["R"], reg["t"], 1.0, grid["origin_mm"], dx,
+                                   grid["active_id_map"], grid["shape"])
+    rows = np.arange(len(grid["active_ids"]))
+    solver = T.TorsoSolver(labels, table, dx, grid["pin_row"], T.heart_neighbours(vox), proj,
+                           0.2625, h, rows)
+    return solver, grid, proj, valid
+
+
+def _oracle(case, grid, proj, valid):
+    from oracle import torso as O
+    lab, sigma_map, dx, vox, coords, reg, h, frames = case
+    sig = grid["sigma_vol"]
+    A, flat, _ = O.assemble_stiffness(sig, dx * 1e-3, grid["active_mask"])
+    K = O.heart_laplacian(vox, len(vox))
+    return A, K, O.Solver(A, grid["pin_row"])
+
+
+@pytest.mark.parametrize("which", ["golden", "random"])
+def test_relative_rule_vs_fp64(golden, which):
+    from oracle import torso as O
+    case = (torso_cases.golden_case(golden("torso.npz")) if which == "golden"
+            else torso_cases.random_case())
+    frames = case[-1] if case[-1].ndim == 2 else case[-1][None]
+    solver, grid, proj, valid = _setup(case)
+    A, K, direct = _oracle(case, grid, proj, valid)
+    Ap = O.pinned(A, grid["pin_row"])
+    its = []
+    for f, vm in enumerate(frames):
+        out, st = solver.solve_frame(vm, 1e-6, "rel", 5000)
+        assert st.status == 0 and st.rel_residual <= 1e-6
+        x = solver.solution()
+        b = solver.rhs().astype(np.float64)
+        # the claim, re-evaluated on the CPU with the FP64 operator
+        rel = np.linalg.norm(b - Ap @ x) / np.linalg.norm(b)
+        assert rel <= 1.05e-6, rel
+        # potentials vs the FP64 direct solve of the FP64 right-hand side
+        bo = O.frame_rhs(K, vm, proj.astype(np.int64), valid, len(x), grid["pin_row"], 0.2625,
+                         case[6] * 1e-3, case[2])
+        xo = direct.solve(bo)
+        d = (x - x.mean()) - (xo - xo.mean())
+        assert np.linalg.norm(d) / np.linalg.norm(xo - xo.mean()) < 2e-5
+        np.testing.assert_allclose(out, (x * 1e3).astype(np.float32), rtol=1e-6, atol=1e-9)
+        its.append(st.iterations)
+    if len(its) > 1:
+        assert min(its[1:]) <= its[0]      # warm start helps
+
+
+def test_reference_mv_rules_match_fp64_pcg(golden):
+    from oracle import torso as O
+    case = torso_cases.golden_case(golden("torso.npz"))
+    solver, grid, proj, valid = _setup(case)
+    A, K, direct = _oracle(case, grid, proj, valid)
+    Ap = O.pinned(A, grid["pin_row"])
+    vm = case[-1]
+    for metric, tol in (("rms", 1e-3), ("linf", 1e-3)):
+        solver.reset()
+        out, st = solver.solve_frame(vm, tol, metric, 2000)
+        b = solver.rhs().astype(np.float64)
+        x_ref, it_ref, stat_ref = O.pcg_reference(Ap, b, None, tol_mV=tol, max_iter=2000,
+                                                  metric=metric)
+        assert st.status == 0 and st.stat * 1e3 < tol
+        assert abs(st.iterations - it_ref) <= max(2, 0.05 * it_ref), (st.iterations, it_ref)
+        x = solver.solution()
+        assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-3
+
+
+def test_zero_source_and_reset(golden):
+    case = torso_cases.golden_case(golden("torso.npz"))
+    solver, grid, proj, valid = _setup(case)
+    vm = np.full(len(case[3]), -85.0, np.float32)     # uniform Vm: no source
+    out, st = solver.solve_frame(vm, 1e-6, "rel", 100)
+    assert st.status == 0 and np.all(solver.solution() == 0.0)
+    out, st = solver.solve_frame(case[-1], 1e-6, "rel", 5000)
+    assert st.rel_residual <= 1e-6 and np.abs(out).max() > 0
+
+
+def test_leads_vs_oracle():
+    from hrdayapy_b200.ecg import torso as T
+    from oracle import torso as O
+    case = torso_cases.random_case(seed=3)
+    solver, grid, proj, valid = _setup(case)
+    A, K, direct = _oracle(case, grid, proj, valid)
+    surf = grid["surface_xyz"]
+    c = surf.mean(0)
+    ext = surf.max(0) - surf.min(0)
+    pts = [c + ext * np.array(o) for o in
+           [(-.5, -.3, .3), (.5, -.3, .3), (-.5, .3, -.4), (.5, .3, -.4), (-.1, -.5, 0),
+            (.05, -.5, 0), (.15, -.5, -.05), (.25, -.45, -.05), (.35, -.4, -.05), (.45, -.3, -.05)]]
+    el = T.nearest_surface_rows(pts, surf, grid["surface_rows"])
+    gpu, ora = [], []
+    for vm in case[-1]:
+        solver.solve_frame(vm, 1e-6, "rel", 5000)
+        x = solver.solution()
+        gpu.append(x[el] * 1e3)
+        bo = O.frame_rhs(K, vm, proj.astype(np.int64), valid, len(x), grid["pin_row"], 0.2625,
+                         case[6] * 1e-3, case[2])
+        ora.append(direct.solve(bo)[el] * 1e3)
+    Lg = T.twelve_lead(np.array(gpu).T)
+    Lo = T.twelve_lead(np.array(ora).T)
+    for k in range(12):
+        rel = np.linalg.norm(Lg[k] - Lo[k]) / max(np.linalg.norm(Lo[k]), 1e-12)
+        assert rel <= LEAD_TOL, (T.LEADS[k], rel)
