@@ -243,6 +243,25 @@ hp_status hp_torso_copy_rhs(HpTorso *h, float *b_rows, void *stream);
 hp_status hp_torso_reset(HpTorso *h);
 hp_status hp_torso_destroy(HpTorso *h);
 
+/* ------------------------------------------------------------------ */
+/* Learned preconditioner building block: tcgen05 3x3x3 convolution    */
+/* ------------------------------------------------------------------ */
+
+/*
+ * One 3x3x3 convolution with zero padding 1 on the 5th-generation tensor
+ * cores (no counterpart in the reference, which has no learned part).
+ * X: device bf16 [D][H][W][cin]; Wp: device bf16 weights packed
+ * [27][cin/8][cout][8] (tap = 9 kz + 3 ky + kx, see hrdayapy_b200/convref.py);
+ * bias: device fp32 [cout]; Y: device bf16 [D][H][W][cout], or fp32
+ * [D][H][W] for epi = 3.  epi: 0 relu(acc + bias), 1 acc + bias,
+ * 2 acc * (mask > 0) (mask: bf16 [D][H][W][cout]), 3 acc[:, 0] + bias[0].
+ * W must be a multiple of 128; cin / cout among the compiled pairs.
+ * *err (device int) receives nonzero if a bounded device wait expired.
+ */
+hp_status hp_conv3_forward(const void *X, const void *Wp, const float *bias, void *Y,
+                           const void *mask, int32_t D, int32_t H, int32_t W, int32_t cin,
+                           int32_t cout, int32_t epi, int32_t *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
