@@ -294,20 +294,22 @@ struct SrcArgs {
   int64_t* mean_count;     // [1] number of projected voxels
 };
 
-// iv_i = coeff * sum_n (V_n - V_i) with V = Vm * 1e-3 (compute_bspm.py:381-387)
+// iv_i = coeff * sum_n (V_n - V_i) with V = Vm * 1e-3 volts (compute_bspm.py:381-387)
 __global__ void __launch_bounds__(TB) src_laplacian(SrcArgs s) {
   double acc[1] = {0.0};
   for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < s.n_heart;
        i += (int64_t)gridDim.x * TB) {
     if (s.proj[i] < 0) continue;
-    const float vi = s.vm[i] * 1e-3f;
+    // differences of the mV values first (exact for equal neighbours), then
+    // one scaling by 1e-3 * sigma_i / h^2
+    const float vi = s.vm[i];
     float lap = 0.0f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const int32_t n = s.nbr[i * 6 + f];
-      if (n >= 0) lap += s.vm[n] * 1e-3f - vi;
+      if (n >= 0) lap += __fsub_rn(s.vm[n], vi);
     }
-    const float iv = lap * (float)s.coeff;
+    const float iv = lap * (float)(s.coeff * 1e-3);
     s.iv[i] = iv;
     acc[0] += (double)iv;
   }
