@@ -101,6 +101,8 @@ def _declare_optional(L):
     L.hp_torso_copy_rhs.argtypes = [P, P, P]
     L.hp_torso_reset.argtypes = [P]
     L.hp_torso_destroy.argtypes = [P]
+    L.hp_torso_residual_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32,
+                                            C.c_double, C.c_int64, P, P, P, P]
     L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, P, P]
 

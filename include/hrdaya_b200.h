@@ -243,6 +243,29 @@ hp_status hp_torso_copy_rhs(HpTorso *h, float *b_rows, void *stream);
 hp_status hp_torso_reset(HpTorso *h);
 hp_status hp_torso_destroy(HpTorso *h);
 
+/*
+ * Allocation-free FP64 true-residual check (no counterpart in the reference).
+ * For callers that may not allocate device memory (a host framework that
+ * owns every allocation, a real-time loop, a fixed memory budget): computes
+ * out[0] = ||b - A x|| and out[1] = ||b|| (host doubles) for the torso
+ * operator of hp_torso_create, with no cudaMalloc -- its only scratch is a
+ * fixed array inside the library (HP_NOALLOC_MAX_BLOCKS partials, 1.5 MB per
+ * GPU, held until exit).  label (uint8), x (fp64) and b (fp32) are device
+ * arrays over the PADDED grid (ni+2) x (nj+2) x (nk+2), k fastest, whose
+ * one-voxel border is air; pin_cell is the padded flat index of the pinned
+ * voxel (-1: none); sigma (host) holds n_materials conductivities in S/m
+ * (label 0 = air).  Padded grids above HP_NOALLOC_MAX_CELLS are rejected
+ * with HP_ERR_INVALID.  Every call shares the scratch array: calls that
+ * overlap on the GPU race.  The first call on a device resolves the array's
+ * address on that device, so make it before any stream capture.
+ */
+#define HP_NOALLOC_MAX_BLOCKS 65536
+#define HP_NOALLOC_MAX_CELLS (HP_NOALLOC_MAX_BLOCKS * 256LL)
+hp_status hp_torso_residual_noalloc(int32_t ni, int32_t nj, int32_t nk, const uint8_t *label,
+                                    const double *sigma, int32_t n_materials, double h_m,
+                                    int64_t pin_cell, const double *x, const float *b,
+                                    double *out, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Learned preconditioner building block: tcgen05 3x3x3 convolution    */
 /* ------------------------------------------------------------------ */
