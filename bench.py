@@ -48,59 +48,102 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle samples (every 100 ms) around the timed
+    region; summary() keeps the samples taken inside [mark_start, mark_end]
+    (or the nearest ones when the region is shorter than the period)."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index=0):
         self.index = index
-        self.samples = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}",
-                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        import tempfile
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.5)
         return self
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        time.sleep(0.3)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
 
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        import datetime as _dt
+        rows = []
+        try:
+            with open(self.out.name) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 8:
+                        continue
+                    try:
+                        ts = _dt.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                        rows.append((ts, float(parts[1]), float(parts[2]), parts[4:8]))
+                    except ValueError:
+                        continue
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        t0, t1 = self.t0 or rows[0][0], self.t1 or rows[-1][0]
+        inside = [r for r in rows if t0 - 0.05 <= r[0] <= t1 + 0.05]
+        if not inside:
+            mid = 0.5 * (t0 + t1)
+            inside = sorted(rows, key=lambda r: abs(r[0] - mid))[:2]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4)
-                          if len(s) > 3 + i and s[3 + i].lower().startswith("active")})
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+        reasons = sorted({names[i] for r in inside for i in range(4)
+                          if r[3][i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median([r[1] for r in inside])),
+                "sm_max_mhz": max(r[2] for r in inside), "reasons": reasons,
+                "samples": len(inside)}
 
 
 def build_workload(name, seed=0):
+    """Prepared problem of a workload.  With HP_BENCH_CACHE=<dir> the
+    prepared arrays are pickled there and reused by later runs of the same
+    workload (set-up only; nothing of the timed region is cached)."""
+    import pickle
     from hrdayapy_b200 import synthetic
+    cache = os.environ.get("HP_BENCH_CACHE")
+    path = Path(cache) / f"{name}_{seed}.pkl" if cache else None
+    if path is not None and path.exists():
+        with open(path, "rb") as f:
+            prob, info, last = pickle.load(f)
+        synthetic.last_inputs().clear()
+        synthetic.last_inputs().update(last)
+        return prob, info
     if name == "slab64":
-        return synthetic.slab_problem()
-    if name == "biv_shell":
-        return synthetic.biv_shell_problem(seed=seed)
-    raise SystemExit(f"unknown workload {name}")
+        out = synthetic.slab_problem()
+    elif name == "biv_shell":
+        out = synthetic.biv_shell_problem(seed=seed)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    if path is not None:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        with open(path, "wb") as f:
+            pickle.dump((out[0], out[1], dict(synthetic.last_inputs())), f, protocol=4)
+    return out
 
 
 def bytes_per_voxel_step(prob):
@@ -142,10 +185,12 @@ def run_ours(args):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
+            clk.mark_start()
             ev0.record(stream)
             sim.run(args.steps * fs, graph_chunk=fs)
             ev1.record(stream)
             ev1.synchronize()
+            clk.mark_end()
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
         vm_last = sim.voltage()[0]

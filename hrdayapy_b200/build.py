@@ -44,10 +44,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                     "-I", str(PKG.parent / "include"), "--expt-relaxed-constexpr"]
     if os.environ.get("HP_PRECISE_EXP", "0") != "1":
         flags += ["-DHP_FAST_EXP"]
+    # the TTP06 kinetics (mono.cu) use the approximate SFU divide / exp / log;
+    # every other unit keeps IEEE FP32 division and square root
+    fast = {"mono"}
     objs = []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc()] + flags + ["-c", str(src), "-o", str(obj)]
+        extra = ["--use_fast_math"] if src.stem in fast else []
+        cmd = [nvcc()] + flags + extra + ["-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
