@@ -201,8 +201,14 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
+// Blocks per SM the register budget is sized for (8 x 128 threads -> 64 regs).
+template <int BV>
+struct MinBlocks {
+  static constexpr int value = BV <= 128 ? 8 : (BV <= 256 ? 4 : 2);
+};
+
 template <int BI, int BJ, int BK, bool ANISO>
-__global__ void __launch_bounds__(BI * BJ * BK)
+__global__ void __launch_bounds__(BI * BJ * BK, MinBlocks<BI * BJ * BK>::value)
 mono_step_kernel(MonoArgs a, int step_off, int mode) {
   using G = TileGeom<BI, BJ, BK>;
   constexpr int BV = G::BV, SI = G::SI, SJ = G::SJ;
@@ -219,10 +225,24 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
   float* __restrict__ Wout = odd ? a.Vs0 : a.Vs1;
 
   __shared__ int nb27[27];
+  __shared__ int64_t s_vm_frame, s_anim_frame;
   __shared__ float tV[G::N];
   __shared__ float tW[ANISO ? 3 * G::N : 1];
   __shared__ float tD[ANISO ? 3 * G::N : 1];
   if (tid < 27) nb27[tid] = a.nbr[(int64_t)b * 27 + tid];
+  if (tid == 32) {
+    // per-step output decisions, once per block (64-bit modulo is costly)
+    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+  }
+  // issue this voxel's own loads first so their latency overlaps the halo
+  // loads and the stencil: tag, previous post-diffusion V, 18 TTP06 states
+  const int64_t slot = (int64_t)b * BV + tid;
+  const uint32_t tag = a.tag[slot];
+  const float Vprev = a.Vpost[slot];
+  CellState cs;
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * a.n_slots + slot];
   __syncthreads();
   if (mode == 0) {
     load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, -1, BK + 1>(tV, Win, nb27, tid);
@@ -238,8 +258,6 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
   }
   __syncthreads();
 
-  const int64_t slot = (int64_t)b * BV + tid;
-  const uint32_t tag = a.tag[slot];
   const int ph = tag & HP_TAG_PHENO_MASK;
   if (ph == 0) return;
 
@@ -302,7 +320,7 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
 
     // threshold crossings between the snapshots labelled t_{i-1} and t_i
     if (step >= 1) {
-      const float Vp = a.Vpost[slot];
+      const float Vp = Vprev;
       const bool was_act = Vp >= a.act_thr, is_act = Vn >= a.act_thr;
       const bool was_dea = Vp >= a.deact_thr, is_dea = Vn >= a.deact_thr;
       if ((!was_act && is_act) || (was_dea && !is_dea)) {
@@ -316,13 +334,12 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
       }
     }
     a.Vpost[slot] = Vn;
-    if (a.vm_every > 0 && step % a.vm_every == 0)
-      a.vm_snap[(step / a.vm_every) * a.n_myo + a.node_of_slot[slot]] = Vn;
-    if ((tag & HP_TAG_SURF) && a.frame_every > 0 && step % a.frame_every == 0)
-      a.surf_frames[(step / a.frame_every) * a.n_surf + a.surf_of_slot[slot]] = Vn;
+    if (s_vm_frame >= 0) a.vm_snap[s_vm_frame * a.n_myo + a.node_of_slot[slot]] = Vn;
+    if ((tag & HP_TAG_SURF) && s_anim_frame >= 0)
+      a.surf_frames[s_anim_frame * a.n_surf + a.surf_of_slot[slot]] = Vn;
     istep = step + 1;
   } else {
-    Vn = a.Vpost[slot];
+    Vn = Vprev;
     istep = 0;
     Wout = a.Vs0;
   }
@@ -330,9 +347,6 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
   // ionic half of step istep on V = Vn
   const int var = a.brick_variant ? a.brick_variant[b] : 0;
   const CellParams cp = pheno_params(ph, a.var_gks[var], a.var_gkr[var]);
-  CellState cs;
-#pragma unroll
-  for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * a.n_slots + slot];
   const float Iion = ttp06_step(Vn, cs, a.dt, cp);
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];

@@ -1,0 +1,837 @@
+// Learned preconditioner for the torso Poisson solve (no counterpart in the
+// reference, whose solver is Jacobi-PCG only).
+//
+//   M(r) = omega * D^-1 r  +  P( s * CNN( [R(D^-1 r) / s, geometry] ) )
+//
+// R restricts the fine torso grid (padded, see torso.cu) by 2 x 2 x 2
+// averaging onto the network grid (half resolution, NDHWC BF16, 16 input
+// channels: the Jacobi-scaled residual normalised by its RMS s, the active
+// fraction and the per-material fractions of each coarse cell); P is the
+// piecewise-constant prolongation back to the active fine cells.  The CNN is
+// a 3-level encoder-decoder with 16 / 32 / 64 channels, 3x3x3 convolutions
+// (tcgen05 implicit GEMM, BF16 operands, FP32 accumulation, csrc/conv.cu),
+// ReLU, 2 x 2 average pooling / nearest upsampling in (D, H) so every level
+// keeps the 128-voxel W lines the convolution tiles on, and skip
+// concatenation.  It is trained on the GPU by its own kernels: forward,
+// data gradients through the same tensor-core convolution with flipped and
+// transposed weights (ReLU masks fused in its epilogue), weight gradients on
+// the CUDA cores, and Adam on FP32 master weights.  Loss: squared error of
+// M(r) against the error e the plain solver's iterates leave, normalised by
+// ||e||^2.
+#include "hp_common.cuh"
+#include "tc_conv.cuh"
+
+#include <math.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace hp {
+namespace pc {
+
+enum Layer { E1A, E1B, E2A, E2B, E3A, E3B, D2A, D2B, D1A, D1B, OUT, NL };
+static const int LCIN[NL] = {16, 16, 16, 32, 32, 64, 96, 32, 48, 16, 16};
+static const int LCOUT[NL] = {16, 16, 32, 32, 64, 64, 32, 32, 16, 16, 1};
+static const int LLEV[NL] = {1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 1};
+
+__host__ __device__ inline int padc(int c) { return c < 16 ? 16 : c; }
+
+constexpr int TB = 256;
+
+struct Dims {
+  int D, H, W;            // network level dims
+  int64_t n() const { return (int64_t)D * H * W; }
+};
+
+// ------------------------------------------------------------------ kernels
+
+// Packs FP32 master weights w[co][ci][27] into the forward operand
+// [27][ci/8][coP][8] and the data-gradient operand [27][coP/8][ci][8]
+// (spatially flipped, channels transposed); padded channels are zero.
+__global__ void pack_kernel(const float* __restrict__ w, int cin, int cout,
+                            __nv_bfloat16* __restrict__ wp, __nv_bfloat16* __restrict__ wpt) {
+  const int coP = padc(cout);
+  const int64_t n = (int64_t)27 * cin * coP;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    // forward: q = ((t * cin/8 + g) * coP + co) * 8 + j, ci = 8 g + j
+    {
+      const int j = q % 8, co = (q / 8) % coP, g = (q / (8 * coP)) % (cin / 8),
+                t = (int)(q / ((int64_t)8 * coP * (cin / 8)));
+      const int ci = 8 * g + j;
+      const float v = co < cout ? w[((int64_t)co * cin + ci) * 27 + t] : 0.0f;
+      wp[q] = __float2bfloat16(v);
+    }
+    // data gradient: q = ((t * coP/8 + g) * cin + ci) * 8 + j, co = 8 g + j
+    {
+      const int j = q % 8, ci = (q / 8) % cin, g = (q / (8 * cin)) % (coP / 8),
+                t = (int)(q / ((int64_t)8 * cin * (coP / 8)));
+      const int co = 8 * g + j;
+      const float v = co < cout ? w[((int64_t)co * cin + ci) * 27 + (26 - t)] : 0.0f;
+      wpt[q] = __float2bfloat16(v);
+    }
+  }
+}
+
+struct FeatArgs {
+  int pj, pk;                 // padded fine dims j, k
+  int64_t pin;                // padded fine index of the pinned voxel
+  const uint8_t* label;       // padded fine labels
+  const float* invd;          // padded fine inverse diagonal
+  const float* r;             // padded fine residual
+  Dims c;                     // coarse dims
+};
+
+__device__ __forceinline__ int64_t fine_of(const FeatArgs& a, int d, int h, int w, int q) {
+  const int fi = 2 * d + ((q >> 2) & 1) + 1, fj = 2 * h + ((q >> 1) & 1) + 1,
+            fk = 2 * w + (q & 1) + 1;
+  return ((int64_t)fi * a.pj + fj) * a.pk + fk;
+}
+
+// raw[c] = mean over the 8 children of invd * r; partial sum of raw^2
+__global__ void __launch_bounds__(TB) feat_raw_kernel(FeatArgs a, float* __restrict__ raw,
+                                                     double* __restrict__ part) {
+  double acc = 0.0;
+  const int64_t n = a.c.n();
+  for (int64_t c = blockIdx.x * (int64_t)TB + threadIdx.x; c < n; c += (int64_t)gridDim.x * TB) {
+    const int w = c % a.c.W, h = (c / a.c.W) % a.c.H, d = (int)(c / ((int64_t)a.c.W * a.c.H));
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int64_t g = fine_of(a, d, h, w, q);
+      if (a.label[g] != 0 && g != a.pin) s += a.invd[g] * a.r[g];
+    }
+    s *= 0.125f;
+    raw[c] = s;
+    acc += (double)s * s;
+  }
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// scale s = sqrt(mean raw^2) (single block), stored as float
+__global__ void scale_kernel(const double* part, int nparts, int64_t n, float* scale) {
+  __shared__ double sh[TB];
+  double a = 0.0;
+  for (int q = threadIdx.x; q < nparts; q += TB) a += part[q];
+  sh[threadIdx.x] = a;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double rms = sqrt(sh[0] / (double)(n > 0 ? n : 1));
+    scale[0] = (float)(rms > 1e-30 ? rms : 1e-30);
+  }
+}
+
+// feat[c][0] = raw / s, channels 1.. from the geometry tensor
+__global__ void feat_write_kernel(const float* __restrict__ raw, const __nv_bfloat16* __restrict__ geo,
+                                  const float* __restrict__ scale, __nv_bfloat16* __restrict__ feat,
+                                  int64_t n) {
+  const float inv = 1.0f / scale[0];
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    __align__(16) __nv_bfloat16 v[16];
+    *(uint4*)&v[0] = ((const uint4*)(geo + c * 16))[0];
+    *(uint4*)&v[8] = ((const uint4*)(geo + c * 16))[1];
+    v[0] = __float2bfloat16(raw[c] * inv);
+    ((uint4*)(feat + c * 16))[0] = *(uint4*)&v[0];
+    ((uint4*)(feat + c * 16))[1] = *(uint4*)&v[8];
+  }
+}
+
+// 2 x 2 average pooling over (D, H): out dims (D/2, H/2, W)
+__global__ void pool_kernel(const __nv_bfloat16* __restrict__ in, __nv_bfloat16* __restrict__ out,
+                            Dims o, int C) {
+  const int64_t n = o.n() * C;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int c = q % C;
+    const int64_t v = q / C;
+    const int w = v % o.W, h = (v / o.W) % o.H, d = (int)(v / ((int64_t)o.W * o.H));
+    const int Hi = 2 * o.H;
+    float s = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        s += __bfloat162float(in[((((int64_t)(2 * d + a) * Hi + 2 * h + b) * o.W) + w) * C + c]);
+    out[q] = __float2bfloat16(0.25f * s);
+  }
+}
+
+// backward of pooling: gin (fine) += 0.25 * gout (coarse)
+__global__ void pool_back_kernel(const __nv_bfloat16* __restrict__ gout, __nv_bfloat16* __restrict__ gin,
+                                 Dims f, int C) {
+  const int64_t n = f.n() * C;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int c = q % C;
+    const int64_t v = q / C;
+    const int w = v % f.W, h = (v / f.W) % f.H, d = (int)(v / ((int64_t)f.W * f.H));
+    const int64_t vc = ((int64_t)(d / 2) * (f.H / 2) + h / 2) * f.W + w;
+    gin[q] = __float2bfloat16(__bfloat162float(gin[q]) + 0.25f * __bfloat162float(gout[vc * C + c]));
+  }
+}
+
+// out (fine, C1 + C2 channels) = [nearest-upsampled coarse (C1) | skip (C2)]
+__global__ void upcat_kernel(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
+                             __nv_bfloat16* __restrict__ out, Dims f, int C1, int C2) {
+  const int C = C1 + C2;
+  const int64_t n = f.n() * (C / 8);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int g = q % (C / 8);
+    const int64_t v = q / (C / 8);
+    const int w = v % f.W, h = (v / f.W) % f.H, d = (int)(v / ((int64_t)f.W * f.H));
+    uint4 val;
+    if (g * 8 < C1) {
+      const int64_t vc = ((int64_t)(d / 2) * (f.H / 2) + h / 2) * f.W + w;
+      val = *(const uint4*)(coarse + vc * C1 + g * 8);
+    } else {
+      val = *(const uint4*)(skip + v * C2 + (g * 8 - C1));
+    }
+    *(uint4*)(out + v * C + g * 8) = val;
+  }
+}
+
+// backward of upcat: gcoarse = sum of the 4 fine children's first C1
+// channels, gskip = remaining channels (overwrites both)
+__global__ void upcat_back_kernel(const __nv_bfloat16* __restrict__ gu, __nv_bfloat16* __restrict__ gcoarse,
+                                  __nv_bfloat16* __restrict__ gskip, Dims f, int C1, int C2) {
+  const int C = C1 + C2;
+  const Dims c{f.D / 2, f.H / 2, f.W};
+  const int64_t nc = c.n() * C1;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nc;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int ch = q % C1;
+    const int64_t v = q / C1;
+    const int w = v % c.W, h = (v / c.W) % c.H, d = (int)(v / ((int64_t)c.W * c.H));
+    float s = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        s += __bfloat162float(gu[((((int64_t)(2 * d + a) * f.H + 2 * h + b) * f.W) + w) * C + ch]);
+    gcoarse[q] = __float2bfloat16(s);
+  }
+  const int64_t nf = f.n() * C2;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nf;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int ch = q % C2;
+    const int64_t v = q / C2;
+    gskip[q] = gu[v * C + C1 + ch];
+  }
+}
+
+// g = g * (a > 0) (ReLU backward on a stored activation)
+__global__ void relu_mask_kernel(__nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ a, int64_t n) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    if (!(__bfloat162float(a[q]) > 0.0f)) g[q] = __float2bfloat16(0.0f);
+}
+
+struct ProlongArgs {
+  int pj, pk;
+  int64_t ng, pin;
+  const uint8_t* label;
+  const float* invd;
+  const float* r;
+  const float* y;       // coarse FP32 output
+  const float* scale;
+  float omega;
+  Dims c;
+  int use_net;
+};
+
+// z = omega * invd * r + s * y[parent] on active fine cells (0 elsewhere)
+__global__ void prolong_kernel(ProlongArgs a, float* __restrict__ z) {
+  const float s = a.use_net ? a.scale[0] : 0.0f;
+  const int64_t SI = (int64_t)a.pj * a.pk;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    float v = 0.0f;
+    if (a.label[g] != 0 && g != a.pin) {
+      v = a.omega * a.invd[g] * a.r[g];
+      if (a.use_net) {
+        const int i = (int)(g / SI) - 1, j = (int)((g / a.pk) % a.pj) - 1, k = (int)(g % a.pk) - 1;
+        v += s * a.y[((int64_t)(i / 2) * a.c.H + j / 2) * a.c.W + k / 2];
+      }
+    }
+    z[g] = v;
+  }
+}
+
+struct LossArgs {
+  FeatArgs f;
+  const float* e;        // padded fine error (FP32)
+  const float* y;
+  const float* scale;
+  float omega;
+  const double* enorm;   // [1] sum e^2
+};
+
+// sum e^2 over active fine cells (block partials)
+__global__ void __launch_bounds__(TB) enorm_kernel(FeatArgs a, const float* __restrict__ e, int64_t ng,
+                                                   double* part) {
+  double acc = 0.0;
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += (int64_t)gridDim.x * TB)
+    if (a.label[g] != 0 && g != a.pin) acc += (double)e[g] * e[g];
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void sum_kernel(const double* part, int nparts, double* out) {
+  __shared__ double sh[TB];
+  double a = 0.0;
+  for (int q = threadIdx.x; q < nparts; q += TB) a += part[q];
+  sh[threadIdx.x] = a;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+// Per coarse cell: loss partial and dL/d(net output) into channel 0 of a
+// 16-channel BF16 gradient tensor (other channels zero).
+//   L = sum_fine (omega invd r + s y_parent - e)^2 / ||e||^2
+__global__ void __launch_bounds__(TB) loss_kernel(LossArgs a, __nv_bfloat16* __restrict__ gout,
+                                                  double* part) {
+  const float s = a.scale[0];
+  const double inv_norm = 1.0 / fmax(a.enorm[0], 1e-300);
+  double acc = 0.0;
+  const int64_t n = a.f.c.n();
+  for (int64_t c = blockIdx.x * (int64_t)TB + threadIdx.x; c < n; c += (int64_t)gridDim.x * TB) {
+    const int w = c % a.f.c.W, h = (c / a.f.c.W) % a.f.c.H, d = (int)(c / ((int64_t)a.f.c.W * a.f.c.H));
+    const float yv = s * a.y[c];
+    double g = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int64_t fg = fine_of(a.f, d, h, w, q);
+      if (a.f.label[fg] != 0 && fg != a.f.pin) {
+        const double res = (double)a.omega * a.f.invd[fg] * a.f.r[fg] + yv - a.e[fg];
+        acc += res * res;
+        g += 2.0 * res;
+      }
+    }
+    // dL/dy_net = dL/dyv * s
+    const float gv = (float)(g * inv_norm * s);
+    __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) o[q] = __float2bfloat16(0.0f);
+    o[0] = __float2bfloat16(gv);
+    ((uint4*)(gout + c * 16))[0] = *(uint4*)&o[0];
+    ((uint4*)(gout + c * 16))[1] = *(uint4*)&o[8];
+  }
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = acc * inv_norm;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// Weight gradient of one 3x3x3 layer on the CUDA cores (FP32 accumulation):
+//   gw[co][ci][t] += sum_v X[v + off(t)][ci] * G[v][co],  gb[co] += sum_v G[v][co] (t = 13)
+// grid.x = 27 taps, grid.y = voxel chunks; each thread owns a 4 x 4 block of
+// (ci, co) pairs; voxel tiles of 32 are staged in shared memory as FP32.
+constexpr int WG_T = 32;
+__global__ void __launch_bounds__(TB)
+wgrad_kernel(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ G, Dims dm,
+             int cin, int cout, int coP, float* __restrict__ gw, float* __restrict__ gb) {
+  extern __shared__ float wsm[];
+  float* xs = wsm;                       // [WG_T][cin]
+  float* gs = wsm + WG_T * cin;          // [WG_T][cout]
+  const int t = blockIdx.x;
+  const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+  const int64_t n = dm.n();
+  const int64_t chunk = (n + gridDim.y - 1) / gridDim.y;
+  const int64_t v0 = blockIdx.y * chunk, v1 = min(n, v0 + chunk);
+  const int nci = cin / 4, nco = (cout + 3) / 4;
+  const int npair = nci * nco;
+  float acc[2][16];
+  float bacc[2] = {0.0f, 0.0f};
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[p][q] = 0.0f;
+  for (int64_t vt = v0; vt < v1; vt += WG_T) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < WG_T * cin; q += TB) {
+      const int vv = q / cin, ci = q % cin;
+      const int64_t v = vt + vv;
+      float xv = 0.0f;
+      if (v < v1) {
+        const int w = v % dm.W, h = (v / dm.W) % dm.H, d = (int)(v / ((int64_t)dm.W * dm.H));
+        const int dd = d + dz, hh = h + dy, ww = w + dx;
+        if (dd >= 0 && dd < dm.D && hh >= 0 && hh < dm.H && ww >= 0 && ww < dm.W)
+          xv = __bfloat162float(X[(((int64_t)dd * dm.H + hh) * dm.W + ww) * cin + ci]);
+      }
+      xs[q] = xv;
+    }
+    for (int q = threadIdx.x; q < WG_T * cout; q += TB) {
+      const int vv = q / cout, co = q % cout;
+      const int64_t v = vt + vv;
+      gs[q] = v < v1 ? __bfloat162float(G[v * coP + co]) : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const int pair = threadIdx.x + p * TB;
+      if (pair < npair) {
+        const int cb = (pair / nco) * 4, ob = (pair % nco) * 4;
+        for (int vv = 0; vv < WG_T; ++vv) {
+          float xv[4], gv[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) xv[a] = xs[vv * cin + cb + a];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) gv[b] = ob + b < cout ? gs[vv * cout + ob + b] : 0.0f;
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[p][a * 4 + b] += xv[a] * gv[b];
+        }
+      }
+    }
+    if (t == 13) {
+      for (int co = threadIdx.x; co < cout; co += TB)
+        for (int vv = 0; vv < WG_T; ++vv) bacc[co / TB] += gs[vv * cout + co];
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int pair = threadIdx.x + p * TB;
+    if (pair < npair) {
+      const int cb = (pair / nco) * 4, ob = (pair % nco) * 4;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (ob + b < cout) atomicAdd(&gw[((int64_t)(ob + b) * cin + cb + a) * 27 + t], acc[p][a * 4 + b]);
+    }
+  }
+  if (t == 13)
+    for (int co = threadIdx.x; co < cout; co += TB) atomicAdd(&gb[co], bacc[co / TB]);
+}
+
+// Adam on the flat parameter vector
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps,
+                            float c1, float c2) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const float gq = g[q];
+    const float mq = b1 * m[q] + (1.0f - b1) * gq;
+    const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
+    m[q] = mq;
+    v[q] = vq;
+    p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+  }
+}
+
+}  // namespace pc
+}  // namespace hp
+
+using namespace hp;
+using namespace hp::pc;
+
+struct HpPrecond {
+  int ni, nj, nk;            // fine (unpadded) torso dims
+  int pj, pk;
+  int64_t ng, pin;
+  Dims L[4];                 // L[1..3] network levels
+  float omega;
+  const uint8_t* label;      // borrowed (torso handle's padded labels) or owned
+  std::vector<void*> allocs;
+  // parameters: flat FP32 [all layers: w then b]
+  int64_t n_par;
+  float* par;
+  float* grad;
+  float* adam_m;
+  float* adam_v;
+  int64_t off_w[NL], off_b[NL];
+  __nv_bfloat16* wp[NL];
+  __nv_bfloat16* wpt[NL];
+  float* zero_bias;          // 96 zeros
+  // activations
+  __nv_bfloat16 *geo, *feat, *e1a, *e1b, *p1, *e2a, *e2b, *p2, *e3a, *e3b, *u2, *d2a, *d2b, *u1,
+      *d1a, *d1b;
+  float* y;
+  float* raw;
+  float* scale;
+  // gradients
+  __nv_bfloat16 *gout, *g_d1b, *g_d1a, *g_u1, *g_d2b, *g_e1b, *g_d2a, *g_u2, *g_e3b, *g_e2b,
+      *g_e3a, *g_p2, *g_e2a, *g_p1, *g_e1a;
+  double* part;
+  double* enorm;
+  double* loss;
+  int* err;
+  int64_t step;
+  int nblk;
+};
+
+template <typename T>
+static hp_status pal(HpPrecond* h, T** dst, size_t n) {
+  hp_status st = dev_alloc(dst, n);
+  if (st == HP_OK && *dst) h->allocs.push_back((void*)*dst);
+  return st;
+}
+
+#define PC_TRY(x)                \
+  do {                           \
+    hp_status _s = (x);          \
+    if (_s != HP_OK) {           \
+      hp_precond_destroy(h);     \
+      return _s;                 \
+    }                            \
+  } while (0)
+
+extern "C" hp_status hp_precond_destroy(HpPrecond* h);
+
+static hp_status repack(HpPrecond* h, cudaStream_t s) {
+  for (int l = 0; l < NL; ++l) {
+    pack_kernel<<<256, 256, 0, s>>>(h->par + h->off_w[l], LCIN[l], LCOUT[l], h->wp[l], h->wpt[l]);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, void* stream) {
+  HP_REQUIRE(d && out, "hp_precond_create: null argument");
+  *out = nullptr;
+  HP_REQUIRE(d->ni % 8 == 0 && d->nj % 8 == 0 && d->nk % 256 == 0,
+             "hp_precond_create: torso dims (%d,%d,%d) must be multiples of (8,8,256)", d->ni,
+             d->nj, d->nk);
+  HP_REQUIRE(d->label && d->n_materials >= 1 && d->n_materials <= HP_MAX_MATERIALS,
+             "hp_precond_create: bad labels");
+  cudaStream_t s = (cudaStream_t)stream;
+  HpPrecond* h = new HpPrecond();
+  h->ni = d->ni; h->nj = d->nj; h->nk = d->nk;
+  h->pj = d->nj + 2; h->pk = d->nk + 2;
+  h->ng = (int64_t)(d->ni + 2) * h->pj * h->pk;
+  h->pin = d->pin_cell;
+  h->omega = d->omega;
+  h->L[1] = Dims{d->ni / 2, d->nj / 2, d->nk / 2};
+  h->L[2] = Dims{d->ni / 4, d->nj / 4, d->nk / 2};
+  h->L[3] = Dims{d->ni / 8, d->nj / 8, d->nk / 2};
+  h->step = 0;
+  int nsm = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  h->nblk = nsm * 8;
+  // parameters
+  int64_t o = 0;
+  for (int l = 0; l < NL; ++l) {
+    h->off_w[l] = o;
+    o += (int64_t)LCOUT[l] * LCIN[l] * 27;
+    h->off_b[l] = o;
+    o += LCOUT[l];
+  }
+  h->n_par = o;
+  PC_TRY(pal(h, &h->par, o));
+  PC_TRY(pal(h, &h->grad, o));
+  PC_TRY(pal(h, &h->adam_m, o));
+  PC_TRY(pal(h, &h->adam_v, o));
+  {
+    // He-normal initial weights, zero biases (seeded, host-generated)
+    std::vector<float> w0(o, 0.0f);
+    uint64_t st = d->seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto unif = [&]() {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      return ((st >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    };
+    for (int l = 0; l < NL; ++l) {
+      const double sd = sqrt(2.0 / (27.0 * LCIN[l])) * (l == OUT ? 0.1 : 1.0);
+      for (int64_t q = 0; q < (int64_t)LCOUT[l] * LCIN[l] * 27; ++q) {
+        const double u1 = unif(), u2 = unif();
+        w0[h->off_w[l] + q] = (float)(sd * sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
+      }
+    }
+    if (d->init_params) std::copy(d->init_params, d->init_params + o, w0.begin());
+    HP_CUDA_TRY(cudaMemcpyAsync(h->par, w0.data(), o * 4, cudaMemcpyHostToDevice, s));
+    HP_CUDA_TRY(cudaMemsetAsync(h->adam_m, 0, o * 4, s));
+    HP_CUDA_TRY(cudaMemsetAsync(h->adam_v, 0, o * 4, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  for (int l = 0; l < NL; ++l) {
+    const size_t np = (size_t)27 * LCIN[l] * padc(LCOUT[l]);
+    PC_TRY(pal(h, &h->wp[l], np));
+    PC_TRY(pal(h, &h->wpt[l], np));
+  }
+  PC_TRY(pal(h, &h->zero_bias, 96));
+  HP_CUDA_TRY(cudaMemsetAsync(h->zero_bias, 0, 96 * 4, s));
+  const int64_t n1 = h->L[1].n(), n2 = h->L[2].n(), n3 = h->L[3].n();
+  PC_TRY(pal(h, &h->geo, n1 * 16));
+  PC_TRY(pal(h, &h->feat, n1 * 16));
+  PC_TRY(pal(h, &h->e1a, n1 * 16));
+  PC_TRY(pal(h, &h->e1b, n1 * 16));
+  PC_TRY(pal(h, &h->p1, n2 * 16));
+  PC_TRY(pal(h, &h->e2a, n2 * 32));
+  PC_TRY(pal(h, &h->e2b, n2 * 32));
+  PC_TRY(pal(h, &h->p2, n3 * 32));
+  PC_TRY(pal(h, &h->e3a, n3 * 64));
+  PC_TRY(pal(h, &h->e3b, n3 * 64));
+  PC_TRY(pal(h, &h->u2, n2 * 96));
+  PC_TRY(pal(h, &h->d2a, n2 * 32));
+  PC_TRY(pal(h, &h->d2b, n2 * 32));
+  PC_TRY(pal(h, &h->u1, n1 * 48));
+  PC_TRY(pal(h, &h->d1a, n1 * 16));
+  PC_TRY(pal(h, &h->d1b, n1 * 16));
+  PC_TRY(pal(h, &h->y, n1));
+  PC_TRY(pal(h, &h->raw, n1));
+  PC_TRY(pal(h, &h->scale, 1));
+  PC_TRY(pal(h, &h->gout, n1 * 16));
+  PC_TRY(pal(h, &h->g_d1b, n1 * 16));
+  PC_TRY(pal(h, &h->g_d1a, n1 * 16));
+  PC_TRY(pal(h, &h->g_u1, n1 * 48));
+  PC_TRY(pal(h, &h->g_d2b, n2 * 32));
+  PC_TRY(pal(h, &h->g_e1b, n1 * 16));
+  PC_TRY(pal(h, &h->g_d2a, n2 * 32));
+  PC_TRY(pal(h, &h->g_u2, n2 * 96));
+  PC_TRY(pal(h, &h->g_e3b, n3 * 64));
+  PC_TRY(pal(h, &h->g_e2b, n2 * 32));
+  PC_TRY(pal(h, &h->g_e3a, n3 * 64));
+  PC_TRY(pal(h, &h->g_p2, n3 * 32));
+  PC_TRY(pal(h, &h->g_e2a, n2 * 32));
+  PC_TRY(pal(h, &h->g_p1, n2 * 16));
+  PC_TRY(pal(h, &h->g_e1a, n1 * 16));
+  PC_TRY(pal(h, &h->part, h->nblk));
+  PC_TRY(pal(h, &h->enorm, 1));
+  PC_TRY(pal(h, &h->loss, 1));
+  PC_TRY(pal(h, &h->err, 1));
+  HP_CUDA_TRY(cudaMemsetAsync(h->err, 0, 4, s));
+  // geometry channels on the network grid (host): active fraction and the
+  // fraction of each material among the 8 fine children
+  {
+    const int ni = d->ni, nj = d->nj, nk = d->nk;
+    std::vector<__nv_bfloat16> geo((size_t)n1 * 16, __float2bfloat16(0.0f));
+    const Dims c = h->L[1];
+    for (int a = 0; a < c.D; ++a)
+      for (int b = 0; b < c.H; ++b)
+        for (int w = 0; w < c.W; ++w) {
+          float frac[HP_MAX_MATERIALS] = {0};
+          for (int q = 0; q < 8; ++q) {
+            const int i = 2 * a + ((q >> 2) & 1), j = 2 * b + ((q >> 1) & 1), k = 2 * w + (q & 1);
+            frac[d->label[((int64_t)i * nj + j) * nk + k]] += 0.125f;
+          }
+          const int64_t cc = ((int64_t)a * c.H + b) * c.W + w;
+          geo[cc * 16 + 1] = __float2bfloat16(1.0f - frac[0]);
+          for (int m = 1; m < d->n_materials && m < 15; ++m)
+            geo[cc * 16 + 1 + m] = __float2bfloat16(frac[m]);
+        }
+    (void)ni;
+    (void)nk;
+    HP_CUDA_TRY(cudaMemcpyAsync(h->geo, geo.data(), geo.size() * 2, cudaMemcpyHostToDevice, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  PC_TRY(repack(h, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  *out = h;
+  return HP_OK;
+}
+
+namespace hp {
+namespace pc {
+
+static hp_status conv(HpPrecond* h, int l, const __nv_bfloat16* X, void* Y, int epi,
+                      const __nv_bfloat16* mask, cudaStream_t s) {
+  const Dims dm = h->L[LLEV[l]];
+  return tc::conv3_launch(X, h->wp[l], h->par + h->off_b[l], Y, mask, dm.D, dm.H, dm.W, LCIN[l],
+                          padc(LCOUT[l]), epi, h->err, s);
+}
+
+// data gradient of layer l: gin = conv(gpre, flipped W^T), optional mask
+static hp_status dgrad(HpPrecond* h, int l, const __nv_bfloat16* gpre, __nv_bfloat16* gin,
+                       const __nv_bfloat16* mask, cudaStream_t s) {
+  const Dims dm = h->L[LLEV[l]];
+  return tc::conv3_launch(gpre, h->wpt[l], h->zero_bias, gin, mask, dm.D, dm.H, dm.W,
+                          padc(LCOUT[l]), LCIN[l], mask ? tc::EPI_MASK : tc::EPI_LINEAR, h->err, s);
+}
+
+static void wgrad(HpPrecond* h, int l, const __nv_bfloat16* X, const __nv_bfloat16* G,
+                  cudaStream_t s) {
+  const Dims dm = h->L[LLEV[l]];
+  const int cin = LCIN[l], cout = LCOUT[l];
+  const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, dm.n() / 4096));
+  const size_t smem = (size_t)WG_T * (cin + cout) * 4;
+  wgrad_kernel<<<dim3(27, chunks), TB, smem, s>>>(X, G, dm, cin, cout, padc(cout),
+                                                  h->grad + h->off_w[l], h->grad + h->off_b[l]);
+}
+
+static int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)); }
+
+hp_status precond_forward(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
+                          cudaStream_t s) {
+  FeatArgs fa{h->pj, h->pk, h->pin, label, invd, r, h->L[1]};
+  const int64_t n1 = h->L[1].n();
+  feat_raw_kernel<<<h->nblk, TB, 0, s>>>(fa, h->raw, h->part);
+  scale_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, n1, h->scale);
+  feat_write_kernel<<<grid_for(n1), 256, 0, s>>>(h->raw, h->geo, h->scale, h->feat, n1);
+  HP_CUDA_TRY(cudaGetLastError());
+  hp_status st;
+#define FW(x) do { st = (x); if (st != HP_OK) return st; } while (0)
+  FW(conv(h, E1A, h->feat, h->e1a, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, E1B, h->e1a, h->e1b, tc::EPI_RELU, nullptr, s));
+  pool_kernel<<<grid_for(h->L[2].n() * 16), 256, 0, s>>>(h->e1b, h->p1, h->L[2], 16);
+  FW(conv(h, E2A, h->p1, h->e2a, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, E2B, h->e2a, h->e2b, tc::EPI_RELU, nullptr, s));
+  pool_kernel<<<grid_for(h->L[3].n() * 32), 256, 0, s>>>(h->e2b, h->p2, h->L[3], 32);
+  FW(conv(h, E3A, h->p2, h->e3a, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, E3B, h->e3a, h->e3b, tc::EPI_RELU, nullptr, s));
+  upcat_kernel<<<grid_for(h->L[2].n() * 12), 256, 0, s>>>(h->e3b, h->e2b, h->u2, h->L[2], 64, 32);
+  FW(conv(h, D2A, h->u2, h->d2a, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, D2B, h->d2a, h->d2b, tc::EPI_RELU, nullptr, s));
+  upcat_kernel<<<grid_for(h->L[1].n() * 6), 256, 0, s>>>(h->d2b, h->e1b, h->u1, h->L[1], 32, 16);
+  FW(conv(h, D1A, h->u1, h->d1a, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, D1B, h->d1a, h->d1b, tc::EPI_RELU, nullptr, s));
+  FW(conv(h, OUT, h->d1b, h->y, tc::EPI_F32_C0, nullptr, s));
+#undef FW
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
+                        float* z, int use_net, cudaStream_t s) {
+  if (use_net) {
+    hp_status st = precond_forward(h, label, invd, r, s);
+    if (st != HP_OK) return st;
+  }
+  ProlongArgs pa{h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y, h->scale, h->omega,
+                 h->L[1], use_net};
+  prolong_kernel<<<grid_for(h->ng), 256, 0, s>>>(pa, z);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+}  // namespace pc
+}  // namespace hp
+
+extern "C" hp_status hp_precond_apply(HpPrecond* h, const uint8_t* label, const float* invd,
+                                      const float* r, float* z, int32_t use_net, void* stream) {
+  HP_REQUIRE(h && label && invd && r && z, "hp_precond_apply: null argument");
+  return hp::pc::precond_apply(h, label, invd, r, z, use_net, (cudaStream_t)stream);
+}
+
+extern "C" hp_status hp_precond_train_step(HpPrecond* h, const uint8_t* label, const float* invd,
+                                           const float* r, const float* e, float lr,
+                                           float* loss_out, void* stream) {
+  HP_REQUIRE(h && label && invd && r && e, "hp_precond_train_step: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  hp_status st = precond_forward(h, label, invd, r, s);
+  if (st != HP_OK) return st;
+  const Dims L1 = h->L[1], L2 = h->L[2], L3 = h->L[3];
+  const int64_t n1 = L1.n(), n2 = L2.n(), n3 = L3.n();
+  FeatArgs fa{h->pj, h->pk, h->pin, label, invd, r, L1};
+  enorm_kernel<<<h->nblk, TB, 0, s>>>(fa, e, h->ng, h->part);
+  sum_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->enorm);
+  LossArgs la{fa, e, h->y, h->scale, h->omega, h->enorm};
+  loss_kernel<<<h->nblk, TB, 0, s>>>(la, h->gout, h->part);
+  sum_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->loss);
+  HP_CUDA_TRY(cudaMemsetAsync(h->grad, 0, h->n_par * 4, s));
+#define BW(x) do { st = (x); if (st != HP_OK) return st; } while (0)
+  // OUT (linear, 16 -> 1 padded to 16)
+  wgrad(h, OUT, h->d1b, h->gout, s);
+  BW(dgrad(h, OUT, h->gout, h->g_d1b, h->d1b, s));          // -> dpre of D1B
+  wgrad(h, D1B, h->d1a, h->g_d1b, s);
+  BW(dgrad(h, D1B, h->g_d1b, h->g_d1a, h->d1a, s));         // -> dpre of D1A
+  wgrad(h, D1A, h->u1, h->g_d1a, s);
+  BW(dgrad(h, D1A, h->g_d1a, h->g_u1, nullptr, s));         // d u1 (48)
+  upcat_back_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_u1, h->g_d2b, h->g_e1b, L1, 32, 16);
+  relu_mask_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_d2b, h->d2b, n2 * 32);
+  wgrad(h, D2B, h->d2a, h->g_d2b, s);
+  BW(dgrad(h, D2B, h->g_d2b, h->g_d2a, h->d2a, s));
+  wgrad(h, D2A, h->u2, h->g_d2a, s);
+  BW(dgrad(h, D2A, h->g_d2a, h->g_u2, nullptr, s));         // d u2 (96)
+  upcat_back_kernel<<<grid_for(n2 * 64), 256, 0, s>>>(h->g_u2, h->g_e3b, h->g_e2b, L2, 64, 32);
+  relu_mask_kernel<<<grid_for(n3 * 64), 256, 0, s>>>(h->g_e3b, h->e3b, n3 * 64);
+  wgrad(h, E3B, h->e3a, h->g_e3b, s);
+  BW(dgrad(h, E3B, h->g_e3b, h->g_e3a, h->e3a, s));
+  wgrad(h, E3A, h->p2, h->g_e3a, s);
+  BW(dgrad(h, E3A, h->g_e3a, h->g_p2, nullptr, s));
+  pool_back_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_p2, h->g_e2b, L2, 32);
+  relu_mask_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_e2b, h->e2b, n2 * 32);
+  wgrad(h, E2B, h->e2a, h->g_e2b, s);
+  BW(dgrad(h, E2B, h->g_e2b, h->g_e2a, h->e2a, s));
+  wgrad(h, E2A, h->p1, h->g_e2a, s);
+  BW(dgrad(h, E2A, h->g_e2a, h->g_p1, nullptr, s));
+  pool_back_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_p1, h->g_e1b, L1, 16);
+  relu_mask_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_e1b, h->e1b, n1 * 16);
+  wgrad(h, E1B, h->e1a, h->g_e1b, s);
+  BW(dgrad(h, E1B, h->g_e1b, h->g_e1a, h->e1a, s));
+  wgrad(h, E1A, h->feat, h->g_e1a, s);
+#undef BW
+  HP_CUDA_TRY(cudaGetLastError());
+  if (lr > 0.0f) {
+    h->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)h->step), c2 = 1.0f - powf(b2, (float)h->step);
+    adam_kernel<<<grid_for(h->n_par), 256, 0, s>>>(h->par, h->grad, h->adam_m, h->adam_v,
+                                                   h->n_par, lr, b1, b2, 1e-8f, c1, c2);
+    st = repack(h, s);
+    if (st != HP_OK) return st;
+  }
+  if (loss_out) {
+    double l = 0.0;
+    HP_CUDA_TRY(cudaMemcpyAsync(&l, h->loss, 8, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    *loss_out = (float)l;
+  }
+  return HP_OK;
+}
+
+extern "C" hp_status hp_precond_params(HpPrecond* h, float* host_params, float* host_grads,
+                                       int64_t* n, int32_t set, void* stream) {
+  HP_REQUIRE(h && n, "hp_precond_params: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  *n = h->n_par;
+  if (set && host_params) {
+    HP_CUDA_TRY(cudaMemcpyAsync(h->par, host_params, h->n_par * 4, cudaMemcpyHostToDevice, s));
+    hp_status st = repack(h, s);
+    if (st != HP_OK) return st;
+  } else if (host_params) {
+    HP_CUDA_TRY(cudaMemcpyAsync(host_params, h->par, h->n_par * 4, cudaMemcpyDeviceToHost, s));
+  }
+  if (host_grads)
+    HP_CUDA_TRY(cudaMemcpyAsync(host_grads, h->grad, h->n_par * 4, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_precond_output(HpPrecond* h, float* host_y, float* host_scale,
+                                       int32_t* host_err, void* stream) {
+  HP_REQUIRE(h, "hp_precond_output: null handle");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (host_y) HP_CUDA_TRY(cudaMemcpyAsync(host_y, h->y, h->L[1].n() * 4, cudaMemcpyDeviceToHost, s));
+  if (host_scale) HP_CUDA_TRY(cudaMemcpyAsync(host_scale, h->scale, 4, cudaMemcpyDeviceToHost, s));
+  if (host_err) HP_CUDA_TRY(cudaMemcpyAsync(host_err, h->err, 4, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_precond_destroy(HpPrecond* h) {
+  if (!h) return HP_OK;
+  for (void* p : h->allocs) cudaFree(p);
+  delete h;
+  return HP_OK;
+}

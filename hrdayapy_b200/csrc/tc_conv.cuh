@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/hrdaya_b200.h"
+
 namespace hp {
 namespace tc {
 
@@ -170,6 +172,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 #pragma unroll
   for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
+
+// Host launcher of the convolution (conv.cu): epi 0 relu(acc + b),
+// 1 acc + b, 2 acc * (mask > 0), 3 fp32 channel 0.
+hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y,
+                       const void* mask, int D, int H, int W, int cin, int cout, int epi,
+                       int* err, cudaStream_t s);
 
 template <int N>
 struct TmemCols {
