@@ -90,6 +90,17 @@ class HpSolveStats(C.Structure):
                 ("rel_residual", C.c_double), ("stat", C.c_double), ("restarts", C.c_int32)]
 
 
+class HpPrecondDesc(C.Structure):
+    _fields_ = [("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("label", P),
+                ("n_materials", C.c_int32), ("pin_cell", C.c_int64), ("omega", C.c_float),
+                ("seed", C.c_uint64), ("init_params", P)]
+
+
+class HpTorsoArrays(C.Structure):
+    _fields_ = [("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("n_cells", C.c_int64),
+                ("pin_cell", C.c_int64), ("label", P), ("invd", P), ("r", P), ("x", P), ("b", P)]
+
+
 def _declare_optional(L):
     """Signatures of the torso entry points (include/hrdaya_b200.h)."""
     L.hp_torso_create.argtypes = [C.POINTER(HpTorsoDesc), C.POINTER(P), P]
@@ -103,6 +114,17 @@ def _declare_optional(L):
     L.hp_torso_destroy.argtypes = [P]
     L.hp_torso_residual_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32,
                                             C.c_double, C.c_int64, P, P, P, P]
+    L.hp_precond_create.argtypes = [C.POINTER(HpPrecondDesc), C.POINTER(P), P]
+    L.hp_precond_apply.argtypes = [P, P, P, P, P, C.c_int32, P]
+    L.hp_precond_train_step.argtypes = [P, P, P, P, P, C.c_float, P, P]
+    L.hp_precond_params.argtypes = [P, P, P, P, C.c_int32, P]
+    L.hp_precond_output.argtypes = [P, P, P, P, P]
+    L.hp_precond_destroy.argtypes = [P]
+    L.hp_torso_arrays.argtypes = [P, C.POINTER(HpTorsoArrays)]
+    L.hp_torso_solve_frame_fcg.argtypes = [P, P, P, C.c_int32, P, C.c_int32, C.c_double,
+                                           C.c_int32, C.c_int32, C.POINTER(HpSolveStats), P]
+    L.hp_torso_train_precond.argtypes = [P, P, P, C.c_int64, C.c_int32, P, C.c_int32, C.c_int32,
+                                         C.c_float, C.c_double, P, P]
     L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, P, P]
 

@@ -10,13 +10,6 @@
 namespace hp {
 namespace tc {
 
-enum Epi : int {
-  EPI_RELU = 0,     // y = relu(acc + bias)                 (bf16)
-  EPI_LINEAR = 1,   // y = acc + bias                        (bf16)
-  EPI_MASK = 2,     // y = acc * (mask > 0)                  (bf16)  ReLU backward
-  EPI_F32_C0 = 3    // y = acc[:, 0] + bias[0]               (fp32, one channel)
-};
-
 template <int CIN, int COUT>
 struct ConvCfg {
   static constexpr int G = CIN / 8;

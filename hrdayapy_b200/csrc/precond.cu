@@ -24,6 +24,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <vector>
 
 namespace hp {
@@ -40,7 +41,7 @@ constexpr int TB = 256;
 
 struct Dims {
   int D, H, W;            // network level dims
-  int64_t n() const { return (int64_t)D * H * W; }
+  __host__ __device__ int64_t n() const { return (int64_t)D * H * W; }
 };
 
 // ------------------------------------------------------------------ kernels

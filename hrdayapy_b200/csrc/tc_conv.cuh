@@ -173,6 +173,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+enum Epi : int {
+  EPI_RELU = 0,     // y = relu(acc + bias)                 (bf16)
+  EPI_LINEAR = 1,   // y = acc + bias                        (bf16)
+  EPI_MASK = 2,     // y = acc * (mask > 0)                  (bf16)  ReLU backward
+  EPI_F32_C0 = 3    // y = acc[:, 0] + bias[0]               (fp32, one channel)
+};
+
 // Host launcher of the convolution (conv.cu): epi 0 relu(acc + b),
 // 1 acc + b, 2 acc * (mask > 0), 3 fp32 channel 0.
 hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y,

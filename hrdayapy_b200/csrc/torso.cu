@@ -622,20 +622,14 @@ static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
   return HP_OK;
 }
 
-extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t vm_on_device,
-                                          float* out, int32_t out_on_device, double tol,
-                                          int32_t rule, int32_t max_iter, HpSolveStats* stats,
-                                          void* stream) {
-  HP_REQUIRE(h, "hp_torso_solve_frame: null handle");
-  HP_REQUIRE(rule >= 0 && rule <= 2, "hp_torso_solve_frame: unknown rule %d", rule);
-  HP_REQUIRE(max_iter >= 1, "hp_torso_solve_frame: max_iter must be >= 1");
-  HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame: tol must be positive");
-  cudaStream_t s = (cudaStream_t)stream;
+namespace hp {
+
+// b <- per-frame source (compute_bspm.py:381-419)
+static hp_status build_rhs(HpTorso* h, const float* vm, int vm_on_device, cudaStream_t s) {
   TorsoArgs& a = h->a;
   SrcArgs& sa = h->s;
-  // 1. sources -> b
   if (sa.n_heart > 0) {
-    HP_REQUIRE(vm, "hp_torso_solve_frame: vm is null");
+    HP_REQUIRE(vm, "torso solve: vm is null");
     HP_CUDA_TRY(cudaMemcpyAsync(h->vm_dev, vm, (size_t)sa.n_heart * 4,
                                 vm_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   }
@@ -647,12 +641,27 @@ extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t v
                                                            h->seg_grid, h->n_seg, a.scal,
                                                            h->inv_nexp, a.b, a.pin);
   }
-  // 2. scalars: rule, tolerance (stat units: volts for RMS/LINF), limits
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+static hp_status read_scalars(HpTorso* h, cudaStream_t s) {
+  HP_CUDA_TRY(cudaMemcpyAsync(h->h_scal, h->a.scal, N_SCAL * 8, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+// Jacobi-PCG from the current x on the current b.  *result receives the
+// outcome (HP_OK, NOT_CONVERGED, STAGNATED, NONFINITE).
+static hp_status pcg_solve(HpTorso* h, double tol, int rule, int max_iter, HpSolveStats* stats,
+                           hp_status* result_out, cudaStream_t s) {
+  TorsoArgs& a = h->a;
   double tol_dev = rule == HP_STOP_REL ? tol : tol * 1e-3;   // mV -> V for the mV rules
   HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol_dev, 8, cudaMemcpyHostToDevice, s));
   int32_t is_init[N_ISCAL] = {0, 0, rule, max_iter, 0, 0};
   HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_init, sizeof(is_init), cudaMemcpyHostToDevice, s));
-  // 3. r = b - A x0 (warm start; x = 0 for the first frame), beta = 0
+  // r = b - A x0 (warm start; x = 0 for the first frame), beta = 0
   true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
   HP_CUDA_TRY(cudaGetLastError());
   int restarts = 0;
@@ -671,19 +680,16 @@ extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t v
     }
     if (rule == HP_STOP_REL && rel <= tol) break;
     if (total_it >= max_iter) { result = HP_ERR_NOT_CONVERGED; break; }
-    // iterate
     int32_t is_run[N_ISCAL] = {0, 0, rule, max_iter - total_it, 0, 0};
     HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_run, sizeof(is_run), cudaMemcpyHostToDevice, s));
     const int par0 = h->parity;
     hp_status st = run_iterations(h, max_iter - total_it, s);
     if (st != HP_OK) return st;
-    HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
-    HP_CUDA_TRY(cudaMemcpyAsync(h->h_scal, a.scal, N_SCAL * 8, cudaMemcpyDeviceToHost, s));
-    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    st = read_scalars(h, s);
+    if (st != HP_OK) return st;
     const int its = h->h_iscal[IS_ITER];
     total_it += its;
-    // p of the last iteration lives in buffer (par0 ^ its) ^ ... : iteration q
-    // (0-based) reads parity par0^(q&1) and writes the other one
+    // iteration q (0-based) reads parity par0 ^ (q & 1) and writes the other
     const int last_out = (par0 ^ ((its - 1) & 1)) ^ 1;
     h->parity = (par0 ^ (its & 1));
     if (its > 0) {
@@ -701,26 +707,13 @@ extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t v
       if (h->h_iscal[IS_BREAKDOWN]) result = HP_OK;   // reference: break, return x
       break;
     }
-    if (h->h_iscal[IS_BREAKDOWN] && total_it < max_iter) {
-      // Krylov breakdown: restart from the true residual
-      ++restarts;
-    }
-    // relative rule: true residual decides; replace r and restart if needed
+    // relative rule: the true residual decides; replace r and restart if needed
     true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
     HP_CUDA_TRY(cudaGetLastError());
     ++restarts;
     if (restarts > 50) { result = HP_ERR_STAGNATED; break; }
   }
   if (rule == HP_STOP_REL && restarts > 0) --restarts;   // the final check is not a restart
-  // read-out
-  if (h->n_read > 0 && out) {
-    gather_out<<<(h->n_read + 255) / 256, 256, 0, s>>>(a.x, h->grid_of_read, h->n_read,
-                                                        out_on_device ? out : h->out_dev);
-    if (!out_on_device)
-      HP_CUDA_TRY(cudaMemcpyAsync(out, h->out_dev, h->n_read * 4, cudaMemcpyDeviceToHost, s));
-  }
-  HP_CUDA_TRY(cudaGetLastError());
-  HP_CUDA_TRY(cudaStreamSynchronize(s));
   if (stats) {
     stats->iterations = total_it;
     stats->status = result;
@@ -728,13 +721,311 @@ extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t v
     stats->stat = h->h_scal[SC_STAT];
     stats->restarts = restarts;
   }
-  h->have_x = true;
-  if (result == HP_ERR_NOT_CONVERGED || result == HP_ERR_STAGNATED) return HP_OK;  // reported in stats
+  *result_out = result;
+  return HP_OK;
+}
+
+static hp_status readout(HpTorso* h, float* out, int out_on_device, cudaStream_t s) {
+  if (h->n_read > 0 && out) {
+    gather_out<<<(h->n_read + 255) / 256, 256, 0, s>>>(h->a.x, h->grid_of_read, h->n_read,
+                                                        out_on_device ? out : h->out_dev);
+    if (!out_on_device)
+      HP_CUDA_TRY(cudaMemcpyAsync(out, h->out_dev, h->n_read * 4, cudaMemcpyDeviceToHost, s));
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+static hp_status finish(hp_status result, const char* what) {
+  if (result == HP_ERR_NOT_CONVERGED || result == HP_ERR_STAGNATED) return HP_OK;  // in stats
   if (result != HP_OK) {
-    hp::set_error("hp_torso_solve_frame: non-finite values in the solve");
+    hp::set_error("%s: non-finite values in the solve", what);
     return result;
   }
   return HP_OK;
+}
+
+}  // namespace hp
+
+extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t vm_on_device,
+                                          float* out, int32_t out_on_device, double tol,
+                                          int32_t rule, int32_t max_iter, HpSolveStats* stats,
+                                          void* stream) {
+  HP_REQUIRE(h, "hp_torso_solve_frame: null handle");
+  HP_REQUIRE(rule >= 0 && rule <= 2, "hp_torso_solve_frame: unknown rule %d", rule);
+  HP_REQUIRE(max_iter >= 1, "hp_torso_solve_frame: max_iter must be >= 1");
+  HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame: tol must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  hp_status st = build_rhs(h, vm, vm_on_device, s);
+  if (st != HP_OK) return st;
+  hp_status result = HP_OK;
+  st = pcg_solve(h, tol, rule, max_iter, stats, &result, s);
+  if (st != HP_OK) return st;
+  st = readout(h, out, out_on_device, s);
+  if (st != HP_OK) return st;
+  h->have_x = true;
+  return finish(result, "hp_torso_solve_frame");
+}
+
+extern "C" hp_status hp_torso_arrays(HpTorso* h, HpTorsoArrays* o) {
+  HP_REQUIRE(h && o, "hp_torso_arrays: null argument");
+  o->ni = h->ni; o->nj = h->nj; o->nk = h->nk;
+  o->n_cells = h->a.ng;
+  o->pin_cell = h->a.pin;
+  o->label = h->a.label;
+  o->invd = h->a.invd;
+  o->r = h->a.r;
+  o->x = h->a.x;
+  o->b = h->a.b;
+  return HP_OK;
+}
+
+// ------------------------------------------------------------ flexible CG
+
+namespace hp {
+namespace pc {
+hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
+                        float* z, int use_net, cudaStream_t s);
+}
+
+// q = A p (p in p0), partial p.q and p.r; last block: alpha = p.r / p.q
+__global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
+  if (a.iscal[IS_DONE]) return;
+  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB) {
+    const int l = a.label[g];
+    if (l == 0 || g == a.pin) continue;
+    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+    float diag = 0.0f, off = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const float t = c_T32[l * HP_MAX_MATERIALS + a.label[nb[f]]];
+      diag += t;
+      off += t * a.p0[nb[f]];
+    }
+    const float pv = a.p0[g];
+    const float q = diag * pv - off;
+    a.Ap[g] = q;
+    acc[0] += (double)pv * q;
+    acc[1] += (double)pv * a.r[g];
+  }
+  double tot[2];
+  if (block_reduce_last<2>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+    a.scal[SC_PAP] = tot[0];
+    if (!(fabs(tot[0]) >= 1e-30) || !isfinite(tot[0])) {
+      a.iscal[IS_BREAKDOWN] = isfinite(tot[0]) ? 1 : 0;
+      a.iscal[IS_NONFINITE] = isfinite(tot[0]) ? 0 : 1;
+      a.iscal[IS_DONE] = 1;
+      a.scal[SC_ALPHA] = 0.0;
+    } else {
+      a.scal[SC_ALPHA] = tot[1] / tot[0];
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q, partial r.r; last block: recursive stat, done test
+__global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
+  if (a.iscal[IS_DONE]) return;
+  const double alpha = a.scal[SC_ALPHA];
+  const float af = (float)alpha;
+  double acc[1] = {0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB) {
+    if (!is_row(a, g)) continue;
+    a.x[g] += alpha * (double)a.p0[g];
+    const float r = a.r[g] - af * a.Ap[g];
+    a.r[g] = r;
+    acc[0] += (double)r * r;
+  }
+  double tot[1];
+  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+    a.scal[SC_RR] = tot[0];
+    const double stat = sqrt(tot[0] / fmax(a.scal[SC_BB], 1e-300));
+    a.scal[SC_STAT] = stat;
+    const int it = ++a.iscal[IS_ITER];
+    if (!isfinite(tot[0])) { a.iscal[IS_NONFINITE] = 1; a.iscal[IS_DONE] = 1; }
+    else if (stat < 0.5 * a.scal[SC_TOL] || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
+  }
+}
+
+// partial z.q (z in p1); last block: beta = -z.q / p.q
+__global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a) {
+  double acc[1] = {0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB)
+    if (is_row(a, g)) acc[0] += (double)a.p1[g] * a.Ap[g];
+  double tot[1];
+  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0)
+    a.scal[SC_BETA] = -tot[0] / a.scal[SC_PAP];
+}
+
+// p = z + beta p
+__global__ void fcg_p(TorsoArgs a, int first) {
+  const float beta = first ? 0.0f : (float)a.scal[SC_BETA];
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * blockDim.x)
+    if (is_row(a, g)) a.p0[g] = a.p1[g] + beta * a.p0[g];
+}
+
+__global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, float* __restrict__ e) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * blockDim.x)
+    e[g] = is_row(a, g) ? (float)(xstar[g] - a.x[g]) : 0.0f;
+}
+
+static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
+                           HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
+  TorsoArgs& a = h->a;
+  HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol, 8, cudaMemcpyHostToDevice, s));
+  int32_t is_init[N_ISCAL] = {0, 0, HP_STOP_REL, fallback_iter, 0, 0};
+  HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_init, sizeof(is_init), cudaMemcpyHostToDevice, s));
+  true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+  HP_CUDA_TRY(cudaGetLastError());
+  hp_status st = read_scalars(h, s);
+  if (st != HP_OK) return st;
+  double bb = h->h_scal[SC_BB];
+  double rel = bb > 0.0 ? sqrt(h->h_scal[SC_TRUE_RR] / bb) : 0.0;
+  int it = 0, restarts = 0;
+  hp_status result = HP_OK;
+  bool fallback = false;
+  if (bb == 0.0) {
+    HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, a.ng * 8, s));
+    rel = 0.0;
+  } else if (rel > tol) {
+    bool restart = true;
+    double hist[8];
+    int nh = 0;
+    while (true) {
+      if (restart) {
+        st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, 1, s);
+        if (st != HP_OK) return st;
+        fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
+        restart = false;
+      }
+      fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
+      fcg_update<<<h->nblk, TB, 0, s>>>(a);
+      HP_CUDA_TRY(cudaGetLastError());
+      st = read_scalars(h, s);
+      if (st != HP_OK) return st;
+      it = h->h_iscal[IS_ITER];
+      if (h->h_iscal[IS_NONFINITE] || h->h_iscal[IS_BREAKDOWN]) { fallback = true; break; }
+      const double stat = h->h_scal[SC_STAT];
+      hist[nh % 8] = stat;
+      ++nh;
+      const bool stagnant = nh > 6 && stat > 0.97 * hist[(nh - 6) % 8];
+      if (h->h_iscal[IS_DONE]) {
+        if (it >= fallback_iter) { fallback = true; break; }
+        // recursive residual below tol / 2: the FP64 true residual decides
+        true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+        st = read_scalars(h, s);
+        if (st != HP_OK) return st;
+        rel = sqrt(h->h_scal[SC_TRUE_RR] / h->h_scal[SC_BB]);
+        if (rel <= tol) break;
+        ++restarts;
+        int32_t is_re[N_ISCAL] = {0, it, HP_STOP_REL, fallback_iter, 0, 0};
+        HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_re, sizeof(is_re), cudaMemcpyHostToDevice, s));
+        restart = true;
+        continue;
+      }
+      if (stagnant) { fallback = true; break; }
+      st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, 1, s);
+      if (st != HP_OK) return st;
+      fcg_beta<<<h->nblk, TB, 0, s>>>(a);
+      fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
+    }
+  }
+  if (fallback) {
+    HpSolveStats st2;
+    hp_status r2 = HP_OK;
+    st = pcg_solve(h, tol, HP_STOP_REL, std::max(1, max_iter - it), &st2, &r2, s);
+    if (st != HP_OK) return st;
+    it += st2.iterations;
+    rel = st2.rel_residual;
+    result = r2;
+    restarts += 1000;
+  }
+  if (stats) {
+    stats->iterations = it;
+    stats->status = result;
+    stats->rel_residual = rel;
+    stats->stat = rel;
+    stats->restarts = restarts;
+  }
+  *result_out = result;
+  return HP_OK;
+}
+
+}  // namespace hp
+
+extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const float* vm,
+                                              int32_t vm_on_device, float* out,
+                                              int32_t out_on_device, double tol, int32_t max_iter,
+                                              int32_t fallback_iter, HpSolveStats* stats,
+                                              void* stream) {
+  HP_REQUIRE(h && p, "hp_torso_solve_frame_fcg: null handle");
+  HP_REQUIRE(max_iter >= 1 && fallback_iter >= 1, "hp_torso_solve_frame_fcg: bad iteration limits");
+  HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame_fcg: tol must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  hp_status st = build_rhs(h, vm, vm_on_device, s);
+  if (st != HP_OK) return st;
+  hp_status result = HP_OK;
+  st = fcg_solve(h, p, tol, max_iter, fallback_iter, stats, &result, s);
+  if (st != HP_OK) return st;
+  st = readout(h, out, out_on_device, s);
+  if (st != HP_OK) return st;
+  h->have_x = true;
+  return finish(result, "hp_torso_solve_frame_fcg");
+}
+
+extern "C" hp_status hp_torso_train_precond(HpTorso* h, HpPrecond* p, const float* vm_frames,
+                                            int64_t frame_stride, int32_t n_frames,
+                                            const int32_t* ks, int32_t n_ks, int32_t repeats,
+                                            float lr, double tol_exact, float* loss_hist,
+                                            void* stream) {
+  HP_REQUIRE(h && p && vm_frames && ks && n_frames >= 1 && n_ks >= 1 && repeats >= 1,
+             "hp_torso_train_precond: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  TorsoArgs& a = h->a;
+  double *xstar = nullptr, *x0 = nullptr;
+  float* e = nullptr;
+  HP_CUDA_TRY(cudaMalloc((void**)&xstar, a.ng * 8));
+  HP_CUDA_TRY(cudaMalloc((void**)&x0, a.ng * 8));
+  HP_CUDA_TRY(cudaMalloc((void**)&e, a.ng * 4));
+  hp_status ret = HP_OK;
+  int64_t q = 0;
+  for (int f = 0; f < n_frames && ret == HP_OK; ++f) {
+    ret = build_rhs(h, vm_frames + (int64_t)f * frame_stride, 1, s);
+    if (ret != HP_OK) break;
+    if (cudaMemcpyAsync(x0, a.x, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
+    hp_status res = HP_OK;
+    ret = pcg_solve(h, tol_exact, HP_STOP_REL, 20000, nullptr, &res, s);
+    if (ret != HP_OK) break;
+    if (cudaMemcpyAsync(xstar, a.x, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
+    for (int kq = 0; kq < n_ks && ret == HP_OK; ++kq) {
+      if (cudaMemcpyAsync(a.x, x0, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
+      if (ks[kq] > 0) {
+        // exactly ks[kq] plain iterations; r ends as the true residual of x_k
+        ret = pcg_solve(h, 1e-300, HP_STOP_REL, ks[kq], nullptr, &res, s);
+        if (ret != HP_OK) break;
+      } else {
+        true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+      }
+      error_kernel<<<h->nblk, TB, 0, s>>>(a, xstar, e);
+      for (int rp = 0; rp < repeats && ret == HP_OK; ++rp) {
+        float loss = 0.0f;
+        ret = hp_precond_train_step(p, a.label, a.invd, a.r, e, lr, &loss, s);
+        if (loss_hist) loss_hist[q] = loss;
+        ++q;
+      }
+    }
+    if (ret == HP_OK && cudaMemcpyAsync(a.x, xstar, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      ret = HP_ERR_CUDA;
+  }
+  cudaStreamSynchronize(s);
+  cudaFree(xstar);
+  cudaFree(x0);
+  cudaFree(e);
+  return ret;
 }
 
 extern "C" hp_status hp_torso_copy_solution(HpTorso* h, double* x_rows, void* stream) {

@@ -285,6 +285,85 @@ hp_status hp_conv3_forward(const void *X, const void *Wp, const float *bias, voi
                            const void *mask, int32_t D, int32_t H, int32_t W, int32_t cin,
                            int32_t cout, int32_t epi, int32_t *err, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Learned torso preconditioner and flexible CG (no counterpart in the  */
+/* reference, whose torso solver is Jacobi-PCG only)                    */
+/* ------------------------------------------------------------------ */
+
+/*
+ * M(r) = omega D^-1 r + P(s * CNN([R(D^-1 r) / s, geometry])) on a network
+ * grid of half the torso resolution (see csrc/precond.cu).  Torso dims must
+ * be multiples of (8, 8, 256).  label: HOST unpadded material labels;
+ * pin_cell: padded flat index of the pinned voxel; init_params: HOST flat
+ * parameter vector or NULL for a seeded random initialisation.
+ */
+typedef struct {
+  int32_t ni, nj, nk;
+  const uint8_t *label;
+  int32_t n_materials;
+  int64_t pin_cell;
+  float omega;
+  uint64_t seed;
+  const float *init_params;
+} HpPrecondDesc;
+
+typedef struct HpPrecond HpPrecond;
+
+hp_status hp_precond_create(const HpPrecondDesc *desc, HpPrecond **out, void *stream);
+/* z = M(r) over the padded torso grid (device arrays: label uint8, invd and
+ * r fp32, z fp32 out); use_net = 0 applies the Jacobi term only. */
+hp_status hp_precond_apply(HpPrecond *h, const uint8_t *label, const float *invd, const float *r,
+                           float *z, int32_t use_net, void *stream);
+/* One training step on the pair (r, e) (padded device fp32 arrays): forward,
+ * loss ||M(r) - e||^2 / ||e||^2, backward, and an Adam step of size lr
+ * (lr = 0: gradients only).  *loss_out (host) receives the loss. */
+hp_status hp_precond_train_step(HpPrecond *h, const uint8_t *label, const float *invd,
+                                const float *r, const float *e, float lr, float *loss_out,
+                                void *stream);
+/* Flat FP32 parameters / last gradients to or from host memory (set = 1
+ * uploads host_params); *n receives the parameter count. */
+hp_status hp_precond_params(HpPrecond *h, float *host_params, float *host_grads, int64_t *n,
+                            int32_t set, void *stream);
+/* Network output of the last forward (half-resolution grid, fp32), the
+ * input scale s and the device error flag, to host memory. */
+hp_status hp_precond_output(HpPrecond *h, float *host_y, float *host_scale, int32_t *host_err,
+                            void *stream);
+hp_status hp_precond_destroy(HpPrecond *h);
+
+/* Device pointers of a torso handle's padded arrays (for the preconditioner
+ * and for tests). */
+typedef struct {
+  int32_t ni, nj, nk;
+  int64_t n_cells, pin_cell;
+  const uint8_t *label;
+  const float *invd;
+  float *r;
+  double *x;
+  float *b;
+} HpTorsoArrays;
+hp_status hp_torso_arrays(HpTorso *h, HpTorsoArrays *out);
+
+/* Flexible CG with the learned preconditioner for one frame, judged by the
+ * same FP64 true relative residual <= tol.  If it has not converged after
+ * fallback_iter iterations, or stagnates, the frame is finished by plain
+ * Jacobi-PCG (stats->restarts counts the fallback as 1000). */
+hp_status hp_torso_solve_frame_fcg(HpTorso *h, HpPrecond *p, const float *vm,
+                                   int32_t vm_on_device, float *out, int32_t out_on_device,
+                                   double tol, int32_t max_iter, int32_t fallback_iter,
+                                   HpSolveStats *stats, void *stream);
+
+/* Trains the preconditioner on residual/error pairs generated by the plain
+ * solver: for each of n_frames frames (vm_frames: device fp32, frame f at
+ * vm_frames + f * frame_stride) the frame is solved to tol_exact (warm
+ * start from the previous frame), then for each k in ks (host, n_ks values)
+ * plain PCG is restarted from the warm start for k iterations and the pair
+ * (r_k, x* - x_k) gives `repeats` Adam steps of size lr.  loss_hist (host,
+ * n_frames * n_ks * repeats) receives the losses. */
+hp_status hp_torso_train_precond(HpTorso *h, HpPrecond *p, const float *vm_frames,
+                                 int64_t frame_stride, int32_t n_frames, const int32_t *ks,
+                                 int32_t n_ks, int32_t repeats, float lr, double tol_exact,
+                                 float *loss_hist, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
