@@ -169,6 +169,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     prob, info = build_workload(args.workload)
+    prob.kernel = args.kernel
     fs = prob.frame_steps
     total_steps = (args.warmup + args.steps) * fs
     prob.n_steps = total_steps
@@ -177,6 +178,7 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         sim = M.MonoHandle(prob, stream=M._lib.C.c_void_p(stream.cuda_stream))
+        kinfo = sim.kernel_info()
         sim.run(args.warmup * fs, graph_chunk=fs)
         stream.synchronize()
         if dist:
@@ -217,6 +219,7 @@ def run_ours(args):
             "config": {"workload": args.workload, "n_voxels": int(n_vox),
                        "n_purkinje": int(prob.n_pk), "dt_ms": prob.dt,
                        "time_steps_per_bench_step": fs, "brick": list(prob.layout.brick),
+                       "kernel": {1: "brick", 2: "pipelined"}[kinfo[0]], "grid": kinfo[1],
                        "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -331,6 +334,8 @@ def main():
     ap.add_argument("--workload", default="biv_shell")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="monodomain step kernel: 0 auto, 1 per-brick, 2 pipelined")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -44,6 +44,7 @@ class HpMonoDesc(C.Structure):
         ("n_myo", C.c_int32), ("slot_of_node", P), ("vm_every", C.c_int64),
         ("n_surf", C.c_int32), ("surf_of_slot", P), ("frame_every", C.c_int64),
         ("act_threshold", C.c_float), ("deact_threshold", C.c_float), ("max_events", C.c_int32),
+        ("kernel", C.c_int32),
     ]
 
 
@@ -71,6 +72,7 @@ def lib():
     L.hp_mono_copy_v.argtypes = [P, P, P, P]
     L.hp_mono_copy_state.argtypes = [P, P, P, P]
     L.hp_mono_destroy.argtypes = [P]
+    L.hp_mono_kernel_info.argtypes = [P, P, P, P]
     _lib = L
     _declare_optional(L)
     return L

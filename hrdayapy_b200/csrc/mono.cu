@@ -29,6 +29,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 
+#include <algorithm>
 #include <vector>
 
 namespace hp {
@@ -84,6 +85,9 @@ struct MonoArgs {
   float* deact_t;
   uint8_t* deact_n;
   const int64_t* d_step;
+  // pipelined kernel: halo copy table of the brick shape
+  int32_t n_halo;
+  const uint32_t* halo_tab;
 };
 
 // TTP06 phenotype table (ttp06_phenotype_constants.py:54-61), index = pheno-1.
@@ -201,12 +205,114 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
+// Diffusion half of one voxel: V_{i+1} = clamp(W + sum coef (W_j - W), ...)
+// from shared tiles with strides SI (i), SJ (j), 1 (k); face weights and
+// off-diagonal tensor components are three tiles each, NS floats apart.
+template <int SI, int SJ, int NS, bool ANISO>
+__device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, const float* tW,
+                                         const float* tD, int c, uint32_t tag, int64_t slot,
+                                         bool odd) {
+  const float Vc = tV[c];
+  float acc = 0.0f;
+  const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
+  if constexpr (!ANISO) {
+    float s = 0.0f;
+    if (fb & 1u) s += tV[c + SI] - Vc;
+    if (fb & 2u) s += tV[c - SI] - Vc;
+    if (fb & 4u) s += tV[c + SJ] - Vc;
+    if (fb & 8u) s += tV[c - SJ] - Vc;
+    if (fb & 16u) s += tV[c + 1] - Vc;
+    if (fb & 32u) s += tV[c - 1] - Vc;
+    acc = a.iso_coef * s;
+  } else {
+    const float* tWx = tW;
+    const float* tWy = tW + NS;
+    const float* tWz = tW + 2 * NS;
+    if (fb & 1u) acc += tWx[c] * (tV[c + SI] - Vc);
+    if (fb & 2u) acc += tWx[c - SI] * (tV[c - SI] - Vc);
+    if (fb & 4u) acc += tWy[c] * (tV[c + SJ] - Vc);
+    if (fb & 8u) acc += tWy[c - SJ] * (tV[c - SJ] - Vc);
+    if (fb & 16u) acc += tWz[c] * (tV[c + 1] - Vc);
+    if (fb & 32u) acc += tWz[c - 1] * (tV[c - 1] - Vc);
+    const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
+    const float* t01 = tD;
+    const float* t02 = tD + NS;
+    const float* t12 = tD + 2 * NS;
+    // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
+#define HP_DIAG(bit, T, OFF, SGN)                                            \
+  if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
+                                 (tV[c + (OFF)] - Vc);
+    HP_DIAG(0, t01, SI + SJ, 1.0f)
+    HP_DIAG(1, t01, -SI - SJ, 1.0f)
+    HP_DIAG(2, t01, SI - SJ, -1.0f)
+    HP_DIAG(3, t01, -SI + SJ, -1.0f)
+    HP_DIAG(4, t02, SI + 1, 1.0f)
+    HP_DIAG(5, t02, -SI - 1, 1.0f)
+    HP_DIAG(6, t02, SI - 1, -1.0f)
+    HP_DIAG(7, t02, -SI + 1, -1.0f)
+    HP_DIAG(8, t12, SJ + 1, 1.0f)
+    HP_DIAG(9, t12, -SJ - 1, 1.0f)
+    HP_DIAG(10, t12, SJ - 1, -1.0f)
+    HP_DIAG(11, t12, -SJ + 1, -1.0f)
+#undef HP_DIAG
+  }
+  if (tag & HP_TAG_PMJ) {
+    const float* __restrict__ Wpk = odd ? a.pk_Vs1 : a.pk_Vs0;
+    const int r = a.pmj_row[slot];
+    for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
+      acc += a.pmj_coef[q] * (Wpk[a.pmj_pk[q]] - Vc);
+  }
+  return fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
+}
+
+// Everything a tissue voxel does once V_{i+1} = Vn is known (mode 0): the
+// threshold-crossing test against V_i = Vprev, the Vm / surface snapshots,
+// then the ionic half of step i+1 and the stores of state and W_{i+1}.
+// Mode 1 (prologue) runs only the ionic half of step 0 on Vn = V_0.
+__device__ __forceinline__ void voxel_finish(const MonoArgs& a, int64_t slot, uint32_t tag,
+                                             int ph, float Vn, float Vprev, CellState& cs,
+                                             int64_t step, int mode, int64_t vm_frame,
+                                             int64_t anim_frame, int var, float* Wout) {
+  int64_t istep = 0;
+  if (mode == 0) {
+    // threshold crossings between the snapshots labelled t_{i-1} and t_i
+    if (step >= 1) {
+      const bool was_act = Vprev >= a.act_thr, is_act = Vn >= a.act_thr;
+      const bool was_dea = Vprev >= a.deact_thr, is_dea = Vn >= a.deact_thr;
+      if ((!was_act && is_act) || (was_dea && !is_dea)) {
+        const float t0 = (float)((double)(step - 1) * a.dt_d);
+        const float t1 = (float)((double)step * a.dt_d);
+        if (!was_act && is_act)
+          record_event(a.act_t, a.act_n, slot, a.n_slots, a.max_events, a.act_thr, Vprev, Vn, t0,
+                       t1);
+        if (was_dea && !is_dea)
+          record_event(a.deact_t, a.deact_n, slot, a.n_slots, a.max_events, a.deact_thr, Vprev,
+                       Vn, t0, t1);
+      }
+    }
+    a.Vpost[slot] = Vn;
+    if (vm_frame >= 0) a.vm_snap[vm_frame * a.n_myo + a.node_of_slot[slot]] = Vn;
+    if ((tag & HP_TAG_SURF) && anim_frame >= 0)
+      a.surf_frames[anim_frame * a.n_surf + a.surf_of_slot[slot]] = Vn;
+    istep = step + 1;
+  }
+  // ionic half of step istep on V = Vn
+  const CellParams cp = pheno_params(ph, a.var_gks[var], a.var_gkr[var]);
+  const float Iion = ttp06_step(Vn, cs, a.dt, cp);
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
+  const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep);
+  Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
 // Blocks per SM the register budget is sized for (8 x 128 threads -> 64 regs).
 template <int BV>
 struct MinBlocks {
   static constexpr int value = BV <= 128 ? 8 : (BV <= 256 ? 4 : 2);
 };
 
+// One brick per CTA, thread per voxel, halo tiles gathered with plain loads.
+// Used for the prologue (mode 1) and where the pipelined kernel does not fit.
 template <int BI, int BJ, int BK, bool ANISO>
 __global__ void __launch_bounds__(BI * BJ * BK, MinBlocks<BI * BJ * BK>::value)
 mono_step_kernel(MonoArgs a, int step_off, int mode) {
@@ -222,7 +328,7 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
   const int b = blockIdx.x;
   const bool odd = step & 1;
   const float* __restrict__ Win = odd ? a.Vs1 : a.Vs0;
-  float* __restrict__ Wout = odd ? a.Vs0 : a.Vs1;
+  float* __restrict__ Wout = mode == 0 ? (odd ? a.Vs0 : a.Vs1) : a.Vs0;
 
   __shared__ int nb27[27];
   __shared__ int64_t s_vm_frame, s_anim_frame;
@@ -260,98 +366,221 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
 
   const int ph = tag & HP_TAG_PHENO_MASK;
   if (ph == 0) return;
-
-  float Vn;
-  int64_t istep;
+  float Vn = Vprev;
   if (mode == 0) {
     const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
     const int c = (li + 1) * SI + (lj + 1) * SJ + (lk + 1);
-    const float Vc = tV[c];
-    float acc = 0.0f;
-    const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
-    if constexpr (!ANISO) {
-      float s = 0.0f;
-      if (fb & 1u) s += tV[c + SI] - Vc;
-      if (fb & 2u) s += tV[c - SI] - Vc;
-      if (fb & 4u) s += tV[c + SJ] - Vc;
-      if (fb & 8u) s += tV[c - SJ] - Vc;
-      if (fb & 16u) s += tV[c + 1] - Vc;
-      if (fb & 32u) s += tV[c - 1] - Vc;
-      acc = a.iso_coef * s;
-    } else {
-      const float* tWx = tW;
-      const float* tWy = tW + G::N;
-      const float* tWz = tW + 2 * G::N;
-      if (fb & 1u) acc += tWx[c] * (tV[c + SI] - Vc);
-      if (fb & 2u) acc += tWx[c - SI] * (tV[c - SI] - Vc);
-      if (fb & 4u) acc += tWy[c] * (tV[c + SJ] - Vc);
-      if (fb & 8u) acc += tWy[c - SJ] * (tV[c - SJ] - Vc);
-      if (fb & 16u) acc += tWz[c] * (tV[c + 1] - Vc);
-      if (fb & 32u) acc += tWz[c - 1] * (tV[c - 1] - Vc);
-      const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
-      const float* t01 = tD;
-      const float* t02 = tD + G::N;
-      const float* t12 = tD + 2 * G::N;
-      // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
-#define HP_DIAG(bit, T, OFF, SGN)                                            \
-  if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
-                                 (tV[c + (OFF)] - Vc);
-      HP_DIAG(0, t01, SI + SJ, 1.0f)
-      HP_DIAG(1, t01, -SI - SJ, 1.0f)
-      HP_DIAG(2, t01, SI - SJ, -1.0f)
-      HP_DIAG(3, t01, -SI + SJ, -1.0f)
-      HP_DIAG(4, t02, SI + 1, 1.0f)
-      HP_DIAG(5, t02, -SI - 1, 1.0f)
-      HP_DIAG(6, t02, SI - 1, -1.0f)
-      HP_DIAG(7, t02, -SI + 1, -1.0f)
-      HP_DIAG(8, t12, SJ + 1, 1.0f)
-      HP_DIAG(9, t12, -SJ - 1, 1.0f)
-      HP_DIAG(10, t12, SJ - 1, -1.0f)
-      HP_DIAG(11, t12, -SJ + 1, -1.0f)
-#undef HP_DIAG
-    }
-    if (tag & HP_TAG_PMJ) {
-      const float* __restrict__ Wpk = odd ? a.pk_Vs1 : a.pk_Vs0;
-      const int r = a.pmj_row[slot];
-      for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
-        acc += a.pmj_coef[q] * (Wpk[a.pmj_pk[q]] - Vc);
-    }
-    Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
-
-    // threshold crossings between the snapshots labelled t_{i-1} and t_i
-    if (step >= 1) {
-      const float Vp = Vprev;
-      const bool was_act = Vp >= a.act_thr, is_act = Vn >= a.act_thr;
-      const bool was_dea = Vp >= a.deact_thr, is_dea = Vn >= a.deact_thr;
-      if ((!was_act && is_act) || (was_dea && !is_dea)) {
-        const float t0 = (float)((double)(step - 1) * a.dt_d);
-        const float t1 = (float)((double)step * a.dt_d);
-        if (!was_act && is_act)
-          record_event(a.act_t, a.act_n, slot, a.n_slots, a.max_events, a.act_thr, Vp, Vn, t0, t1);
-        if (was_dea && !is_dea)
-          record_event(a.deact_t, a.deact_n, slot, a.n_slots, a.max_events, a.deact_thr, Vp, Vn,
-                       t0, t1);
-      }
-    }
-    a.Vpost[slot] = Vn;
-    if (s_vm_frame >= 0) a.vm_snap[s_vm_frame * a.n_myo + a.node_of_slot[slot]] = Vn;
-    if ((tag & HP_TAG_SURF) && s_anim_frame >= 0)
-      a.surf_frames[s_anim_frame * a.n_surf + a.surf_of_slot[slot]] = Vn;
-    istep = step + 1;
-  } else {
-    Vn = Vprev;
-    istep = 0;
-    Wout = a.Vs0;
+    Vn = diffuse<SI, SJ, G::N, ANISO>(a, tV, tW, tD, c, tag, slot, odd);
   }
-
-  // ionic half of step istep on V = Vn
   const int var = a.brick_variant ? a.brick_variant[b] : 0;
-  const CellParams cp = pheno_params(ph, a.var_gks[var], a.var_gkr[var]);
-  const float Iion = ttp06_step(Vn, cs, a.dt, cp);
+  voxel_finish(a, slot, tag, ph, Vn, Vprev, cs, step, mode, s_vm_frame, s_anim_frame, var, Wout);
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined persistent step (mode 0).
+//
+// Each CTA walks the work items blockIdx.x, blockIdx.x + gridDim.x, ...
+// (items [0, n_bricks) are bricks, the rest chunks of BV Purkinje nodes).
+// While it computes one brick, the data of its next brick -- the W tile with
+// its one-voxel halo, for the 19-point operator the face-weight and
+// off-diagonal tiles, the 18 TTP06 states, the tag and V_i -- streams into
+// the other shared-memory stage with cp.async, so HBM latency is hidden
+// behind the TTP06 arithmetic instead of being exposed once per brick.
+// Interior rows move as 16-byte copies; the halo elements follow a per-shape
+// copy table built on the host (tile position, field, neighbour direction,
+// offset in that brick), with zeros where the neighbour brick is absent.
+//
+// Tile layout in shared memory: k rows of RK = round_up(BK + 2, 4) floats,
+// local (li, lj, lk) at 4 + ((li + 1) * TJ + (lj + 1)) * RK + lk, so every
+// interior row starts on a 16-byte boundary; lk = -1 of a row sits in the
+// previous row's padding.
+template <int BI, int BJ, int BK>
+struct PipeGeom {
+  static constexpr int TI = BI + 2, TJ = BJ + 2, RK = ((BK + 2 + 3) / 4) * 4;
+  static constexpr int NT = TI * TJ * RK + 4;  // floats per tile (multiple of 4)
+  static constexpr int SI = TJ * RK, SJ = RK;
+  static constexpr int BV = BI * BJ * BK;
+  __host__ __device__ static constexpr int pos(int li, int lj, int lk) {
+    return 4 + ((li + 1) * TJ + (lj + 1)) * RK + lk;
+  }
+};
+
+template <int BI, int BJ, int BK, bool ANISO>
+struct PipeStage {
+  using G = PipeGeom<BI, BJ, BK>;
+  static constexpr int NF = ANISO ? 7 : 1;             // staged tiles
+  static constexpr int ST = NF * G::NT;                // 18 x BV states
+  static constexpr int TAG = ST + N_STATE * G::BV;     // BV tags
+  static constexpr int VP = TAG + G::BV;               // BV previous V
+  static constexpr int FLOATS = VP + G::BV;
+  static constexpr int NCHUNK = (N_STATE + 2) * G::BV / 4;  // 16-byte own-brick copies
+};
+
+// halo copy table entry: tile position | field << 11 | direction << 14 | offset << 19
+constexpr int HALO_POS_BITS = 11;
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <int BI, int BJ, int BK, bool ANISO>
+__device__ __forceinline__ void pipe_issue(const MonoArgs& a, float* stage, const uint32_t* tab,
+                                           int n_halo, const int* nb27, int b, const float* Win,
+                                           int tid) {
+  using G = PipeGeom<BI, BJ, BK>;
+  using P = PipeStage<BI, BJ, BK, ANISO>;
+  constexpr int BV = G::BV;
+  const int64_t ns = a.n_slots;
+  const int64_t base = (int64_t)b * BV;
+  // own brick: 18 states, tag, V_i (contiguous BV-float runs)
+  for (int q = tid; q < P::NCHUNK; q += BV) {
+    const int f = q / (BV / 4), o = (q % (BV / 4)) * 4;
+    const float* src = f < N_STATE ? a.state + (int64_t)f * ns
+                                   : (f == N_STATE ? (const float*)a.tag : a.Vpost);
+    cp_async16(stage + P::ST + f * BV + o, src + base + o);
+  }
+  // own brick rows of the staged tiles
+  for (int q = tid; q < P::NF * (BV / 4); q += BV) {
+    const int f = q / (BV / 4), o = (q % (BV / 4)) * 4;
+    const int gi = o / (BJ * BK), gj = (o / BK) % BJ, gk = o % BK;
+    const float* src = f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns);
+    cp_async16(stage + f * G::NT + G::pos(gi, gj, gk), src + base + o);
+  }
+  // halo elements
+  for (int e = tid; e < n_halo; e += BV) {
+    const uint32_t t = tab[e];
+    const int pos = t & ((1u << HALO_POS_BITS) - 1), f = (t >> 11) & 7, dir = (t >> 14) & 31,
+              off = (int)(t >> 19);
+    const int nb = nb27[dir];
+    float* dst = stage + f * G::NT + pos;
+    if (nb >= 0) {
+      const float* src = f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns);
+      cp_async4(dst, src + (int64_t)nb * BV + off);
+    } else {
+      *dst = 0.0f;
+    }
+  }
+}
+
+template <int BV>
+struct PipeMinBlocks {
+  static constexpr int value = BV <= 128 ? 4 : (BV <= 256 ? 2 : 1);
+};
+
+template <int BI, int BJ, int BK, bool ANISO>
+__global__ void __launch_bounds__(BI * BJ * BK, PipeMinBlocks<BI * BJ * BK>::value)
+mono_pipe_kernel(MonoArgs a, int step_off) {
+  using G = PipeGeom<BI, BJ, BK>;
+  using P = PipeStage<BI, BJ, BK, ANISO>;
+  constexpr int BV = G::BV;
+  extern __shared__ __align__(16) float smem[];
+  float* stages = smem;                                       // 2 x FLOATS
+  uint32_t* tab = (uint32_t*)(smem + 2 * P::FLOATS);          // n_halo
+  int* ring = (int*)(tab + ((a.n_halo + 3) & ~3));            // 2 x 27 neighbour lists
+  __shared__ int64_t s_vm_frame, s_anim_frame;
+
+  const int tid = threadIdx.x;
+  const int64_t step = *a.d_step + step_off;
+  const bool odd = step & 1;
+  const float* __restrict__ Win = odd ? a.Vs1 : a.Vs0;
+  float* __restrict__ Wout = odd ? a.Vs0 : a.Vs1;
+  const int G_ = gridDim.x;
+  const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
+
+  for (int e = tid; e < a.n_halo; e += BV) tab[e] = a.halo_tab[e];
+  if (tid == 0) {
+    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+  }
+  int cur = blockIdx.x;
+  if (cur < a.n_bricks && tid < 27) ring[tid] = a.nbr[(int64_t)cur * 27 + tid];
+  __syncthreads();
+  if (cur < a.n_bricks) {
+    pipe_issue<BI, BJ, BK, ANISO>(a, stages, tab, a.n_halo, ring, cur, Win, tid);
+    const int nx = cur + G_;
+    if (nx < a.n_bricks && tid < 27) cp_async4(ring + 27 + tid, a.nbr + (int64_t)nx * 27 + tid);
+  }
+  cp_async_commit();
+
+  for (int n = 0; cur < n_items; ++n, cur += G_) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int nxt = cur + G_;
+    if (nxt < a.n_bricks) {
+      pipe_issue<BI, BJ, BK, ANISO>(a, stages + ((n + 1) & 1) * P::FLOATS, tab, a.n_halo,
+                                    ring + ((n + 1) & 1) * 27, nxt, Win, tid);
+      const int nn = nxt + G_;
+      if (nn < a.n_bricks && tid < 27)
+        cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
+    }
+    cp_async_commit();
+    if (cur < a.n_bricks) {
+      const float* st = stages + (n & 1) * P::FLOATS;
+      const uint32_t tag = ((const uint32_t*)(st + P::TAG))[tid];
+      const int ph = tag & HP_TAG_PHENO_MASK;
+      if (ph != 0) {
+        const int64_t slot = (int64_t)cur * BV + tid;
+        const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
+        const float Vn = diffuse<G::SI, G::SJ, G::NT, ANISO>(
+            a, st, st + G::NT, st + 4 * G::NT, G::pos(li, lj, lk), tag, slot, odd);
+        CellState cs;
 #pragma unroll
-  for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
-  const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep);
-  Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+        for (int v = 0; v < N_STATE; ++v) cs.v[v] = st[P::ST + v * BV + tid];
+        const float Vprev = st[P::VP + tid];
+        const int var = a.brick_variant ? a.brick_variant[cur] : 0;
+        voxel_finish(a, slot, tag, ph, Vn, Vprev, cs, step, 0, s_vm_frame, s_anim_frame, var,
+                     Wout);
+      }
+    } else {
+      const int p = (cur - a.n_bricks) * BV + tid;
+      if (p < a.n_pk) purkinje_part(a, p, step, 0);
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
+}
+
+// Host: halo copy table of the pipelined kernel for one brick shape (the
+// union of the regions the stencil reads, minus the brick's own voxels).
+template <int BI, int BJ, int BK>
+static std::vector<uint32_t> pipe_halo_table(bool aniso) {
+  using G = PipeGeom<BI, BJ, BK>;
+  std::vector<uint32_t> t;
+  auto region = [&](int f, int i0, int i1, int j0, int j1, int k0, int k1) {
+    for (int li = i0; li < i1; ++li)
+      for (int lj = j0; lj < j1; ++lj)
+        for (int lk = k0; lk < k1; ++lk) {
+          const int di = li < 0 ? -1 : (li >= BI ? 1 : 0);
+          const int dj = lj < 0 ? -1 : (lj >= BJ ? 1 : 0);
+          const int dk = lk < 0 ? -1 : (lk >= BK ? 1 : 0);
+          if (di == 0 && dj == 0 && dk == 0) continue;
+          const int gi = li - di * BI, gj = lj - dj * BJ, gk = lk - dk * BK;
+          const uint32_t off = (uint32_t)((gi * BJ + gj) * BK + gk);
+          const uint32_t dir = (uint32_t)((di + 1) * 9 + (dj + 1) * 3 + (dk + 1));
+          t.push_back((uint32_t)G::pos(li, lj, lk) | ((uint32_t)f << 11) | (dir << 14) | (off << 19));
+        }
+  };
+  region(0, -1, BI + 1, -1, BJ + 1, -1, BK + 1);
+  if (aniso) {
+    region(1, -1, BI, 0, BJ, 0, BK);
+    region(2, 0, BI, -1, BJ, 0, BK);
+    region(3, 0, BI, 0, BJ, -1, BK);
+    region(4, -1, BI + 1, -1, BJ + 1, 0, BK);
+    region(5, -1, BI + 1, 0, BJ, -1, BK + 1);
+    region(6, 0, BI, -1, BJ + 1, -1, BK + 1);
+  }
+  return t;
 }
 
 __global__ void init_cells_kernel(float* state, float* Vpost, int64_t n, float v0) {
@@ -376,18 +605,24 @@ __global__ void fill_kernel(float* p, int64_t n, float v) {
 __global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
 
 typedef void (*StepFn)(MonoArgs, int, int);
+typedef void (*PipeFn)(MonoArgs, int);
+typedef std::vector<uint32_t> (*HaloFn)(bool);
 
 struct ShapeEntry {
   int bi, bj, bk;
   StepFn iso, aniso;
+  PipeFn pipe_iso, pipe_aniso;
+  HaloFn halo;
+  int stage_floats_iso, stage_floats_aniso;
 };
 
-static const ShapeEntry kShapes[] = {
-    {4, 4, 8, mono_step_kernel<4, 4, 8, false>, mono_step_kernel<4, 4, 8, true>},
-    {4, 8, 8, mono_step_kernel<4, 8, 8, false>, mono_step_kernel<4, 8, 8, true>},
-    {2, 4, 16, mono_step_kernel<2, 4, 16, false>, mono_step_kernel<2, 4, 16, true>},
-    {8, 8, 8, mono_step_kernel<8, 8, 8, false>, mono_step_kernel<8, 8, 8, true>},
-};
+#define HP_SHAPE(I, J, K)                                                                    \
+  {I, J, K, mono_step_kernel<I, J, K, false>, mono_step_kernel<I, J, K, true>,               \
+   mono_pipe_kernel<I, J, K, false>, mono_pipe_kernel<I, J, K, true>, pipe_halo_table<I, J, K>, \
+   PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS}
+static const ShapeEntry kShapes[] = {HP_SHAPE(4, 4, 8), HP_SHAPE(4, 8, 8), HP_SHAPE(2, 4, 16),
+                                     HP_SHAPE(8, 8, 8)};
+#undef HP_SHAPE
 
 }  // namespace hp
 
@@ -396,6 +631,9 @@ using namespace hp;
 struct HpMono {
   MonoArgs a;
   StepFn fn;
+  PipeFn pipe;       // persistent pipelined step, or null
+  int pipe_grid;     // CTAs of the persistent launch
+  size_t pipe_smem;  // dynamic shared memory per CTA
   int bv;
   int64_t n_steps, steps_done;
   int64_t n_vm_frames, n_anim_frames;
@@ -421,6 +659,12 @@ static hp_status al(HpMono* h, T** dst, size_t n) {
   return st;
 }
 
+#define HP_TRY_NODESTROY(x)            \
+  do {                                 \
+    hp_status _s = (x);                \
+    if (_s != HP_OK) return _s;        \
+  } while (0)
+
 #define HP_TRY(x)                      \
   do {                                 \
     hp_status _s = (x);                \
@@ -433,8 +677,52 @@ static hp_status al(HpMono* h, T** dst, size_t n) {
 static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) {
   const int grid = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   if (grid == 0) return HP_OK;
-  h->fn<<<grid, h->bv, 0, s>>>(h->a, step_off, mode);
+  if (mode == 0 && h->pipe)
+    h->pipe<<<h->pipe_grid, h->bv, h->pipe_smem, s>>>(h->a, step_off);
+  else
+    h->fn<<<grid, h->bv, 0, s>>>(h->a, step_off, mode);
   HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// Chooses the persistent pipelined step for a handle: uploads the shape's
+// halo copy table, raises the dynamic shared-memory limit and sizes the grid
+// to the resident CTAs of the whole GPU.  Without `required`, a shape whose
+// two stages do not fit keeps the per-brick kernel.
+static hp_status setup_pipe(HpMono* h, const ShapeEntry* se, int aniso, bool required,
+                            cudaStream_t s) {
+  const std::vector<uint32_t> tab = se->halo(aniso != 0);
+  const int floats = aniso ? se->stage_floats_aniso : se->stage_floats_iso;
+  const size_t smem = (2 * (size_t)floats + ((tab.size() + 3) & ~(size_t)3) + 54) * sizeof(float);
+  const PipeFn fn = aniso ? se->pipe_aniso : se->pipe_iso;
+  int dev = 0, max_optin = 0, n_sm = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  HP_CUDA_TRY(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  if (smem > (size_t)max_optin) {
+    if (!required) return HP_OK;
+    hp::set_error("hp_mono_create: pipelined kernel needs %zu B of shared memory, device has %d",
+                  smem, max_optin);
+    return HP_ERR_UNSUPPORTED;
+  }
+  HP_CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  int per_sm = 0;
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, h->bv, smem));
+  if (per_sm < 1) {
+    if (!required) return HP_OK;
+    hp::set_error("hp_mono_create: pipelined kernel cannot be resident");
+    return HP_ERR_UNSUPPORTED;
+  }
+  uint32_t* dtab = nullptr;
+  HP_TRY_NODESTROY(up(h, &dtab, tab.data(), tab.size(), s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));  // tab is a stack temporary
+  h->a.halo_tab = dtab;
+  h->a.n_halo = (int32_t)tab.size();
+  const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  h->pipe_grid = std::min(n_items, per_sm * n_sm);
+  h->pipe_smem = smem;
+  h->pipe = fn;
   return HP_OK;
 }
 
@@ -462,6 +750,7 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   HP_REQUIRE(d->n_pk == 0 || (d->pk_ptr && d->pk_stim), "hp_mono_create: missing Purkinje arrays");
   HP_REQUIRE(d->site_on, "hp_mono_create: missing site_on");
   HP_REQUIRE(d->n_myo >= 0 && (d->n_myo == 0 || d->slot_of_node), "hp_mono_create: missing slot_of_node");
+  HP_REQUIRE(d->kernel >= 0 && d->kernel <= 2, "hp_mono_create: kernel must be 0, 1 or 2");
 
   HpMono* h = new HpMono();
   h->graph = nullptr;
@@ -473,6 +762,9 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   memset(&a, 0, sizeof(a));
   h->bv = d->bi * d->bj * d->bk;
   h->fn = d->anisotropic ? se->aniso : se->iso;
+  h->pipe = nullptr;
+  h->pipe_grid = 0;
+  h->pipe_smem = 0;
   h->anisotropic = d->anisotropic;
   h->n_steps = d->n_steps;
   h->steps_done = 0;
@@ -603,6 +895,7 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
     HP_CUDA_TRY(cudaMemsetAsync(a.pk_Vs1, 0, d->n_pk * sizeof(float), s));
   }
   HP_CUDA_TRY(cudaGetLastError());
+  if (d->kernel != 1 && d->n_bricks > 0) HP_TRY(setup_pipe(h, se, d->anisotropic, d->kernel == 2, s));
   HP_TRY(launch_step(h, 0, 1, s));  // W_0 = ionic(V_0)
   // the caller's host arrays may be released once this returns
   HP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -655,6 +948,15 @@ extern "C" hp_status hp_mono_run(HpMono* h, int64_t n, int32_t graph_chunk, void
 }
 
 extern "C" int64_t hp_mono_steps_done(const HpMono* h) { return h ? h->steps_done : -1; }
+
+extern "C" hp_status hp_mono_kernel_info(const HpMono* h, int32_t* kernel, int32_t* grid,
+                                         int64_t* smem_bytes) {
+  HP_REQUIRE(h, "hp_mono_kernel_info: null handle");
+  if (kernel) *kernel = h->pipe ? HP_MONO_KERNEL_PIPELINED : HP_MONO_KERNEL_BRICK;
+  if (grid) *grid = h->pipe ? h->pipe_grid : h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  if (smem_bytes) *smem_bytes = h->pipe ? (int64_t)h->pipe_smem : 0;
+  return HP_OK;
+}
 
 extern "C" hp_status hp_mono_copy_vm(HpMono* h, int64_t f0, int64_t nf, float* dst,
                                      int32_t dst_on_device, void* stream) {

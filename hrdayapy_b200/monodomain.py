@@ -126,6 +126,7 @@ class MonoProblem:
     pk_variant: np.ndarray | None = None
     variant_gks: np.ndarray | None = None
     variant_gkr: np.ndarray | None = None
+    kernel: int = 0          # HP_MONO_KERNEL_AUTO / _BRICK (1) / _PIPELINED (2)
 
     @property
     def n_pk(self):
@@ -194,6 +195,7 @@ class MonoHandle:
         d.act_threshold = float(prob.act_threshold)
         d.deact_threshold = float(prob.deact_threshold)
         d.max_events = int(prob.max_events)
+        d.kernel = int(prob.kernel)
         self._desc = d
         if stream is None:
             # a dedicated stream: CUDA graphs cannot capture the legacy stream
@@ -213,6 +215,13 @@ class MonoHandle:
     def run(self, n: int, graph_chunk: int = 50):
         _lib.check(_lib.lib().hp_mono_run(self.h, int(n), int(graph_chunk), self.stream),
                    "hp_mono_run")
+
+    def kernel_info(self):
+        """(kernel id, grid CTAs, dynamic shared memory bytes) of the step."""
+        k, g, sm = C.c_int32(), C.c_int32(), C.c_int64()
+        _lib.check(_lib.lib().hp_mono_kernel_info(self.h, C.byref(k), C.byref(g), C.byref(sm)),
+                   "hp_mono_kernel_info")
+        return int(k.value), int(g.value), int(sm.value)
 
     @property
     def steps_done(self) -> int:

@@ -134,7 +134,15 @@ typedef struct {
   float act_threshold;          /* mV, upstroke crossing */
   float deact_threshold;        /* mV, downstroke crossing */
   int32_t max_events;           /* activation events kept per voxel (1..16) */
+
+  /* step kernel: HP_MONO_KERNEL_AUTO picks the pipelined one when its two
+   * shared-memory stages fit the device, else the per-brick one */
+  int32_t kernel;
 } HpMonoDesc;
+
+#define HP_MONO_KERNEL_AUTO 0
+#define HP_MONO_KERNEL_BRICK 1     /* one CTA per brick, plain halo loads */
+#define HP_MONO_KERNEL_PIPELINED 2 /* persistent CTAs, cp.async double-buffered bricks */
 
 typedef struct HpMono HpMono;
 
@@ -147,6 +155,9 @@ hp_status hp_mono_create(const HpMonoDesc *desc, HpMono **out, void *stream);
 hp_status hp_mono_run(HpMono *h, int64_t n, int32_t graph_chunk, void *stream);
 /* Steps done so far. */
 int64_t hp_mono_steps_done(const HpMono *h);
+/* Step kernel in use (HP_MONO_KERNEL_BRICK or _PIPELINED), its grid size
+ * and dynamic shared memory per CTA; any output may be NULL. */
+hp_status hp_mono_kernel_info(const HpMono *h, int32_t *kernel, int32_t *grid, int64_t *smem_bytes);
 /* Copies snapshots [f0, f0 + nf) (each n_myo floats, reference node order)
  * to dst; dst_on_device selects cudaMemcpyDeviceToDevice. */
 hp_status hp_mono_copy_vm(HpMono *h, int64_t f0, int64_t nf, float *dst,

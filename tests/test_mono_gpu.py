@@ -19,7 +19,7 @@ def _rms(a, b):
     return float(np.sqrt(np.mean((np.asarray(a, np.float64) - b) ** 2)))
 
 
-def _run_gpu(args, kw, fibre=None, **extra):
+def _run_gpu(args, kw, fibre=None, kernel=0, **extra):
     from hrdayapy_b200 import monodomain as M
     nodes, el, act, S, phi = args
     aniso = fibre is not None
@@ -29,7 +29,10 @@ def _run_gpu(args, kw, fibre=None, **extra):
     prob, info = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=aniso,
                            vm_save_dt=kw["dt"], act_threshold=-20.0, deact_threshold=-20.0,
                            **{**kwx, **extra})
+    prob.kernel = kernel
     sim = M.MonoHandle(prob)
+    if kernel:
+        assert sim.kernel_info()[0] == kernel
     sim.run(prob.n_steps, graph_chunk=50)
     vm = sim.vm_frames()
     a, na, d, nd = sim.events()
@@ -61,11 +64,12 @@ def test_aniso_purkinje_vs_upstream_golden(golden):
     assert np.max(np.abs(a[0] - ref)) <= ACT_TOL
 
 
+@pytest.mark.parametrize("kernel", [1, 2])
 @pytest.mark.parametrize("brick", [(4, 4, 8), (4, 8, 8), (2, 4, 16), (8, 8, 8)])
-def test_ragged_vs_oracle(brick):
+def test_ragged_vs_oracle(brick, kernel):
     from oracle import mono as orc
     args, fibre, kw = cases.ragged_aniso_case(T=25.0)
-    prob, info, vm, a, na = _run_gpu(args, kw, fibre=fibre, brick=brick)
+    prob, info, vm, a, na = _run_gpu(args, kw, fibre=fibre, brick=brick, kernel=kernel)
     nodes, el, act, S, phi = args
     r = orc.run(nodes, el, act, S, phi, fibre_dir=fibre, anisotropic=True, vm_save_dt=kw["dt"],
                 **kw)
@@ -77,6 +81,22 @@ def test_ragged_vs_oracle(brick):
     assert ok.sum() > 0.5 * len(ok)
     assert (na[ok] >= 1).all() and (na[~ok] == 0).all()
     assert np.max(np.abs(a[0][ok] - ra[ok, 0])) <= ACT_TOL
+
+
+@pytest.mark.parametrize("aniso", [False, True])
+@pytest.mark.parametrize("brick", [(4, 4, 8), (4, 8, 8), (2, 4, 16), (8, 8, 8)])
+def test_pipelined_and_brick_kernels_identical(brick, aniso):
+    """The persistent cp.async kernel and the per-brick kernel do the same
+    arithmetic in the same order: snapshots and events agree bit for bit."""
+    if aniso:
+        args, fibre, kw = cases.ragged_aniso_case(T=6.0)
+    else:
+        args, kw = cases.iso_case()
+        kw, fibre = dict(kw, T=6.0), None
+    res = [_run_gpu(args, kw, fibre=fibre, brick=brick, kernel=k) for k in (1, 2)]
+    np.testing.assert_array_equal(res[0][2], res[1][2])
+    np.testing.assert_array_equal(res[0][3], res[1][3])
+    np.testing.assert_array_equal(res[0][4], res[1][4])
 
 
 def test_graph_and_direct_launch_agree():
