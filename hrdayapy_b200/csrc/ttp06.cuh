@@ -9,11 +9,18 @@
 //   * FP32 instead of FP64;
 //   * constant divisors are folded into multipliers, and exponentials that
 //     the reference evaluates twice are shared (exp((V+30)/10) in tau_f and
-//     tau_f2, exp((-45-V)/10) etc. are separate in the reference but the
-//     values are identical);
+//     tau_f2; exp((gamma-1) V F/RT) = exp(gamma V F/RT) exp(-V F/RT));
+//   * quotients are merged so that each rate needs at most one reciprocal
+//     (the special-function unit is the scarce pipe of this kernel): a
+//     product or sum of logistic terms is written over a common denominator,
+//     the Rush-Larsen factor exp(-dt/tau) is formed from dt/tau directly
+//     where 1/tau is a sum of rates (h, j) or a product of logistic
+//     denominators (m, Xr1, Xr2), log(a/b) is log(a) - log(b) with the
+//     constant's logarithm folded, and buffer factors 1/(1 + B K/(c+K)^2)
+//     are (c+K)^2 / ((c+K)^2 + B K);
 //   * exp2V - 1 in I_CaL is evaluated with expm1f, which is the same
 //     quantity with less cancellation near V = 15 mV (the reference's FP64
-//     has the digits to spare; FP32 does not).
+//     has the digits to spare; FP32 does not), and exp2V as that plus one.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -48,8 +55,9 @@ __device__ __forceinline__ float hexp(float x) { return expf(x); }
 __device__ __forceinline__ float hlog(float x) { return logf(x); }
 #endif
 
-__device__ __forceinline__ float rl_gate(float x, float xinf, float tau, float dt) {
-  return xinf - (xinf - x) * hexp(-dt / tau);
+// Rush-Larsen update with the exponent given as dt/tau.
+__device__ __forceinline__ float rl_gate(float x, float xinf, float dt_over_tau) {
+  return xinf - (xinf - x) * hexp(-dt_over_tau);
 }
 
 __device__ __forceinline__ float sig(float x) {  // 1 / (1 + exp(x))
@@ -63,11 +71,11 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   constexpr double Rg = 8314.472, Tk = 310.0, Fc = 96485.3415;
   constexpr float RTF = (float)(Rg * Tk / Fc);
   constexpr float FRT = (float)(Fc / (Rg * Tk));
-  constexpr float Ko = 5.4f, Nao = 140.0f, Cao = 2.0f;
+  constexpr float Cao = 2.0f;
   constexpr float g_Na = 14.838f, g_K1 = 5.405f, g_bna = 0.00029f, g_bca = 0.000592f;
-  constexpr float g_pCa = 0.1238f, g_pK = 0.0146f, P_NaK = 2.724f, K_mk = 1.0f;
+  constexpr float g_pCa = 0.1238f, g_pK = 0.0146f, P_NaK = 2.724f, K_mk = 1.0f, Ko = 5.4f;
   constexpr float K_mNa = 40.0f, K_NaCa = 1000.0f, K_sat = 0.1f, alpha_ = 2.5f;
-  constexpr float gamma_ = 0.35f, Km_Ca = 1.38f, Km_Nai = 87.5f, P_kna = 0.03f;
+  constexpr float gamma_ = 0.35f, P_kna = 0.03f;
   constexpr float K_pCa = 0.0005f;
   constexpr float k1p = 0.15f, k2p = 0.045f, k3 = 0.06f, k4 = 0.005f, EC = 1.5f;
   constexpr float max_sr = 2.5f, min_sr = 1.0f, V_rel = 0.102f, V_xfer = 0.0038f;
@@ -88,7 +96,9 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
       (float)((87.5 * 87.5 * 87.5 + 140.0 * 140.0 * 140.0) * (1.38 + 2.0));
   constexpr float Nao3 = 140.0f * 140.0f * 140.0f;
   constexpr float NaK_k = P_NaK * Ko / (Ko + K_mk);
-  constexpr float E_Ks_num = Ko + P_kna * Nao;
+  // logarithms of Nao = 140, Ko = 5.4, Ko + P_kna Nao = 9.6 and Cao = 2 (mM)
+  constexpr float LN_NAO = 4.941642422609304f, LN_KO = 1.6863989535702288f;
+  constexpr float LN_KS = 2.2617630984737906f, LN_CAO = 0.6931471805599453f;
   // sqrt(Ko / 5.4) == 1 for Ko = 5.4
   constexpr float sqko = 1.0f;
 
@@ -99,96 +109,121 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   const float Rp = c.v[S_RPRIME];
 
   // reversal potentials
-  const float E_Na = RTF * hlog(Nao / Nai);
-  const float E_K = RTF * hlog(Ko / Ki);
-  const float E_Ks = RTF * hlog(E_Ks_num / (Ki + P_kna * Nai));
-  const float E_Ca = (0.5f * RTF) * hlog(Cao / Cai);
+  const float E_Na = RTF * (LN_NAO - hlog(Nai));
+  const float E_K = RTF * (LN_KO - hlog(Ki));
+  const float E_Ks = RTF * (LN_KS - hlog(Ki + P_kna * Nai));
+  const float E_Ca = (0.5f * RTF) * (LN_CAO - hlog(Cai));
 
-  // INa
+  // INa.  tau_m = alpha_m beta_m with alpha_m = 1/(1+e_am) and
+  // beta_m = 0.1/(1+e_b1) + 0.1/(1+e_b2) = 0.1 (2+e_b1+e_b2) / ((1+e_b1)(1+e_b2))
   float t1 = sig((-56.86f - V) * (1.0f / 9.03f));
   const float m_inf = t1 * t1;
-  const float alpha_m = sig((-60.0f - V) * 0.2f);
-  const float beta_m = 0.1f * sig((V + 35.0f) * 0.2f) + 0.1f * sig((V - 50.0f) * 0.005f);
-  const float tau_m = alpha_m * beta_m;
+  const float e_am = hexp((-60.0f - V) * 0.2f);
+  const float e_b1 = hexp((V + 35.0f) * 0.2f);
+  const float e_b2 = hexp((V - 50.0f) * 0.005f);
+  const float dtr_m = dt * (1.0f + e_am) * (1.0f + e_b1) * (1.0f + e_b2) /
+                      (0.1f * (2.0f + e_b1 + e_b2));
   t1 = sig((V + 71.55f) * (1.0f / 7.43f));
   const float h_inf = t1 * t1;
-  float alpha_h, beta_h, alpha_j, beta_j;
+  // 1/tau_h = alpha_h + beta_h, 1/tau_j = alpha_j + beta_j (+1e-30)
+  float rate_h, rate_j;
   if (V < -40.0f) {
-    alpha_h = 0.057f * hexp(-(V + 80.0f) * (1.0f / 6.8f));
-    beta_h = 2.7f * hexp(0.079f * V) + 3.1e5f * hexp(0.3485f * V);
-    alpha_j = ((-25428.0f * hexp(0.2444f * V) - 6.948e-6f * hexp(-0.04391f * V)) *
-               (V + 37.78f)) * sig(0.311f * (V + 79.23f));
-    beta_j = 0.02424f * hexp(-0.01052f * V) * sig(-0.1378f * (V + 40.14f));
+    rate_h = 0.057f * hexp(-(V + 80.0f) * (1.0f / 6.8f)) + 2.7f * hexp(0.079f * V) +
+             3.1e5f * hexp(0.3485f * V);
+    const float ea = hexp(0.311f * (V + 79.23f));    // alpha_j = Aj / (1 + ea)
+    const float eb = hexp(-0.1378f * (V + 40.14f));  // beta_j = Bj / (1 + eb)
+    const float Aj = (-25428.0f * hexp(0.2444f * V) - 6.948e-6f * hexp(-0.04391f * V)) *
+                     (V + 37.78f);
+    const float Bj = 0.02424f * hexp(-0.01052f * V);
+    rate_j = (Aj * (1.0f + eb) + Bj * (1.0f + ea)) / ((1.0f + ea) * (1.0f + eb));
   } else {
-    alpha_h = 0.0f;
-    beta_h = 0.77f / (0.13f * (1.0f + hexp((V + 10.66f) * (-1.0f / 11.1f))));
-    alpha_j = 0.0f;
-    beta_j = 0.6f * hexp(0.057f * V) * sig(-0.1f * (V + 32.0f));
+    rate_h = (0.77f / 0.13f) / (1.0f + hexp((V + 10.66f) * (-1.0f / 11.1f)));
+    rate_j = 0.6f * hexp(0.057f * V) / (1.0f + hexp(-0.1f * (V + 32.0f)));
   }
-  const float tau_h = 1.0f / (alpha_h + beta_h + 1e-30f);
-  const float tau_j = 1.0f / (alpha_j + beta_j + 1e-30f);
+  const float dtr_h = dt * (rate_h + 1e-30f);
+  const float dtr_j = dt * (rate_j + 1e-30f);
   const float i_Na = g_Na * m * m * m * h * j * (V - E_Na);
 
-  // IKr
+  // IKr.  tau_xr1 = 2700 / ((1+e_m45)(1+e_x1)), tau_xr2 = 3.36 / ((1+e_x2)(1+e_x3))
   const float xr1_inf = sig((-26.0f - V) * (1.0f / 7.0f));
   const float e_m45 = hexp((-45.0f - V) * 0.1f);
-  const float e_p30_10 = hexp((V + 30.0f) * 0.1f);  // shared by tau_f, tau_f2
-  const float tau_xr1 = 450.0f / (1.0f + e_m45) * 6.0f * sig((V + 30.0f) * (1.0f / 11.5f));
+  const float e_p30 = hexp((V + 30.0f) * 0.1f);  // shared by tau_f, tau_f2
+  const float dtr_xr1 = dt * (1.0f + e_m45) * (1.0f + hexp((V + 30.0f) * (1.0f / 11.5f))) *
+                        (1.0f / 2700.0f);
   const float xr2_inf = sig((V + 88.0f) * (1.0f / 24.0f));
-  const float tau_xr2 = 3.0f * sig((-60.0f - V) * 0.05f) * 1.12f * sig((V - 60.0f) * 0.05f);
+  const float dtr_xr2 = dt * (1.0f + hexp((-60.0f - V) * 0.05f)) *
+                        (1.0f + hexp((V - 60.0f) * 0.05f)) * (1.0f / 3.36f);
   const float i_Kr = p.g_Kr * sqko * Xr1 * Xr2 * (V - E_K);
 
-  // IKs
+  // IKs.  tau_xs = 1400 q / (1+e) + 80 = (1400 q + 80 (1+e)) / (1+e)
   const float xs_inf = sig((-5.0f - V) * (1.0f / 14.0f));
-  const float axs = 1400.0f * rsqrtf(1.0f + hexp((5.0f - V) * (1.0f / 6.0f)));
-  const float bxs = sig((V - 35.0f) * (1.0f / 15.0f));
-  const float tau_xs = axs * bxs + 80.0f;
+  const float q_xs = rsqrtf(1.0f + hexp((5.0f - V) * (1.0f / 6.0f)));
+  const float e_xs = hexp((V - 35.0f) * (1.0f / 15.0f));
+  const float dtr_xs = dt * (1.0f + e_xs) / (1400.0f * q_xs + 80.0f * (1.0f + e_xs));
   const float i_Ks = p.g_Ks * Xs * Xs * (V - E_Ks);
 
-  // IK1
+  // IK1.  xk1 = ak1 / (ak1 + bk1) with ak1 = 0.1/(1+e1), bk1 = nb/(1+e4)
+  // = 0.1 (1+e4) / (0.1 (1+e4) + nb (1+e1)); exponents bounded so that the
+  // merged form stays finite for any state
   const float VmEK = V - E_K;
-  const float ak1 = 0.1f * sig(0.06f * (VmEK - 200.0f));
-  const float bk1 = (3.0f * hexp(2e-4f * (VmEK + 100.0f)) + hexp(0.1f * (VmEK - 10.0f))) *
-                    sig(-0.5f * VmEK);
-  const float xk1_inf = ak1 / (ak1 + bk1);
+  const float e1 = hexp(fminf(0.06f * (VmEK - 200.0f), 80.0f));
+  const float nb = 3.0f * hexp(fminf(2e-4f * (VmEK + 100.0f), 80.0f)) +
+                   hexp(fminf(0.1f * (VmEK - 10.0f), 80.0f));
+  const float a4 = 0.1f * (1.0f + hexp(fminf(-0.5f * VmEK, 80.0f)));
+  const float xk1_inf = a4 / (a4 + nb * (1.0f + e1));
   const float i_K1 = g_K1 * sqko * xk1_inf * VmEK;
 
   // Ito
-  float s_inf, tau_s;
+  float s_inf, dtr_s;
   if (p.endo_s) {
     s_inf = sig((V + 28.0f) * 0.2f);
     const float a = V + 67.0f;
-    tau_s = 1000.0f * hexp(-a * a * 0.001f) + 8.0f;
+    dtr_s = dt / (1000.0f * hexp(-a * a * 0.001f) + 8.0f);
   } else {
+    // tau_s = g + 5/(1+e) + 3 = ((g+3)(1+e) + 5) / (1+e)
     s_inf = sig((V + 20.0f) * 0.2f);
     const float a = V + 45.0f;
-    tau_s = 85.0f * hexp(-a * a * (1.0f / 320.0f)) + 5.0f * sig((V - 20.0f) * 0.2f) + 3.0f;
+    const float g = 85.0f * hexp(-a * a * (1.0f / 320.0f));
+    const float e = hexp((V - 20.0f) * 0.2f);
+    dtr_s = dt * (1.0f + e) / ((g + 3.0f) * (1.0f + e) + 5.0f);
   }
   const float r_inf = sig((20.0f - V) * (1.0f / 6.0f));
   const float a40 = V + 40.0f;
-  const float tau_r = 9.5f * hexp(-a40 * a40 * (1.0f / 1800.0f)) + 0.8f;
+  const float dtr_r = dt / (9.5f * hexp(-a40 * a40 * (1.0f / 1800.0f)) + 0.8f);
   const float i_to = p.g_to * r * s * VmEK;
 
-  // ICaL
+  // ICaL.  tau_d = (1.4/(1+ea) + 0.25) 1.4/(1+eb) + 1/(1+ec)
+  //        = (1.4 (1.4 + 0.25 (1+ea)) (1+ec) + (1+ea)(1+eb)) / ((1+ea)(1+eb)(1+ec))
   const float d_inf = sig((-8.0f - V) * (1.0f / 7.5f));
-  const float tau_d = (1.4f * sig((-35.0f - V) * (1.0f / 13.0f)) + 0.25f) * 1.4f *
-                          sig((V + 5.0f) * 0.2f) +
-                      sig((50.0f - V) * 0.05f);
+  const float ea_d = 1.0f + hexp((-35.0f - V) * (1.0f / 13.0f));
+  const float eb_d = 1.0f + hexp((V + 5.0f) * 0.2f);
+  const float ec_d = 1.0f + hexp((50.0f - V) * 0.05f);
+  const float P_d = ea_d * eb_d;
+  const float dtr_d = dt * P_d * ec_d / (1.4f * (1.4f + 0.25f * ea_d) * ec_d + P_d);
+  // tau_f = G + 200/(1+eA) + 180/(1+eB) + 20, over the denominator (1+eA)(1+eB)
   const float f_inf = sig((V + 20.0f) * (1.0f / 7.0f));
   const float a27 = V + 27.0f;
-  const float tau_f = 1102.5f * hexp(-a27 * a27 * (1.0f / 225.0f)) +
-                      200.0f * sig((13.0f - V) * 0.1f) + 180.0f / (1.0f + e_p30_10) + 20.0f;
+  const float eB = 1.0f + e_p30;
+  const float eA = 1.0f + hexp((13.0f - V) * 0.1f);
+  const float D_f = eA * eB;
+  const float dtr_f = dt * D_f /
+                      ((1102.5f * hexp(-a27 * a27 * (1.0f / 225.0f)) + 20.0f) * D_f +
+                       200.0f * eB + 180.0f * eA);
+  // tau_f2 = G2 + 31/(1+eC) + 80/(1+eB)
   const float f2_inf = 0.67f * sig((V + 35.0f) * (1.0f / 7.0f)) + 0.33f;
-  const float tau_f2 = 562.0f * hexp(-a27 * a27 * (1.0f / 240.0f)) +
-                       31.0f * sig((25.0f - V) * 0.1f) + 80.0f / (1.0f + e_p30_10);
+  const float eC = 1.0f + hexp((25.0f - V) * 0.1f);
+  const float D_f2 = eC * eB;
+  const float dtr_f2 = dt * D_f2 /
+                       (562.0f * hexp(-a27 * a27 * (1.0f / 240.0f)) * D_f2 + 31.0f * eB +
+                        80.0f * eC);
+  // fCass: inf = 0.6/(1+cq) + 0.4, tau = 80/(1+cq) + 2 = (82 + 2 cq)/(1+cq)
   const float cq = (Cass * 20.0f) * (Cass * 20.0f);
-  const float inv_cq = 1.0f / (1.0f + cq);
-  const float fCass_inf = 0.6f * inv_cq + 0.4f;
-  const float tau_fCass = 80.0f * inv_cq + 2.0f;
+  const float fCass_inf = 0.6f / (1.0f + cq) + 0.4f;
+  const float dtr_fCass = dt * (1.0f + cq) / (82.0f + 2.0f * cq);
 
   const float x2v = 2.0f * (V - 15.0f) * FRT;
-  const float exp2V = hexp(x2v);
   float denom = expm1f(x2v);
+  const float exp2V = denom + 1.0f;
   if (fabsf(denom) < 1e-10f) denom = 1e-10f;
   const float i_CaL = g_CaL * d * f * f2 * fCass * CaL_k * (V - 15.0f) *
                       (0.25f * Cass * exp2V - Cao) / denom;
@@ -199,30 +234,33 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   const float i_pCa = g_pCa * Cai / (Cai + K_pCa);
   const float i_pK = g_pK * VmEK * sig((25.0f - V) * (1.0f / 5.98f));
   const float VF = V * FRT;
-  const float i_NaK = NaK_k * Nai / (Nai + K_mNa) /
-                      (1.0f + 0.1245f * hexp(-0.1f * VF) + 0.0353f * hexp(-VF));
+  const float e_mVF = hexp(-VF);
+  const float i_NaK = NaK_k * Nai /
+                      ((Nai + K_mNa) * (1.0f + 0.1245f * hexp(-0.1f * VF) + 0.0353f * e_mVF));
   const float eVg = hexp(gamma_ * VF);
-  const float eVgm1 = hexp((gamma_ - 1.0f) * VF);
+  const float eVgm1 = eVg * e_mVF;  // exp((gamma - 1) V F / RT)
   const float i_NaCa = K_NaCa * (eVg * Nai * Nai * Nai * Cao - eVgm1 * Nao3 * Cai * alpha_) /
                        (NaCa_den * (1.0f + K_sat * eVgm1));
 
   const float I_ion = i_K1 + i_to + i_Kr + i_Ks + i_CaL + i_NaK + i_Na + i_bNa + i_NaCa +
                       i_bCa + i_pCa + i_pK;
 
-  // SR calcium
-  const float ecs = EC / CaSR;
-  const float kcasr = max_sr - (max_sr - min_sr) / (1.0f + ecs * ecs);
-  const float k1 = k1p / kcasr, k2 = k2p * kcasr;
+  // SR calcium.  kcasr = max - (max-min) CaSR^2 / (CaSR^2 + EC^2);
+  // O = k1 Cass^2 R' / (k3 + k1 Cass^2) with k1 = k1p / kcasr
+  const float CaSR2 = CaSR * CaSR;
+  const float kcasr = max_sr - (max_sr - min_sr) * CaSR2 / (CaSR2 + EC * EC);
+  const float k2 = k2p * kcasr;
   const float Cass2 = Cass * Cass;
-  const float O = k1 * Cass2 * Rp / (k3 + k1 * Cass2 + 1e-30f);
+  const float O = k1p * Cass2 * Rp / (k3 * kcasr + k1p * Cass2);
   const float i_rel = V_rel * O * (CaSR - Cass);
-  const float i_up = Vmax_up / (1.0f + K_up * K_up / (Cai * Cai + 1e-30f));
+  const float c2 = Cai * Cai + 1e-30f;
+  const float i_up = Vmax_up * c2 / (c2 + K_up * K_up);
   const float i_leak = V_leak * (CaSR - Cai);
   const float i_xfer = V_xfer * (Cass - Cai);
   const float bc = Cai + K_buf_c, bsr = CaSR + K_buf_sr, bss = Cass + K_buf_ss;
-  const float bufc = 1.0f / (1.0f + Buf_c * K_buf_c / (bc * bc));
-  const float bufsr = 1.0f / (1.0f + Buf_sr * K_buf_sr / (bsr * bsr));
-  const float bufss = 1.0f / (1.0f + Buf_ss * K_buf_ss / (bss * bss));
+  const float bufc = bc * bc / (bc * bc + Buf_c * K_buf_c);
+  const float bufsr = bsr * bsr / (bsr * bsr + Buf_sr * K_buf_sr);
+  const float bufss = bss * bss / (bss * bss + Buf_ss * K_buf_ss);
 
   const float dNai = -(i_Na + i_bNa + 3.0f * i_NaK + 3.0f * i_NaCa) * inv_VcF;
   const float dKi = -(i_K1 + i_to + i_Kr + i_Ks + i_pK - 2.0f * i_NaK) * inv_VcF;
@@ -231,18 +269,18 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   const float dCaSR = bufsr * (i_up - i_rel - i_leak);
   const float dCass = bufss * (-i_CaL * inv_2VssF + i_rel * Vsr_Vss - i_xfer * Vc_Vss);
 
-  c.v[S_M] = rl_gate(m, m_inf, tau_m, dt);
-  c.v[S_H] = rl_gate(h, h_inf, tau_h, dt);
-  c.v[S_J] = rl_gate(j, h_inf, tau_j, dt);
-  c.v[S_XR1] = rl_gate(Xr1, xr1_inf, tau_xr1, dt);
-  c.v[S_XR2] = rl_gate(Xr2, xr2_inf, tau_xr2, dt);
-  c.v[S_XS] = rl_gate(Xs, xs_inf, tau_xs, dt);
-  c.v[S_D] = rl_gate(d, d_inf, tau_d, dt);
-  c.v[S_F] = rl_gate(f, f_inf, tau_f, dt);
-  c.v[S_F2] = rl_gate(f2, f2_inf, tau_f2, dt);
-  c.v[S_FCASS] = rl_gate(fCass, fCass_inf, tau_fCass, dt);
-  c.v[S_S] = rl_gate(s, s_inf, tau_s, dt);
-  c.v[S_R] = rl_gate(r, r_inf, tau_r, dt);
+  c.v[S_M] = rl_gate(m, m_inf, dtr_m);
+  c.v[S_H] = rl_gate(h, h_inf, dtr_h);
+  c.v[S_J] = rl_gate(j, h_inf, dtr_j);
+  c.v[S_XR1] = rl_gate(Xr1, xr1_inf, dtr_xr1);
+  c.v[S_XR2] = rl_gate(Xr2, xr2_inf, dtr_xr2);
+  c.v[S_XS] = rl_gate(Xs, xs_inf, dtr_xs);
+  c.v[S_D] = rl_gate(d, d_inf, dtr_d);
+  c.v[S_F] = rl_gate(f, f_inf, dtr_f);
+  c.v[S_F2] = rl_gate(f2, f2_inf, dtr_f2);
+  c.v[S_FCASS] = rl_gate(fCass, fCass_inf, dtr_fCass);
+  c.v[S_S] = rl_gate(s, s_inf, dtr_s);
+  c.v[S_R] = rl_gate(r, r_inf, dtr_r);
   c.v[S_RPRIME] = Rp + dt * (-k2 * Cass * Rp + k4 * (1.0f - Rp));
   c.v[S_NAI] = fmaxf(Nai + dt * dNai, 1e-3f);
   c.v[S_KI] = fmaxf(Ki + dt * dKi, 1e-3f);
