@@ -219,13 +219,13 @@ def run_ours(args):
             "config": {"workload": args.workload, "n_voxels": int(n_vox),
                        "n_purkinje": int(prob.n_pk), "dt_ms": prob.dt,
                        "time_steps_per_bench_step": fs, "brick": list(prob.layout.brick),
-                       "kernel": {1: "brick", 2: "pipelined"}[kinfo[0]], "grid": kinfo[1],
+                       "kernel": {1: "brick", 2: "pipelined", 3: "split"}[kinfo[0]], "grid": kinfo[1],
                        "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "bytes_per_voxel_step": bpv, "peak_source": peak_kind},
             "e2e": e2e,
-            "gpu_launches": int(args.steps * fs + args.steps),
+            "gpu_launches": int(args.steps * fs * (2 if kinfo[0] == 3 else 1) + args.steps),
             "clocks": clk.summary(),
             "check": {"vm_finite": bool(np.isfinite(vm_last).all()),
                       "vm_range_mV": [float(vm_last.min()), float(vm_last.max())]},
@@ -335,7 +335,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--kernel", type=int, default=0,
-                    help="monodomain step kernel: 0 auto, 1 per-brick, 2 pipelined")
+                    help="monodomain step kernel: 0 auto, 1 per-brick, 2 pipelined, 3 split")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -88,6 +88,10 @@ struct MonoArgs {
   // pipelined kernel: halo copy table of the brick shape
   int32_t n_halo;
   const uint32_t* halo_tab;
+  // split step: tissue slots in increasing order, the Purkinje threads start
+  // at n_active_pad (n_active rounded up to a warp); slot >> bv_shift = brick
+  int32_t n_active, n_active_pad, bv_shift;
+  const int32_t* active_slot;
 };
 
 // TTP06 phenotype table (ttp06_phenotype_constants.py:54-61), index = pheno-1.
@@ -168,31 +172,29 @@ __device__ __forceinline__ void load_region(float* __restrict__ tile,
 
 // Purkinje nodes: thread per node over the CSR adjacency (cable edges and
 // junction edges to myocardial slots), same skewed step as the voxels.
-__device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t step, int mode) {
+// Diffusion half: V_{i+1} of node p from W_i, stored in pk_Vpost (and the
+// animation frame of step i).
+__device__ __forceinline__ float purkinje_diffuse(const MonoArgs& a, int p, int64_t step) {
   const bool odd = step & 1;
   const float* __restrict__ Win = odd ? a.pk_Vs1 : a.pk_Vs0;
-  float* __restrict__ Wout = odd ? a.pk_Vs0 : a.pk_Vs1;
   const float* __restrict__ Wmyo = odd ? a.Vs1 : a.Vs0;
-  float Vn;
-  int64_t istep;
-  if (mode == 0) {
-    const float Vc = Win[p];
-    float acc = 0.0f;
-    for (int q = a.pk_ptr[p]; q < a.pk_ptr[p + 1]; ++q) {
-      const int j = a.pk_idx[q];
-      const float Vj = j >= 0 ? Win[j] : Wmyo[-(int64_t)j - 1];
-      acc += a.pk_coef[q] * (Vj - Vc);
-    }
-    Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
-    a.pk_Vpost[p] = Vn;
-    if (a.frame_every > 0 && step % a.frame_every == 0)
-      a.pk_frames[(step / a.frame_every) * (int64_t)a.n_pk + p] = Vn;
-    istep = step + 1;
-  } else {
-    Vn = a.pk_Vpost[p];
-    istep = 0;
-    Wout = a.pk_Vs0;
+  const float Vc = Win[p];
+  float acc = 0.0f;
+  for (int q = a.pk_ptr[p]; q < a.pk_ptr[p + 1]; ++q) {
+    const int j = a.pk_idx[q];
+    const float Vj = j >= 0 ? Win[j] : Wmyo[-(int64_t)j - 1];
+    acc += a.pk_coef[q] * (Vj - Vc);
   }
+  const float Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
+  a.pk_Vpost[p] = Vn;
+  if (a.frame_every > 0 && step % a.frame_every == 0)
+    a.pk_frames[(step / a.frame_every) * (int64_t)a.n_pk + p] = Vn;
+  return Vn;
+}
+
+// Ionic half of step istep of node p on V = Vn; stores its state and W.
+__device__ __forceinline__ void purkinje_ionic(const MonoArgs& a, int p, float Vn, int64_t istep,
+                                               float* __restrict__ Wout) {
   const int var = a.pk_variant ? a.pk_variant[p] : 0;
   const CellParams cp = pheno_params(1, a.var_gks[var], a.var_gkr[var]);  // Purkinje -> endo
   CellState c;
@@ -203,6 +205,16 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p] = c.v[v];
   const float Is = stim_current(a, a.pk_stim[p], istep);
   Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
+__device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t step, int mode) {
+  const bool odd = step & 1;
+  if (mode == 0) {
+    const float Vn = purkinje_diffuse(a, p, step);
+    purkinje_ionic(a, p, Vn, step + 1, odd ? a.pk_Vs0 : a.pk_Vs1);
+  } else {
+    purkinje_ionic(a, p, a.pk_Vpost[p], 0, a.pk_Vs0);
+  }
 }
 
 // Diffusion half of one voxel: V_{i+1} = clamp(W + sum coef (W_j - W), ...)
@@ -265,44 +277,59 @@ __device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, con
   return fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
 }
 
-// Everything a tissue voxel does once V_{i+1} = Vn is known (mode 0): the
-// threshold-crossing test against V_i = Vprev, the Vm / surface snapshots,
-// then the ionic half of step i+1 and the stores of state and W_{i+1}.
-// Mode 1 (prologue) runs only the ionic half of step 0 on Vn = V_0.
-__device__ __forceinline__ void voxel_finish(const MonoArgs& a, int64_t slot, uint32_t tag,
-                                             int ph, float Vn, float Vprev, CellState& cs,
-                                             int64_t step, int mode, int64_t vm_frame,
-                                             int64_t anim_frame, int var, float* Wout) {
-  int64_t istep = 0;
-  if (mode == 0) {
-    // threshold crossings between the snapshots labelled t_{i-1} and t_i
-    if (step >= 1) {
-      const bool was_act = Vprev >= a.act_thr, is_act = Vn >= a.act_thr;
-      const bool was_dea = Vprev >= a.deact_thr, is_dea = Vn >= a.deact_thr;
-      if ((!was_act && is_act) || (was_dea && !is_dea)) {
-        const float t0 = (float)((double)(step - 1) * a.dt_d);
-        const float t1 = (float)((double)step * a.dt_d);
-        if (!was_act && is_act)
-          record_event(a.act_t, a.act_n, slot, a.n_slots, a.max_events, a.act_thr, Vprev, Vn, t0,
-                       t1);
-        if (was_dea && !is_dea)
-          record_event(a.deact_t, a.deact_n, slot, a.n_slots, a.max_events, a.deact_thr, Vprev,
-                       Vn, t0, t1);
-      }
+// Outputs of a tissue voxel once V_{i+1} = Vn is known: the
+// threshold-crossing test against V_i = Vprev, Vpost and the Vm / surface
+// snapshots of step i.
+__device__ __forceinline__ void voxel_outputs(const MonoArgs& a, int64_t slot, uint32_t tag,
+                                              float Vn, float Vprev, int64_t step,
+                                              int64_t vm_frame, int64_t anim_frame) {
+  // threshold crossings between the snapshots labelled t_{i-1} and t_i
+  if (step >= 1) {
+    const bool was_act = Vprev >= a.act_thr, is_act = Vn >= a.act_thr;
+    const bool was_dea = Vprev >= a.deact_thr, is_dea = Vn >= a.deact_thr;
+    if ((!was_act && is_act) || (was_dea && !is_dea)) {
+      const float t0 = (float)((double)(step - 1) * a.dt_d);
+      const float t1 = (float)((double)step * a.dt_d);
+      if (!was_act && is_act)
+        record_event(a.act_t, a.act_n, slot, a.n_slots, a.max_events, a.act_thr, Vprev, Vn, t0,
+                     t1);
+      if (was_dea && !is_dea)
+        record_event(a.deact_t, a.deact_n, slot, a.n_slots, a.max_events, a.deact_thr, Vprev,
+                     Vn, t0, t1);
     }
-    a.Vpost[slot] = Vn;
-    if (vm_frame >= 0) a.vm_snap[vm_frame * a.n_myo + a.node_of_slot[slot]] = Vn;
-    if ((tag & HP_TAG_SURF) && anim_frame >= 0)
-      a.surf_frames[anim_frame * a.n_surf + a.surf_of_slot[slot]] = Vn;
-    istep = step + 1;
   }
-  // ionic half of step istep on V = Vn
+  a.Vpost[slot] = Vn;
+  if (vm_frame >= 0) a.vm_snap[vm_frame * a.n_myo + a.node_of_slot[slot]] = Vn;
+  if ((tag & HP_TAG_SURF) && anim_frame >= 0)
+    a.surf_frames[anim_frame * a.n_surf + a.surf_of_slot[slot]] = Vn;
+}
+
+// Ionic half of step istep of a tissue voxel on V = Vn: stores the state and
+// W_{istep} = Vn + dt/Cm (-Iion Cm + Istim).
+__device__ __forceinline__ void voxel_ionic(const MonoArgs& a, int64_t slot, uint32_t tag, int ph,
+                                            float Vn, CellState& cs, int64_t istep, int var,
+                                            float* __restrict__ Wout) {
   const CellParams cp = pheno_params(ph, a.var_gks[var], a.var_gkr[var]);
   const float Iion = ttp06_step(Vn, cs, a.dt, cp);
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
   const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep);
   Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
+// Everything a tissue voxel does once V_{i+1} = Vn is known (mode 0):
+// outputs of step i, then the ionic half of step i+1.  Mode 1 (prologue)
+// runs only the ionic half of step 0 on Vn = V_0.
+__device__ __forceinline__ void voxel_finish(const MonoArgs& a, int64_t slot, uint32_t tag,
+                                             int ph, float Vn, float Vprev, CellState& cs,
+                                             int64_t step, int mode, int64_t vm_frame,
+                                             int64_t anim_frame, int var, float* Wout) {
+  int64_t istep = 0;
+  if (mode == 0) {
+    voxel_outputs(a, slot, tag, Vn, Vprev, step, vm_frame, anim_frame);
+    istep = step + 1;
+  }
+  voxel_ionic(a, slot, tag, ph, Vn, cs, istep, var, Wout);
 }
 
 // Blocks per SM the register budget is sized for (8 x 128 threads -> 64 regs).
@@ -551,8 +578,174 @@ mono_pipe_kernel(MonoArgs a, int step_off) {
   cp_async_wait_all();
 }
 
-// Host: halo copy table of the pipelined kernel for one brick shape (the
-// union of the regions the stencil reads, minus the brick's own voxels).
+// ---------------------------------------------------------------------------
+// Split step: two launches per step over the same arrays.
+//
+// mono_diffuse_kernel (one CTA per brick, plus CTAs of BV Purkinje nodes)
+// forms V_{i+1} from W_i and its halo, records the crossings and snapshots of
+// step i and stores V_{i+1} in Vpost.  mono_ionic_kernel then runs the ionic
+// half of step i+1 with one thread per tissue slot, taken from the compact
+// list active_slot, so padding slots of partially filled bricks occupy no
+// lane, and without shared memory or barriers, so it runs at full occupancy.
+// Both do the fused kernels' arithmetic in the same order: results are
+// bit-identical to theirs.
+// Halo elements per thread of the diffusion kernel (copy-table entries
+// held in registers for the whole launch).
+template <int BI, int BJ, int BK, bool ANISO>
+struct DiffHalo {
+  static constexpr int BV = BI * BJ * BK;
+  // W: 6 faces + 12 edges; face weights: 3 faces; off-diagonal tiles: 2 face
+  // pairs + 4 edges each
+  static constexpr int W = 2 * (BJ * BK + BI * BK + BI * BJ) + (ANISO ? 4 * (BI + BJ + BK) : 0);
+  static constexpr int A = BJ * BK + BI * BK + BI * BJ +
+                           (2 * (BI * BK + BJ * BK) + 4 * BK) + (2 * (BJ * BK + BI * BJ) + 4 * BJ) +
+                           (2 * (BI * BK + BI * BJ) + 4 * BI);
+  static constexpr int N = ANISO ? W + A : W;
+  static constexpr int PER_THREAD = (N + BV - 1) / BV;
+};
+
+// Shared-memory stage of the diffusion kernel: the staged tiles, then the
+// brick's tags and V_i.
+template <int BI, int BJ, int BK, bool ANISO>
+struct DiffStage {
+  using G = PipeGeom<BI, BJ, BK>;
+  static constexpr int NF = ANISO ? 7 : 1;
+  static constexpr int TAG = NF * G::NT;
+  static constexpr int VP = TAG + G::BV;
+  static constexpr int FLOATS = VP + G::BV;
+  static constexpr int NCHUNK = (NF + 2) * G::BV / 4;  // 16-byte own-brick copies
+};
+
+template <int BI, int BJ, int BK, bool ANISO>
+__global__ void __launch_bounds__(BI * BJ * BK)
+mono_diffuse_kernel(MonoArgs a, int step_off) {
+  using G = PipeGeom<BI, BJ, BK>;
+  using H = DiffHalo<BI, BJ, BK, ANISO>;
+  using D = DiffStage<BI, BJ, BK, ANISO>;
+  constexpr int BV = G::BV, NF = D::NF, PT = H::PER_THREAD;
+  constexpr int QB = BV / 4;  // 16-byte chunks per brick row of one field
+  extern __shared__ __align__(16) float smem[];
+  float* stages = smem;                     // 2 x FLOATS
+  int* ring = (int*)(smem + 2 * D::FLOATS);  // 2 x 27 neighbour lists
+  __shared__ int64_t s_vm_frame, s_anim_frame;
+  const int64_t step = *a.d_step + step_off;
+  const bool odd = step & 1;
+  const float* __restrict__ Win = odd ? a.Vs1 : a.Vs0;
+  const int tid = threadIdx.x;
+  const int64_t ns = a.n_slots;
+  // this thread's halo copies for the whole launch: stage offset (field tile
+  // + position), neighbour direction, source (array + offset in the brick)
+  uint32_t hpos[PT], hdir[PT];
+  const float* hsrc[PT];
+#pragma unroll
+  for (int q = 0; q < PT; ++q) {
+    const int e = tid + q * BV;
+    const uint32_t t = e < a.n_halo ? a.halo_tab[e] : 0u;
+    const int f = (t >> 11) & 7;
+    hpos[q] = e < a.n_halo ? (uint32_t)(f * G::NT + (int)(t & ((1u << HALO_POS_BITS) - 1)))
+                           : 0xFFFFFFFFu;
+    hdir[q] = (t >> 14) & 31;
+    hsrc[q] = e >= a.n_halo ? Win
+                            : (f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)) +
+                                  (t >> 19);
+  }
+  auto issue = [&](float* st, const int* nb27, int b) {
+    const int64_t base = (int64_t)b * BV;
+#pragma unroll
+    for (int k = 0; k < (D::NCHUNK + BV - 1) / BV; ++k) {
+      const int q = tid + k * BV;
+      if (q < D::NCHUNK) {
+        const int f = q / QB, o = (q % QB) * 4;
+        const float* src = f == 0    ? Win
+                           : f < NF  ? (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)
+                           : f == NF ? (const float*)a.tag
+                                     : a.Vpost;
+        float* dst = f < NF ? st + f * G::NT + G::pos(o / (BJ * BK), (o / BK) % BJ, o % BK)
+                            : st + D::TAG + (f - NF) * BV + o;
+        cp_async16(dst, src + base + o);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      if (hpos[q] != 0xFFFFFFFFu) {
+        const int nb = nb27[hdir[q]];
+        if (nb >= 0)
+          cp_async4(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
+        else
+          st[hpos[q]] = 0.0f;
+      }
+    }
+  };
+  const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
+  const int c = G::pos(li, lj, lk);
+  const int G_ = gridDim.x;
+  const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
+  if (tid == 0) {
+    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+  }
+  int cur = blockIdx.x;
+  if (cur < a.n_bricks && tid < 27) ring[tid] = a.nbr[(int64_t)cur * 27 + tid];
+  __syncthreads();
+  if (cur < a.n_bricks) {
+    issue(stages, ring, cur);
+    const int nx = cur + G_;
+    if (nx < a.n_bricks && tid < 27) cp_async4(ring + 27 + tid, a.nbr + (int64_t)nx * 27 + tid);
+  }
+  cp_async_commit();
+  for (int n = 0; cur < n_items; ++n, cur += G_) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int nxt = cur + G_;
+    if (nxt < a.n_bricks) {
+      issue(stages + ((n + 1) & 1) * D::FLOATS, ring + ((n + 1) & 1) * 27, nxt);
+      const int nn = nxt + G_;
+      if (nn < a.n_bricks && tid < 27) cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
+    }
+    cp_async_commit();
+    if (cur < a.n_bricks) {
+      const float* st = stages + (n & 1) * D::FLOATS;
+      const uint32_t tag = ((const uint32_t*)(st + D::TAG))[tid];
+      if (tag & HP_TAG_PHENO_MASK) {
+        const int64_t slot = (int64_t)cur * BV + tid;
+        const float Vn = diffuse<G::SI, G::SJ, G::NT, ANISO>(
+            a, st, ANISO ? st + G::NT : st, ANISO ? st + 4 * G::NT : st, c, tag, slot, odd);
+        voxel_outputs(a, slot, tag, Vn, st[D::VP + tid], step, s_vm_frame, s_anim_frame);
+      }
+    } else {
+      const int p = (cur - a.n_bricks) * BV + tid;
+      if (p < a.n_pk) purkinje_diffuse(a, p, step);
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
+}
+
+__global__ void __launch_bounds__(128, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+  const int64_t step = *a.d_step + step_off;
+  const bool odd = step & 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n_active) {
+    const int64_t slot = a.active_slot[i];
+    const uint32_t tag = a.tag[slot];
+    const float Vn = a.Vpost[slot];
+    CellState cs;
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * a.n_slots + slot];
+    const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
+    voxel_ionic(a, slot, tag, tag & HP_TAG_PHENO_MASK, Vn, cs, step + 1, var,
+                odd ? a.Vs0 : a.Vs1);
+  } else {
+    const int p = i - a.n_active_pad;
+    if (p >= 0 && p < a.n_pk)
+      purkinje_ionic(a, p, a.pk_Vpost[p], step + 1, odd ? a.pk_Vs0 : a.pk_Vs1);
+  }
+}
+
+// Host: halo copy table of the pipelined and split-diffusion kernels for
+// one brick shape: the union of the tile elements the stencil reads, minus
+// the brick's own voxels (the 7-point operator reads face neighbours only,
+// the 19-point one faces and edges, neither the cube's corners).
 template <int BI, int BJ, int BK>
 static std::vector<uint32_t> pipe_halo_table(bool aniso) {
   using G = PipeGeom<BI, BJ, BK>;
@@ -564,7 +757,8 @@ static std::vector<uint32_t> pipe_halo_table(bool aniso) {
           const int di = li < 0 ? -1 : (li >= BI ? 1 : 0);
           const int dj = lj < 0 ? -1 : (lj >= BJ ? 1 : 0);
           const int dk = lk < 0 ? -1 : (lk >= BK ? 1 : 0);
-          if (di == 0 && dj == 0 && dk == 0) continue;
+          const int n_out = (di != 0) + (dj != 0) + (dk != 0);
+          if (n_out == 0 || n_out > (aniso ? 2 : 1)) continue;
           const int gi = li - di * BI, gj = lj - dj * BJ, gk = lk - dk * BK;
           const uint32_t off = (uint32_t)((gi * BJ + gj) * BK + gk);
           const uint32_t dir = (uint32_t)((di + 1) * 9 + (dj + 1) * 3 + (dk + 1));
@@ -605,21 +799,27 @@ __global__ void fill_kernel(float* p, int64_t n, float v) {
 __global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
 
 typedef void (*StepFn)(MonoArgs, int, int);
-typedef void (*PipeFn)(MonoArgs, int);
+typedef void (*PipeFn)(MonoArgs, int);  // also the diffusion half of the split step
 typedef std::vector<uint32_t> (*HaloFn)(bool);
 
 struct ShapeEntry {
   int bi, bj, bk;
   StepFn iso, aniso;
   PipeFn pipe_iso, pipe_aniso;
+  PipeFn diff_iso, diff_aniso;
   HaloFn halo;
   int stage_floats_iso, stage_floats_aniso;
+  int diff_cap_iso, diff_cap_aniso;  // halo entries the diffusion kernel holds
+  int diff_floats_iso, diff_floats_aniso;
 };
 
 #define HP_SHAPE(I, J, K)                                                                    \
   {I, J, K, mono_step_kernel<I, J, K, false>, mono_step_kernel<I, J, K, true>,               \
-   mono_pipe_kernel<I, J, K, false>, mono_pipe_kernel<I, J, K, true>, pipe_halo_table<I, J, K>, \
-   PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS}
+   mono_pipe_kernel<I, J, K, false>, mono_pipe_kernel<I, J, K, true>,                         \
+   mono_diffuse_kernel<I, J, K, false>, mono_diffuse_kernel<I, J, K, true>, pipe_halo_table<I, J, K>, \
+   PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS,                      \
+   DiffHalo<I, J, K, false>::PER_THREAD * I * J * K, DiffHalo<I, J, K, true>::PER_THREAD * I * J * K, \
+   DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS}
 static const ShapeEntry kShapes[] = {HP_SHAPE(4, 4, 8), HP_SHAPE(4, 8, 8), HP_SHAPE(2, 4, 16),
                                      HP_SHAPE(8, 8, 8)};
 #undef HP_SHAPE
@@ -634,6 +834,9 @@ struct HpMono {
   PipeFn pipe;       // persistent pipelined step, or null
   int pipe_grid;     // CTAs of the persistent launch
   size_t pipe_smem;  // dynamic shared memory per CTA
+  PipeFn diff;       // split step: diffusion half, or null
+  int diff_grid;     // its persistent grid
+  size_t diff_smem;  // and dynamic shared memory per CTA
   int bv;
   int64_t n_steps, steps_done;
   int64_t n_vm_frames, n_anim_frames;
@@ -677,7 +880,11 @@ static hp_status al(HpMono* h, T** dst, size_t n) {
 static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) {
   const int grid = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   if (grid == 0) return HP_OK;
-  if (mode == 0 && h->pipe)
+  if (mode == 0 && h->diff) {
+    h->diff<<<h->diff_grid, h->bv, h->diff_smem, s>>>(h->a, step_off);
+    const int n_ion = h->a.n_active_pad + h->a.n_pk;
+    if (n_ion > 0) mono_ionic_kernel<<<(n_ion + 127) / 128, 128, 0, s>>>(h->a, step_off);
+  } else if (mode == 0 && h->pipe)
     h->pipe<<<h->pipe_grid, h->bv, h->pipe_smem, s>>>(h->a, step_off);
   else
     h->fn<<<grid, h->bv, 0, s>>>(h->a, step_off, mode);
@@ -726,6 +933,50 @@ static hp_status setup_pipe(HpMono* h, const ShapeEntry* se, int aniso, bool req
   return HP_OK;
 }
 
+// Split step: the compact list of tissue slots for the ionic launch.
+static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d,
+                             cudaStream_t s) {
+  std::vector<int32_t> act;
+  const int64_t ns = h->a.n_slots;
+  act.reserve((size_t)ns);
+  for (int64_t sl = 0; sl < ns; ++sl)
+    if (d->tag[sl] & HP_TAG_PHENO_MASK) act.push_back((int32_t)sl);
+  int32_t* dact = nullptr;
+  HP_TRY_NODESTROY(up(h, &dact, act.data(), act.size(), s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));  // act is a stack temporary
+  int shift = 0;
+  while ((1 << shift) < h->bv) ++shift;
+  h->a.active_slot = dact;
+  h->a.n_active = (int32_t)act.size();
+  h->a.n_active_pad = (int32_t)((act.size() + 31) / 32 * 32);
+  h->a.bv_shift = shift;
+  h->diff = d->anisotropic ? se->diff_aniso : se->diff_iso;
+  // diffusion half: persistent CTAs over bricks, halo copy table per shape
+  const std::vector<uint32_t> tab = se->halo(d->anisotropic != 0);
+  if ((int)tab.size() > (d->anisotropic ? se->diff_cap_aniso : se->diff_cap_iso)) {
+    hp::set_error("hp_mono_create: halo table of %zu entries exceeds the diffusion kernel's %d",
+                  tab.size(), d->anisotropic ? se->diff_cap_aniso : se->diff_cap_iso);
+    return HP_ERR_UNSUPPORTED;
+  }
+  uint32_t* dtab = nullptr;
+  HP_TRY_NODESTROY(up(h, &dtab, tab.data(), tab.size(), s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));  // tab is a stack temporary
+  h->a.halo_tab = dtab;
+  h->a.n_halo = (int32_t)tab.size();
+  const size_t smem = (2 * (size_t)(d->anisotropic ? se->diff_floats_aniso : se->diff_floats_iso) +
+                       54) * sizeof(float);
+  int dev = 0, n_sm = 0, per_sm = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  HP_CUDA_TRY(cudaFuncSetAttribute((const void*)h->diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->diff, h->bv, smem));
+  h->diff_smem = smem;
+  const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  h->diff_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
+  return HP_OK;
+}
+
 extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* stream) {
   HP_REQUIRE(d && out, "hp_mono_create: null argument");
   *out = nullptr;
@@ -750,7 +1001,7 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   HP_REQUIRE(d->n_pk == 0 || (d->pk_ptr && d->pk_stim), "hp_mono_create: missing Purkinje arrays");
   HP_REQUIRE(d->site_on, "hp_mono_create: missing site_on");
   HP_REQUIRE(d->n_myo >= 0 && (d->n_myo == 0 || d->slot_of_node), "hp_mono_create: missing slot_of_node");
-  HP_REQUIRE(d->kernel >= 0 && d->kernel <= 2, "hp_mono_create: kernel must be 0, 1 or 2");
+  HP_REQUIRE(d->kernel >= 0 && d->kernel <= 3, "hp_mono_create: kernel must be 0..3");
 
   HpMono* h = new HpMono();
   h->graph = nullptr;
@@ -765,6 +1016,9 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   h->pipe = nullptr;
   h->pipe_grid = 0;
   h->pipe_smem = 0;
+  h->diff = nullptr;
+  h->diff_grid = 0;
+  h->diff_smem = 0;
   h->anisotropic = d->anisotropic;
   h->n_steps = d->n_steps;
   h->steps_done = 0;
@@ -895,7 +1149,11 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
     HP_CUDA_TRY(cudaMemsetAsync(a.pk_Vs1, 0, d->n_pk * sizeof(float), s));
   }
   HP_CUDA_TRY(cudaGetLastError());
-  if (d->kernel != 1 && d->n_bricks > 0) HP_TRY(setup_pipe(h, se, d->anisotropic, d->kernel == 2, s));
+  if (d->kernel == HP_MONO_KERNEL_SPLIT) {
+    HP_TRY(setup_split(h, se, d, s));
+  } else if (d->kernel != HP_MONO_KERNEL_BRICK && d->n_bricks > 0) {
+    HP_TRY(setup_pipe(h, se, d->anisotropic, d->kernel == HP_MONO_KERNEL_PIPELINED, s));
+  }
   HP_TRY(launch_step(h, 0, 1, s));  // W_0 = ionic(V_0)
   // the caller's host arrays may be released once this returns
   HP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -952,8 +1210,12 @@ extern "C" int64_t hp_mono_steps_done(const HpMono* h) { return h ? h->steps_don
 extern "C" hp_status hp_mono_kernel_info(const HpMono* h, int32_t* kernel, int32_t* grid,
                                          int64_t* smem_bytes) {
   HP_REQUIRE(h, "hp_mono_kernel_info: null handle");
-  if (kernel) *kernel = h->pipe ? HP_MONO_KERNEL_PIPELINED : HP_MONO_KERNEL_BRICK;
-  if (grid) *grid = h->pipe ? h->pipe_grid : h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  if (kernel)
+    *kernel = h->diff ? HP_MONO_KERNEL_SPLIT
+                      : (h->pipe ? HP_MONO_KERNEL_PIPELINED : HP_MONO_KERNEL_BRICK);
+  if (grid)
+    *grid = h->diff ? h->diff_grid
+                    : (h->pipe ? h->pipe_grid : h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv);
   if (smem_bytes) *smem_bytes = h->pipe ? (int64_t)h->pipe_smem : 0;
   return HP_OK;
 }

@@ -143,6 +143,7 @@ typedef struct {
 #define HP_MONO_KERNEL_AUTO 0
 #define HP_MONO_KERNEL_BRICK 1     /* one CTA per brick, plain halo loads */
 #define HP_MONO_KERNEL_PIPELINED 2 /* persistent CTAs, cp.async double-buffered bricks */
+#define HP_MONO_KERNEL_SPLIT 3     /* diffusion launch per brick + ionic launch per tissue slot */
 
 typedef struct HpMono HpMono;
 
@@ -155,7 +156,7 @@ hp_status hp_mono_create(const HpMonoDesc *desc, HpMono **out, void *stream);
 hp_status hp_mono_run(HpMono *h, int64_t n, int32_t graph_chunk, void *stream);
 /* Steps done so far. */
 int64_t hp_mono_steps_done(const HpMono *h);
-/* Step kernel in use (HP_MONO_KERNEL_BRICK or _PIPELINED), its grid size
+/* Step kernel in use (HP_MONO_KERNEL_BRICK, _PIPELINED or _SPLIT), its grid size
  * and dynamic shared memory per CTA; any output may be NULL. */
 hp_status hp_mono_kernel_info(const HpMono *h, int32_t *kernel, int32_t *grid, int64_t *smem_bytes);
 /* Copies snapshots [f0, f0 + nf) (each n_myo floats, reference node order)

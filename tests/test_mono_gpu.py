@@ -64,7 +64,7 @@ def test_aniso_purkinje_vs_upstream_golden(golden):
     assert np.max(np.abs(a[0] - ref)) <= ACT_TOL
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 @pytest.mark.parametrize("brick", [(4, 4, 8), (4, 8, 8), (2, 4, 16), (8, 8, 8)])
 def test_ragged_vs_oracle(brick, kernel):
     from oracle import mono as orc
@@ -85,18 +85,20 @@ def test_ragged_vs_oracle(brick, kernel):
 
 @pytest.mark.parametrize("aniso", [False, True])
 @pytest.mark.parametrize("brick", [(4, 4, 8), (4, 8, 8), (2, 4, 16), (8, 8, 8)])
-def test_pipelined_and_brick_kernels_identical(brick, aniso):
-    """The persistent cp.async kernel and the per-brick kernel do the same
-    arithmetic in the same order: snapshots and events agree bit for bit."""
+def test_step_kernels_identical(brick, aniso):
+    """The per-brick, persistent cp.async and split (diffusion + ionic)
+    kernels do the same arithmetic in the same order: snapshots and events
+    agree bit for bit."""
     if aniso:
         args, fibre, kw = cases.ragged_aniso_case(T=6.0)
     else:
         args, kw = cases.iso_case()
         kw, fibre = dict(kw, T=6.0), None
-    res = [_run_gpu(args, kw, fibre=fibre, brick=brick, kernel=k) for k in (1, 2)]
-    np.testing.assert_array_equal(res[0][2], res[1][2])
-    np.testing.assert_array_equal(res[0][3], res[1][3])
-    np.testing.assert_array_equal(res[0][4], res[1][4])
+    res = [_run_gpu(args, kw, fibre=fibre, brick=brick, kernel=k) for k in (1, 2, 3)]
+    for r in res[1:]:
+        np.testing.assert_array_equal(res[0][2], r[2])
+        np.testing.assert_array_equal(res[0][3], r[3])
+        np.testing.assert_array_equal(res[0][4], r[4])
 
 
 def test_graph_and_direct_launch_agree():
