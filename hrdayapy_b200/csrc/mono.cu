@@ -418,17 +418,21 @@ mono_step_kernel(MonoArgs a, int step_off, int mode) {
 // offset in that brick), with zeros where the neighbour brick is absent.
 //
 // Tile layout in shared memory: k rows of RK = round_up(BK + 2, 4) floats,
-// local (li, lj, lk) at 4 + ((li + 1) * TJ + (lj + 1)) * RK + lk, so every
-// interior row starts on a 16-byte boundary; lk = -1 of a row sits in the
-// previous row's padding.
+// local (li, lj, lk) at 4 + ((lj + 1) * TI + (li + 1)) * RK + lk, so every
+// interior row starts on a 16-byte boundary and lk = -1 of a row sits in the
+// previous row's padding.  Rows are ordered with i inner: a warp covers
+// consecutive slots (fixed li, several lj, all lk), and the j stride TI * RK
+// is an odd multiple of the row's width modulo the 32 banks for every
+// compiled shape (72, 120 or 80 floats), so the warp's k-rows fall on
+// disjoint banks when the stencil reads them.
 template <int BI, int BJ, int BK>
 struct PipeGeom {
   static constexpr int TI = BI + 2, TJ = BJ + 2, RK = ((BK + 2 + 3) / 4) * 4;
   static constexpr int NT = TI * TJ * RK + 4;  // floats per tile (multiple of 4)
-  static constexpr int SI = TJ * RK, SJ = RK;
+  static constexpr int SI = RK, SJ = TI * RK;
   static constexpr int BV = BI * BJ * BK;
   __host__ __device__ static constexpr int pos(int li, int lj, int lk) {
-    return 4 + ((li + 1) * TJ + (lj + 1)) * RK + lk;
+    return 4 + ((lj + 1) * TI + (li + 1)) * RK + lk;
   }
 };
 
@@ -443,8 +447,11 @@ struct PipeStage {
   static constexpr int NCHUNK = (N_STATE + 2) * G::BV / 4;  // 16-byte own-brick copies
 };
 
-// halo copy table entry: tile position | field << 11 | direction << 14 | offset << 19
+// halo copy table entry: tile position | field << 11 | direction << 14 |
+// offset << 19 | chunk << 31; a chunk entry moves 4 consecutive floats of a
+// k-row (16 bytes, both ends 16-byte aligned), otherwise one float
 constexpr int HALO_POS_BITS = 11;
+constexpr uint32_t HALO_CHUNK = 1u << 31;
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
@@ -488,12 +495,17 @@ __device__ __forceinline__ void pipe_issue(const MonoArgs& a, float* stage, cons
   for (int e = tid; e < n_halo; e += BV) {
     const uint32_t t = tab[e];
     const int pos = t & ((1u << HALO_POS_BITS) - 1), f = (t >> 11) & 7, dir = (t >> 14) & 31,
-              off = (int)(t >> 19);
+              off = (int)((t >> 19) & 0xFFFu);
     const int nb = nb27[dir];
     float* dst = stage + f * G::NT + pos;
     if (nb >= 0) {
       const float* src = f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns);
-      cp_async4(dst, src + (int64_t)nb * BV + off);
+      if (t & HALO_CHUNK)
+        cp_async16(dst, src + (int64_t)nb * BV + off);
+      else
+        cp_async4(dst, src + (int64_t)nb * BV + off);
+    } else if (t & HALO_CHUNK) {
+      *(float4*)dst = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
       *dst = 0.0f;
     }
@@ -589,17 +601,18 @@ mono_pipe_kernel(MonoArgs a, int step_off) {
 // lane, and without shared memory or barriers, so it runs at full occupancy.
 // Both do the fused kernels' arithmetic in the same order: results are
 // bit-identical to theirs.
-// Halo elements per thread of the diffusion kernel (copy-table entries
-// held in registers for the whole launch).
+// Halo copy-table entries per thread of the diffusion kernel (held in
+// registers for the whole launch).  Rows of a face or ij-edge outside the
+// brick in i or j move as BK/4 16-byte chunks, k-face and k-edge elements
+// one by one.
 template <int BI, int BJ, int BK, bool ANISO>
 struct DiffHalo {
-  static constexpr int BV = BI * BJ * BK;
-  // W: 6 faces + 12 edges; face weights: 3 faces; off-diagonal tiles: 2 face
-  // pairs + 4 edges each
-  static constexpr int W = 2 * (BJ * BK + BI * BK + BI * BJ) + (ANISO ? 4 * (BI + BJ + BK) : 0);
-  static constexpr int A = BJ * BK + BI * BK + BI * BJ +
-                           (2 * (BI * BK + BJ * BK) + 4 * BK) + (2 * (BJ * BK + BI * BJ) + 4 * BJ) +
-                           (2 * (BI * BK + BI * BJ) + 4 * BI);
+  static constexpr int BV = BI * BJ * BK, Q = BK / 4;
+  static constexpr int W = ANISO ? 2 * (BI + BJ + 2) * Q + 2 * BI * BJ + 4 * (BI + BJ)
+                                 : 2 * (BI + BJ) * Q + 2 * BI * BJ;
+  // face weights (-i, -j, -k faces) and the three off-diagonal tiles
+  static constexpr int A = (BJ + BI) * Q + BI * BJ + (2 * BJ + 2 * BI + 4) * Q +
+                           (2 * BJ * Q + 2 * BI * BJ + 4 * BJ) + (2 * BI * Q + 2 * BI * BJ + 4 * BI);
   static constexpr int N = ANISO ? W + A : W;
   static constexpr int PER_THREAD = (N + BV - 1) / BV;
 };
@@ -644,10 +657,10 @@ mono_diffuse_kernel(MonoArgs a, int step_off) {
     const int f = (t >> 11) & 7;
     hpos[q] = e < a.n_halo ? (uint32_t)(f * G::NT + (int)(t & ((1u << HALO_POS_BITS) - 1)))
                            : 0xFFFFFFFFu;
-    hdir[q] = (t >> 14) & 31;
+    hdir[q] = ((t >> 14) & 31) | ((t & HALO_CHUNK) ? 32u : 0u);
     hsrc[q] = e >= a.n_halo ? Win
                             : (f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)) +
-                                  (t >> 19);
+                                  ((t >> 19) & 0xFFFu);
   }
   auto issue = [&](float* st, const int* nb27, int b) {
     const int64_t base = (int64_t)b * BV;
@@ -668,11 +681,18 @@ mono_diffuse_kernel(MonoArgs a, int step_off) {
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
       if (hpos[q] != 0xFFFFFFFFu) {
-        const int nb = nb27[hdir[q]];
-        if (nb >= 0)
-          cp_async4(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
-        else
+        const int nb = nb27[hdir[q] & 31];
+        const bool chunk = hdir[q] & 32;
+        if (nb >= 0) {
+          if (chunk)
+            cp_async16(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
+          else
+            cp_async4(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
+        } else if (chunk) {
+          *(float4*)(st + hpos[q]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
           st[hpos[q]] = 0.0f;
+        }
       }
     }
   };
@@ -749,21 +769,37 @@ __global__ void __launch_bounds__(128, 8) mono_ionic_kernel(MonoArgs a, int step
 template <int BI, int BJ, int BK>
 static std::vector<uint32_t> pipe_halo_table(bool aniso) {
   using G = PipeGeom<BI, BJ, BK>;
+  static_assert(BK % 4 == 0, "k rows move as 16-byte chunks");
   std::vector<uint32_t> t;
+  auto entry = [&](int f, int li, int lj, int lk, bool chunk) {
+    const int di = li < 0 ? -1 : (li >= BI ? 1 : 0);
+    const int dj = lj < 0 ? -1 : (lj >= BJ ? 1 : 0);
+    const int dk = lk < 0 ? -1 : (lk >= BK ? 1 : 0);
+    const int gi = li - di * BI, gj = lj - dj * BJ, gk = lk - dk * BK;
+    const uint32_t off = (uint32_t)((gi * BJ + gj) * BK + gk);
+    const uint32_t dir = (uint32_t)((di + 1) * 9 + (dj + 1) * 3 + (dk + 1));
+    t.push_back((uint32_t)G::pos(li, lj, lk) | ((uint32_t)f << 11) | (dir << 14) | (off << 19) |
+                (chunk ? HALO_CHUNK : 0u));
+  };
+  auto needed = [&](int li, int lj, int lk) {
+    const int n_out = (li < 0 || li >= BI) + (lj < 0 || lj >= BJ) + (lk < 0 || lk >= BK);
+    return n_out > 0 && n_out <= (aniso ? 2 : 1);
+  };
   auto region = [&](int f, int i0, int i1, int j0, int j1, int k0, int k1) {
     for (int li = i0; li < i1; ++li)
-      for (int lj = j0; lj < j1; ++lj)
+      for (int lj = j0; lj < j1; ++lj) {
+        const bool side = li < 0 || li >= BI || lj < 0 || lj >= BJ;
+        // the interior part of a k-row outside the brick in i or j is
+        // contiguous in the neighbour brick: 16-byte chunks
+        const bool rows = side && k0 <= 0 && k1 >= BK && needed(li, lj, 0);
         for (int lk = k0; lk < k1; ++lk) {
-          const int di = li < 0 ? -1 : (li >= BI ? 1 : 0);
-          const int dj = lj < 0 ? -1 : (lj >= BJ ? 1 : 0);
-          const int dk = lk < 0 ? -1 : (lk >= BK ? 1 : 0);
-          const int n_out = (di != 0) + (dj != 0) + (dk != 0);
-          if (n_out == 0 || n_out > (aniso ? 2 : 1)) continue;
-          const int gi = li - di * BI, gj = lj - dj * BJ, gk = lk - dk * BK;
-          const uint32_t off = (uint32_t)((gi * BJ + gj) * BK + gk);
-          const uint32_t dir = (uint32_t)((di + 1) * 9 + (dj + 1) * 3 + (dk + 1));
-          t.push_back((uint32_t)G::pos(li, lj, lk) | ((uint32_t)f << 11) | (dir << 14) | (off << 19));
+          if (rows && lk >= 0 && lk < BK) {
+            if (lk % 4 == 0) entry(f, li, lj, lk, true);
+            continue;
+          }
+          if (needed(li, lj, lk)) entry(f, li, lj, lk, false);
         }
+      }
   };
   region(0, -1, BI + 1, -1, BJ + 1, -1, BK + 1);
   if (aniso) {
