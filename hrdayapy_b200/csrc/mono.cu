@@ -192,19 +192,26 @@ __device__ __forceinline__ float purkinje_diffuse(const MonoArgs& a, int p, int6
   return Vn;
 }
 
-// Ionic half of step istep of node p on V = Vn; stores its state and W.
-__device__ __forceinline__ void purkinje_ionic(const MonoArgs& a, int p, float Vn, int64_t istep,
-                                               float* __restrict__ Wout) {
+// Ionic half of step istep of node p on V = Vn with its state c; stores the
+// state and W.
+__device__ __forceinline__ void purkinje_ionic_state(const MonoArgs& a, int p, float Vn,
+                                                     CellState& c, int64_t istep,
+                                                     float* __restrict__ Wout) {
   const int var = a.pk_variant ? a.pk_variant[p] : 0;
   const CellParams cp = pheno_params(1, a.var_gks[var], a.var_gkr[var]);  // Purkinje -> endo
-  CellState c;
-#pragma unroll
-  for (int v = 0; v < N_STATE; ++v) c.v[v] = a.pk_state[(int64_t)v * a.n_pk + p];
   const float Iion = ttp06_step(Vn, c, a.dt, cp);
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p] = c.v[v];
   const float Is = stim_current(a, a.pk_stim[p], istep);
   Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+}
+
+__device__ __forceinline__ void purkinje_ionic(const MonoArgs& a, int p, float Vn, int64_t istep,
+                                               float* __restrict__ Wout) {
+  CellState c;
+#pragma unroll
+  for (int v = 0; v < N_STATE; ++v) c.v[v] = a.pk_state[(int64_t)v * a.n_pk + p];
+  purkinje_ionic_state(a, p, Vn, c, istep, Wout);
 }
 
 __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t step, int mode) {
@@ -741,7 +748,9 @@ mono_diffuse_kernel(MonoArgs a, int step_off) {
   cp_async_wait_all();
 }
 
-__global__ void __launch_bounds__(128, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+constexpr int ION_THREADS = 128;
+
+__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
   const int64_t step = *a.d_step + step_off;
   const bool odd = step & 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -872,6 +881,7 @@ struct HpMono {
   size_t pipe_smem;  // dynamic shared memory per CTA
   PipeFn diff;       // split step: diffusion half, or null
   int diff_grid;     // its persistent grid
+  int ion_grid;      // grid of the ionic half
   size_t diff_smem;  // and dynamic shared memory per CTA
   int bv;
   int64_t n_steps, steps_done;
@@ -918,8 +928,7 @@ static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) 
   if (grid == 0) return HP_OK;
   if (mode == 0 && h->diff) {
     h->diff<<<h->diff_grid, h->bv, h->diff_smem, s>>>(h->a, step_off);
-    const int n_ion = h->a.n_active_pad + h->a.n_pk;
-    if (n_ion > 0) mono_ionic_kernel<<<(n_ion + 127) / 128, 128, 0, s>>>(h->a, step_off);
+    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
   } else if (mode == 0 && h->pipe)
     h->pipe<<<h->pipe_grid, h->bv, h->pipe_smem, s>>>(h->a, step_off);
   else
@@ -1010,6 +1019,7 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   h->diff_smem = smem;
   const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   h->diff_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
+  h->ion_grid = (h->a.n_active_pad + h->a.n_pk + ION_THREADS - 1) / ION_THREADS;
   return HP_OK;
 }
 
@@ -1055,6 +1065,7 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   h->diff = nullptr;
   h->diff_grid = 0;
   h->diff_smem = 0;
+  h->ion_grid = 0;
   h->anisotropic = d->anisotropic;
   h->n_steps = d->n_steps;
   h->steps_done = 0;
@@ -1185,7 +1196,8 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
     HP_CUDA_TRY(cudaMemsetAsync(a.pk_Vs1, 0, d->n_pk * sizeof(float), s));
   }
   HP_CUDA_TRY(cudaGetLastError());
-  if (d->kernel == HP_MONO_KERNEL_SPLIT) {
+  if (d->kernel == HP_MONO_KERNEL_SPLIT ||
+      (d->kernel == HP_MONO_KERNEL_AUTO && d->n_bricks > 0)) {
     HP_TRY(setup_split(h, se, d, s));
   } else if (d->kernel != HP_MONO_KERNEL_BRICK && d->n_bricks > 0) {
     HP_TRY(setup_pipe(h, se, d->anisotropic, d->kernel == HP_MONO_KERNEL_PIPELINED, s));

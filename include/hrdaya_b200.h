@@ -135,8 +135,8 @@ typedef struct {
   float deact_threshold;        /* mV, downstroke crossing */
   int32_t max_events;           /* activation events kept per voxel (1..16) */
 
-  /* step kernel: HP_MONO_KERNEL_AUTO picks the pipelined one when its two
-   * shared-memory stages fit the device, else the per-brick one */
+  /* step kernel (all give bit-identical results): HP_MONO_KERNEL_AUTO is
+   * the split step, the fastest on B200 for every compiled brick shape */
   int32_t kernel;
 } HpMonoDesc;
 
