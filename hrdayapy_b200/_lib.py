@@ -95,7 +95,8 @@ class HpSolveStats(C.Structure):
 class HpPrecondDesc(C.Structure):
     _fields_ = [("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("label", P),
                 ("n_materials", C.c_int32), ("pin_cell", C.c_int64), ("omega", C.c_float),
-                ("seed", C.c_uint64), ("init_params", P)]
+                ("seed", C.c_uint64), ("init_params", P), ("sigma", P), ("h_m", C.c_double),
+                ("coarse_agg", C.c_int32)]
 
 
 class HpTorsoArrays(C.Structure):
@@ -122,9 +123,11 @@ def _declare_optional(L):
     L.hp_precond_params.argtypes = [P, P, P, P, C.c_int32, P]
     L.hp_precond_output.argtypes = [P, P, P, P, P]
     L.hp_precond_destroy.argtypes = [P]
+    L.hp_precond_coarse_info.argtypes = [P, P, P]
     L.hp_torso_arrays.argtypes = [P, C.POINTER(HpTorsoArrays)]
     L.hp_torso_solve_frame_fcg.argtypes = [P, P, P, C.c_int32, P, C.c_int32, C.c_double,
-                                           C.c_int32, C.c_int32, C.POINTER(HpSolveStats), P]
+                                           C.c_int32, C.c_int32, C.c_int32,
+                                           C.POINTER(HpSolveStats), P]
     L.hp_torso_train_precond.argtypes = [P, P, P, C.c_int64, C.c_int32, P, C.c_int32, C.c_int32,
                                          C.c_float, C.c_double, P, P]
     L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,

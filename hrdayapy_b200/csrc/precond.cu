@@ -1,7 +1,16 @@
 // Learned preconditioner for the torso Poisson solve (no counterpart in the
 // reference, whose solver is Jacobi-PCG only).
 //
-//   M(r) = omega * D^-1 r  +  P( s * CNN( [R(D^-1 r) / s, geometry] ) )
+//   M(r) = omega * D^-1 r  +  Q A_c^-1 Q^T r  +  P( s * CNN( [R(D^-1 r) / s, geometry] ) )
+//
+// Q is piecewise-constant aggregation over cubes of ag^3 torso voxels and
+// A_c = Q^T A Q the Galerkin coarse operator (a few thousand unknowns at
+// most), factorised and inverted once on the host and applied as a dense
+// mat-vec: it removes the global, smooth error modes that Jacobi leaves and
+// that no network with a local receptive field can represent.  The network
+// learns what remains between the two scales.  Without the network
+// (use_net = 0) M is the same two-level preconditioner, so the network's
+// gain is measured against exactly the method without it.
 //
 // R restricts the fine torso grid (padded, see torso.cu) by 2 x 2 x 2
 // averaging onto the network grid (half resolution, NDHWC BF16, 16 input
@@ -15,9 +24,9 @@
 // concatenation.  It is trained on the GPU by its own kernels: forward,
 // data gradients through the same tensor-core convolution with flipped and
 // transposed weights (ReLU masks fused in its epilogue), weight gradients on
-// the CUDA cores, and Adam on FP32 master weights.  Loss: squared error of
-// M(r) against the error e the plain solver's iterates leave, normalised by
-// ||e||^2.
+// the CUDA cores, and Adam on FP32 master weights.  Loss: the fraction of
+// the error's energy that one optimal step along M(r) leaves, for the
+// residual / error pairs (r, e) the plain solver's iterates give.
 #include "hp_common.cuh"
 #include "tc_conv.cuh"
 
@@ -133,17 +142,20 @@ __global__ void scale_kernel(const double* part, int nparts, int64_t n, float* s
   }
 }
 
-// feat[c][0] = raw / s, channels 1.. from the geometry tensor
+// feat[c][0] = raw / s, channels 1.. from the geometry tensor, channel 15
+// the coarse correction zh / s_z when there is a coarse level (zh != null)
 __global__ void feat_write_kernel(const float* __restrict__ raw, const __nv_bfloat16* __restrict__ geo,
                                   const float* __restrict__ scale, __nv_bfloat16* __restrict__ feat,
-                                  int64_t n) {
+                                  int64_t n, const float* __restrict__ zh) {
   const float inv = 1.0f / scale[0];
+  const float invz = zh ? 1.0f / scale[1] : 0.0f;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
     __align__(16) __nv_bfloat16 v[16];
     *(uint4*)&v[0] = ((const uint4*)(geo + c * 16))[0];
     *(uint4*)&v[8] = ((const uint4*)(geo + c * 16))[1];
     v[0] = __float2bfloat16(raw[c] * inv);
+    if (zh) v[15] = __float2bfloat16(zh[c] * invz);
     ((uint4*)(feat + c * 16))[0] = *(uint4*)&v[0];
     ((uint4*)(feat + c * 16))[1] = *(uint4*)&v[8];
   }
@@ -240,52 +252,70 @@ __global__ void relu_mask_kernel(__nv_bfloat16* __restrict__ g, const __nv_bfloa
     if (!(__bfloat162float(a[q]) > 0.0f)) g[q] = __float2bfloat16(0.0f);
 }
 
-struct ProlongArgs {
-  int pj, pk;
-  int64_t ng, pin;
+// Coarse level: per aggregate the sum of r over its active, unpinned cells.
+struct CoarseArgs {
+  int ni, nj, nk, pj, pk, ag, nbj, nbk, nc;
+  int64_t pin;
   const uint8_t* label;
-  const float* invd;
-  const float* r;
-  const float* y;       // coarse FP32 output
-  const float* scale;
-  float omega;
-  Dims c;
-  int use_net;
+  const int32_t* c_box;   // nc aggregate boxes
+  const int32_t* box2c;   // per box: coarse index or -1
+  const float* ainv;      // nc x nc, row-major
+  double* rc;
+  float* zc;
 };
 
-// z = omega * invd * r + s * y[parent] on active fine cells (0 elsewhere)
-__global__ void prolong_kernel(ProlongArgs a, float* __restrict__ z) {
-  const float s = a.use_net ? a.scale[0] : 0.0f;
-  const int64_t SI = (int64_t)a.pj * a.pk;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    float v = 0.0f;
-    if (a.label[g] != 0 && g != a.pin) {
-      v = a.omega * a.invd[g] * a.r[g];
-      if (a.use_net) {
-        const int i = (int)(g / SI) - 1, j = (int)((g / a.pk) % a.pj) - 1, k = (int)(g % a.pk) - 1;
-        v += s * a.y[((int64_t)(i / 2) * a.c.H + j / 2) * a.c.W + k / 2];
-      }
-    }
-    z[g] = v;
-  }
+__device__ __forceinline__ int coarse_of(const CoarseArgs& c, int i, int j, int k) {
+  return c.box2c[((i / c.ag) * c.nbj + j / c.ag) * c.nbk + k / c.ag];
 }
 
-struct LossArgs {
-  FeatArgs f;
-  const float* e;        // padded fine error (FP32)
-  const float* y;
-  const float* scale;
-  float omega;
-  const double* enorm;   // [1] sum e^2
-};
-
-// sum e^2 over active fine cells (block partials)
-__global__ void __launch_bounds__(TB) enorm_kernel(FeatArgs a, const float* __restrict__ e, int64_t ng,
-                                                   double* part) {
+__global__ void __launch_bounds__(TB) coarse_restrict_kernel(CoarseArgs c, const float* __restrict__ r) {
+  const int I = blockIdx.x;
+  const int b = c.c_box[I];
+  const int bk = b % c.nbk, bj = (b / c.nbk) % c.nbj, bi = b / (c.nbk * c.nbj);
+  const int n = c.ag * c.ag * c.ag;
   double acc = 0.0;
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += (int64_t)gridDim.x * TB)
-    if (a.label[g] != 0 && g != a.pin) acc += (double)e[g] * e[g];
+  for (int t = threadIdx.x; t < n; t += TB) {
+    const int i = bi * c.ag + t / (c.ag * c.ag), j = bj * c.ag + (t / c.ag) % c.ag,
+              k = bk * c.ag + t % c.ag;
+    if (i >= c.ni || j >= c.nj || k >= c.nk) continue;
+    const int64_t g = ((int64_t)(i + 1) * c.pj + (j + 1)) * c.pk + (k + 1);
+    if (c.label[g] != 0 && g != c.pin) acc += (double)r[g];
+  }
+  __shared__ double sh[TB];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) c.rc[I] = sh[0];
+}
+
+// zc = A_c^-1 rc, one warp per row
+__global__ void __launch_bounds__(TB) coarse_matvec_kernel(CoarseArgs c) {
+  const int row = blockIdx.x * (TB / 32) + threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (row >= c.nc) return;
+  const float* a = c.ainv + (int64_t)row * c.nc;
+  float acc = 0.0f;
+  for (int q = lane; q < c.nc; q += 32) acc += a[q] * (float)c.rc[q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) c.zc[row] = acc;
+}
+
+// zh[c] = coarse correction of the aggregate holding network cell c (its 8
+// fine children share one aggregate, ag being even); partial sums of zh^2
+__global__ void __launch_bounds__(TB) coarse_feat_kernel(CoarseArgs c, Dims cd, float* __restrict__ zh,
+                                                         double* __restrict__ part) {
+  double acc = 0.0;
+  const int64_t n = cd.n();
+  for (int64_t q = blockIdx.x * (int64_t)TB + threadIdx.x; q < n; q += (int64_t)gridDim.x * TB) {
+    const int w = q % cd.W, h = (q / cd.W) % cd.H, d = (int)(q / ((int64_t)cd.W * cd.H));
+    const int I = coarse_of(c, 2 * d, 2 * h, 2 * w);
+    const float v = I >= 0 ? c.zc[I] : 0.0f;
+    zh[q] = v;
+    acc += (double)v * v;
+  }
   __shared__ double sh[TB];
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -296,58 +326,137 @@ __global__ void __launch_bounds__(TB) enorm_kernel(FeatArgs a, const float* __re
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-__global__ void sum_kernel(const double* part, int nparts, double* out) {
-  __shared__ double sh[TB];
-  double a = 0.0;
-  for (int q = threadIdx.x; q < nparts; q += TB) a += part[q];
-  sh[threadIdx.x] = a;
-  __syncthreads();
-  for (int st = TB / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-    __syncthreads();
+struct ProlongArgs {
+  CoarseArgs c;
+  int pj, pk;
+  int64_t ng, pin;
+  const uint8_t* label;
+  const float* invd;
+  const float* r;
+  const float* y;       // coarse FP32 output
+  const float* scale;
+  float omega;
+  Dims cd;
+  int use_net;
+};
+
+// z = omega * invd * r + s * y[parent] on active fine cells (0 elsewhere)
+__global__ void prolong_kernel(ProlongArgs a, float* __restrict__ z) {
+  const float s = a.use_net ? a.scale[2] : 0.0f;
+  const int64_t SI = (int64_t)a.pj * a.pk;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    float v = 0.0f;
+    if (a.label[g] != 0 && g != a.pin) {
+      v = a.omega * a.invd[g] * a.r[g];
+      const int i = (int)(g / SI) - 1, j = (int)((g / a.pk) % a.pj) - 1, k = (int)(g % a.pk) - 1;
+      if (a.use_net) v += s * a.y[((int64_t)(i / 2) * a.cd.H + j / 2) * a.cd.W + k / 2];
+      if (a.c.nc > 0) v += a.c.zc[coarse_of(a.c, i, j, k)];
+    }
+    z[g] = v;
   }
-  if (threadIdx.x == 0) out[0] = sh[0];
 }
 
-// Per coarse cell: loss partial and dL/d(net output) into channel 0 of a
-// 16-channel BF16 gradient tensor (other channels zero).
-//   L = sum_fine (omega invd r + s y_parent - e)^2 / ||e||^2
-__global__ void __launch_bounds__(TB) loss_kernel(LossArgs a, __nv_bfloat16* __restrict__ gout,
-                                                  double* part) {
-  const float s = a.scale[0];
-  const double inv_norm = 1.0 / fmax(a.enorm[0], 1e-300);
-  double acc = 0.0;
-  const int64_t n = a.f.c.n();
+// Training loss: how well one optimal step along z = M(r) reduces the
+// energy of the error e (A e = r):
+//   L = 1 - (r.z)^2 / ((z.A z) (r.e)),   dL/dz = 2 (r.z) / ((z.A z)(r.e)) ((r.z)/(z.A z) A z - r)
+// which is invariant to the scale of M and weighs error components by their
+// energy, as CG does.  The network output enters z as s_out * y[parent].
+struct EnergyArgs {
+  int pj, pk;
+  int64_t ng, pin;
+  const uint8_t* label;
+  const float* T32;     // 16 x 16 face conductances
+  const float* r;
+  const float* e;
+  const float* z;
+  float* az;
+};
+
+// az = A z on unknown cells; block partials of r.z, z.A z, r.e
+__global__ void __launch_bounds__(TB) energy_dots_kernel(EnergyArgs a, double* __restrict__ part) {
+  __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = a.T32[q];
+  __syncthreads();
+  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB) {
+    const int l = a.label[g];
+    if (l == 0 || g == a.pin) continue;
+    const float zg = a.z[g];
+    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+    float q = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) q += T[l * HP_MAX_MATERIALS + a.label[nb[f]]] * (zg - a.z[nb[f]]);
+    a.az[g] = q;
+    const double rg = a.r[g];
+    acc[0] += rg * zg;
+    acc[1] += (double)zg * q;
+    acc[2] += rg * a.e[g];
+  }
+  __shared__ double sh[3][TB];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) part[3 * blockIdx.x + k] = sh[k][0];
+}
+
+__global__ void sum3_kernel(const double* part, int nparts, double* out) {
+  __shared__ double sh[3][TB];
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int q = threadIdx.x; q < nparts; q += TB)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a[k] += part[3 * q + k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int st = TB / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = sh[k][0];
+}
+
+// dL/d(net output) into channel 0 of a 16-channel BF16 gradient tensor
+// (other channels zero); the loss value into *loss
+__global__ void __launch_bounds__(TB) energy_grad_kernel(EnergyArgs a, Dims cd, const double* dots,
+                                                         const float* scale,
+                                                         __nv_bfloat16* __restrict__ gout,
+                                                         double* loss) {
+  const double rz = dots[0], zaz = fmax(dots[1], 1e-300), re = dots[2];
+  const double G = 2.0 * rz / (zaz * re), ratio = rz / zaz;
+  const float s = scale[2];
+  const int64_t n = cd.n();
   for (int64_t c = blockIdx.x * (int64_t)TB + threadIdx.x; c < n; c += (int64_t)gridDim.x * TB) {
-    const int w = c % a.f.c.W, h = (c / a.f.c.W) % a.f.c.H, d = (int)(c / ((int64_t)a.f.c.W * a.f.c.H));
-    const float yv = s * a.y[c];
+    const int w = c % cd.W, h = (c / cd.W) % cd.H, d = (int)(c / ((int64_t)cd.W * cd.H));
     double g = 0.0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int64_t fg = fine_of(a.f, d, h, w, q);
-      if (a.f.label[fg] != 0 && fg != a.f.pin) {
-        const double res = (double)a.omega * a.f.invd[fg] * a.f.r[fg] + yv - a.e[fg];
-        acc += res * res;
-        g += 2.0 * res;
-      }
+      const int fi = 2 * d + ((q >> 2) & 1) + 1, fj = 2 * h + ((q >> 1) & 1) + 1,
+                fk = 2 * w + (q & 1) + 1;
+      const int64_t fg = ((int64_t)fi * a.pj + fj) * a.pk + fk;
+      if (a.label[fg] != 0 && fg != a.pin) g += G * (ratio * a.az[fg] - (double)a.r[fg]);
     }
-    // dL/dy_net = dL/dyv * s
-    const float gv = (float)(g * inv_norm * s);
     __align__(16) __nv_bfloat16 o[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) o[q] = __float2bfloat16(0.0f);
-    o[0] = __float2bfloat16(gv);
+    o[0] = __float2bfloat16((float)(g * s));
     ((uint4*)(gout + c * 16))[0] = *(uint4*)&o[0];
     ((uint4*)(gout + c * 16))[1] = *(uint4*)&o[8];
   }
-  __shared__ double sh[TB];
-  sh[threadIdx.x] = acc * inv_norm;
-  __syncthreads();
-  for (int st = TB / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+  if (blockIdx.x == 0 && threadIdx.x == 0) loss[0] = 1.0 - rz * rz / (zaz * re);
 }
 
 // Weight gradient of one 3x3x3 layer on the CUDA cores (FP32 accumulation):
@@ -478,15 +587,26 @@ struct HpPrecond {
   float* y;
   float* raw;
   float* scale;
+  float* zh;                 // coarse correction on the network grid
   // gradients
   __nv_bfloat16 *gout, *g_d1b, *g_d1a, *g_u1, *g_d2b, *g_e1b, *g_d2a, *g_u2, *g_e3b, *g_e2b,
       *g_e3a, *g_p2, *g_e2a, *g_p1, *g_e1a;
   double* part;
-  double* enorm;
+  double* dots;              // r.z, z.A z, r.e of the energy loss
   double* loss;
+  float* zbuf;               // M(r) on the fine grid (training)
+  float* az;                 // A M(r)
+  float* T32;                // face conductances (device, 16 x 16)
   int* err;
   int64_t step;
   int nblk;
+  // coarse level (nc = 0: none)
+  int ag, nbi, nbj, nbk, nc;
+  int32_t* c_box;
+  int32_t* box2c;
+  float* ainv;
+  double* rc;
+  float* zc;
 };
 
 template <typename T>
@@ -507,11 +627,141 @@ static hp_status pal(HpPrecond* h, T** dst, size_t n) {
 
 extern "C" hp_status hp_precond_destroy(HpPrecond* h);
 
+#define HP_TRY_PC(x)             \
+  do {                           \
+    hp_status _s = (x);          \
+    if (_s != HP_OK) return _s;  \
+  } while (0)
+
 static hp_status repack(HpPrecond* h, cudaStream_t s) {
   for (int l = 0; l < NL; ++l) {
     pack_kernel<<<256, 256, 0, s>>>(h->par + h->off_w[l], LCIN[l], LCOUT[l], h->wp[l], h->wpt[l]);
   }
   HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// Dense SPD inverse on the host (FP64): Cholesky A = L L^T, X = L^-1, then
+// A^-1 = X^T X.  Returns false if A is not positive definite.
+static bool spd_inverse(std::vector<double>& A, int n) {
+  for (int j = 0; j < n; ++j) {
+    double* Aj = &A[(size_t)j * n];
+    double sjj = Aj[j];
+    for (int k = 0; k < j; ++k) sjj -= Aj[k] * Aj[k];
+    if (!(sjj > 0.0)) return false;
+    const double ljj = sqrt(sjj);
+    Aj[j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double* Ai = &A[(size_t)i * n];
+      double sij = Ai[j];
+      for (int k = 0; k < j; ++k) sij -= Ai[k] * Aj[k];
+      Ai[j] = sij / ljj;
+    }
+  }
+  // X = L^-1 (lower), stored transposed as U = X^T (upper, row-major)
+  std::vector<double> U((size_t)n * n, 0.0), x(n);
+  for (int j = 0; j < n; ++j) {
+    for (int i = 0; i < j; ++i) x[i] = 0.0;
+    for (int i = j; i < n; ++i) {
+      const double* Li = &A[(size_t)i * n];
+      double v = i == j ? 1.0 : 0.0;
+      for (int k = j; k < i; ++k) v -= Li[k] * x[k];
+      x[i] = v / Li[i];
+    }
+    for (int i = j; i < n; ++i) U[(size_t)j * n + i] = x[i];
+  }
+  // A^-1[i][j] = sum_k X[k][i] X[k][j] = sum_{k >= max(i,j)} U[i][k] U[j][k]
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const double* Ui = &U[(size_t)i * n];
+      const double* Uj = &U[(size_t)j * n];
+      double v = 0.0;
+      for (int k = i; k < n; ++k) v += Ui[k] * Uj[k];
+      A[(size_t)i * n + j] = v;
+      A[(size_t)j * n + i] = v;
+    }
+  return true;
+}
+
+// Aggregates of ag^3 voxels (ag doubling from 4 until at most HP_PC_MAX_COARSE
+// aggregates hold an active unpinned voxel, unless d->coarse_agg fixes it),
+// the Galerkin operator A_c = Q^T A Q of the torso stiffness (harmonic-mean
+// face conductance / h^2, air faces skipped, the pinned voxel eliminated) and
+// its inverse.
+static hp_status coarse_setup(HpPrecond* h, const HpPrecondDesc* d, cudaStream_t s) {
+  HP_REQUIRE(d->sigma && d->h_m > 0.0, "hp_precond_create: the coarse level needs sigma and h_m");
+  const int ni = d->ni, nj = d->nj, nk = d->nk;
+  const int64_t pin = d->pin_cell;
+  const int pjj = nj + 2, pkk = nk + 2;
+  const int pin_i = pin >= 0 ? (int)(pin / ((int64_t)pjj * pkk)) - 1 : -1;
+  const int pin_j = pin >= 0 ? (int)((pin / pkk) % pjj) - 1 : -1;
+  const int pin_k = pin >= 0 ? (int)(pin % pkk) - 1 : -1;
+  auto lab = [&](int i, int j, int k) -> int {
+    if (i < 0 || j < 0 || k < 0 || i >= ni || j >= nj || k >= nk) return 0;
+    return d->label[((int64_t)i * nj + j) * nk + k];
+  };
+  auto unknown = [&](int i, int j, int k) {
+    return lab(i, j, k) != 0 && !(i == pin_i && j == pin_j && k == pin_k);
+  };
+  int ag = d->coarse_agg > 0 ? d->coarse_agg : 4;
+  std::vector<int32_t> box2c, c_box;
+  int nbi = 0, nbj = 0, nbk = 0;
+  while (true) {
+    nbi = (ni + ag - 1) / ag; nbj = (nj + ag - 1) / ag; nbk = (nk + ag - 1) / ag;
+    box2c.assign((size_t)nbi * nbj * nbk, -1);
+    c_box.clear();
+    for (int i = 0; i < ni; ++i)
+      for (int j = 0; j < nj; ++j)
+        for (int k = 0; k < nk; ++k)
+          if (unknown(i, j, k)) {
+            const int b = ((i / ag) * nbj + j / ag) * nbk + k / ag;
+            if (box2c[b] < 0) box2c[b] = 0;
+          }
+    for (size_t b = 0; b < box2c.size(); ++b)
+      if (box2c[b] == 0) { box2c[b] = (int32_t)c_box.size(); c_box.push_back((int32_t)b); }
+    if ((int)c_box.size() <= HP_PC_MAX_COARSE || d->coarse_agg > 0) break;
+    ag *= 2;
+  }
+  const int nc = (int)c_box.size();
+  HP_REQUIRE(nc <= HP_PC_MAX_COARSE, "hp_precond_create: %d coarse unknowns exceed %d", nc,
+             HP_PC_MAX_COARSE);
+  if (nc == 0) return HP_OK;
+  double T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS] = {0};
+  const double h2 = d->h_m * d->h_m;
+  for (int u = 1; u < d->n_materials; ++u)
+    for (int v = 1; v < d->n_materials; ++v) {
+      const double su = d->sigma[u], sv = d->sigma[v];
+      if (su + sv >= 1e-30) T64[u * HP_MAX_MATERIALS + v] = (2.0 * su * sv) / (su + sv) / h2;
+    }
+  std::vector<double> Ac((size_t)nc * nc, 0.0);
+  auto cid = [&](int i, int j, int k) { return box2c[((i / ag) * nbj + j / ag) * nbk + k / ag]; };
+  const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  for (int i = 0; i < ni; ++i)
+    for (int j = 0; j < nj; ++j)
+      for (int k = 0; k < nk; ++k) {
+        if (!unknown(i, j, k)) continue;
+        const int I = cid(i, j, k), l = lab(i, j, k);
+        for (int f = 0; f < 6; ++f) {
+          const int a = i + off[f][0], b = j + off[f][1], c = k + off[f][2];
+          const double t = T64[l * HP_MAX_MATERIALS + lab(a, b, c)];
+          if (t == 0.0) continue;
+          Ac[(size_t)I * nc + I] += t;
+          if (unknown(a, b, c)) Ac[(size_t)I * nc + cid(a, b, c)] -= t;
+        }
+      }
+  HP_REQUIRE(spd_inverse(Ac, nc), "hp_precond_create: coarse operator is not positive definite "
+             "(torso not connected to the pinned voxel?)");
+  std::vector<float> a32(Ac.begin(), Ac.end());
+  h->ag = ag; h->nbi = nbi; h->nbj = nbj; h->nbk = nbk; h->nc = nc;
+  HP_TRY_PC(pal(h, &h->c_box, nc));
+  HP_TRY_PC(pal(h, &h->box2c, box2c.size()));
+  HP_TRY_PC(pal(h, &h->ainv, (size_t)nc * nc));
+  HP_TRY_PC(pal(h, &h->rc, nc));
+  HP_TRY_PC(pal(h, &h->zc, nc));
+  HP_CUDA_TRY(cudaMemcpyAsync(h->c_box, c_box.data(), nc * 4, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(h->box2c, box2c.data(), box2c.size() * 4, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(h->ainv, a32.data(), a32.size() * 4, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors are temporaries
   return HP_OK;
 }
 
@@ -523,6 +773,7 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
              d->nj, d->nk);
   HP_REQUIRE(d->label && d->n_materials >= 1 && d->n_materials <= HP_MAX_MATERIALS,
              "hp_precond_create: bad labels");
+  HP_REQUIRE(d->sigma && d->h_m > 0.0, "hp_precond_create: sigma and h_m are required");
   cudaStream_t s = (cudaStream_t)stream;
   HpPrecond* h = new HpPrecond();
   h->ni = d->ni; h->nj = d->nj; h->nk = d->nk;
@@ -601,7 +852,8 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
   PC_TRY(pal(h, &h->d1b, n1 * 16));
   PC_TRY(pal(h, &h->y, n1));
   PC_TRY(pal(h, &h->raw, n1));
-  PC_TRY(pal(h, &h->scale, 1));
+  PC_TRY(pal(h, &h->scale, 3));  // input scale s, coarse-field scale s_z, output scale
+  PC_TRY(pal(h, &h->zh, n1));
   PC_TRY(pal(h, &h->gout, n1 * 16));
   PC_TRY(pal(h, &h->g_d1b, n1 * 16));
   PC_TRY(pal(h, &h->g_d1a, n1 * 16));
@@ -617,8 +869,22 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
   PC_TRY(pal(h, &h->g_e2a, n2 * 32));
   PC_TRY(pal(h, &h->g_p1, n2 * 16));
   PC_TRY(pal(h, &h->g_e1a, n1 * 16));
-  PC_TRY(pal(h, &h->part, h->nblk));
-  PC_TRY(pal(h, &h->enorm, 1));
+  PC_TRY(pal(h, &h->part, 3 * h->nblk));
+  PC_TRY(pal(h, &h->dots, 3));
+  PC_TRY(pal(h, &h->zbuf, h->ng));
+  PC_TRY(pal(h, &h->az, h->ng));
+  PC_TRY(pal(h, &h->T32, HP_MAX_MATERIALS * HP_MAX_MATERIALS));
+  {
+    float T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS] = {0};
+    const double h2 = d->h_m * d->h_m;
+    for (int u = 1; u < d->n_materials; ++u)
+      for (int v = 1; v < d->n_materials; ++v) {
+        const double su = d->sigma[u], sv = d->sigma[v];
+        if (su + sv >= 1e-30) T32[u * HP_MAX_MATERIALS + v] = (float)((2.0 * su * sv) / (su + sv) / h2);
+      }
+    HP_CUDA_TRY(cudaMemcpyAsync(h->T32, T32, sizeof(T32), cudaMemcpyHostToDevice, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
   PC_TRY(pal(h, &h->loss, 1));
   PC_TRY(pal(h, &h->err, 1));
   HP_CUDA_TRY(cudaMemsetAsync(h->err, 0, 4, s));
@@ -638,7 +904,7 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
           }
           const int64_t cc = ((int64_t)a * c.H + b) * c.W + w;
           geo[cc * 16 + 1] = __float2bfloat16(1.0f - frac[0]);
-          for (int m = 1; m < d->n_materials && m < 15; ++m)
+          for (int m = 1; m < d->n_materials && m < 14; ++m)  // channel 15: coarse field
             geo[cc * 16 + 1 + m] = __float2bfloat16(frac[m]);
         }
     (void)ni;
@@ -646,6 +912,8 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
     HP_CUDA_TRY(cudaMemcpyAsync(h->geo, geo.data(), geo.size() * 2, cudaMemcpyHostToDevice, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
   }
+  h->nc = 0;
+  if (d->coarse_agg >= 0) PC_TRY(coarse_setup(h, d, s));
   PC_TRY(repack(h, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
   *out = h;
@@ -682,13 +950,38 @@ static void wgrad(HpPrecond* h, int l, const __nv_bfloat16* X, const __nv_bfloat
 
 static int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)); }
 
+static CoarseArgs coarse_args(const HpPrecond* h, const uint8_t* label) {
+  return CoarseArgs{h->ni, h->nj, h->nk, h->pj, h->pk, h->ag, h->nbj, h->nbk, h->nc, h->pin,
+                    label, h->c_box, h->box2c, h->ainv, h->rc, h->zc};
+}
+
+// zc = A_c^-1 Q^T r (no-op without a coarse level)
+static hp_status coarse_solve(HpPrecond* h, const uint8_t* label, const float* r, cudaStream_t s) {
+  if (h->nc == 0) return HP_OK;
+  const CoarseArgs c = coarse_args(h, label);
+  coarse_restrict_kernel<<<h->nc, TB, 0, s>>>(c, r);
+  coarse_matvec_kernel<<<(h->nc + TB / 32 - 1) / (TB / 32), TB, 0, s>>>(c);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 hp_status precond_forward(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
                           cudaStream_t s) {
   FeatArgs fa{h->pj, h->pk, h->pin, label, invd, r, h->L[1]};
   const int64_t n1 = h->L[1].n();
   feat_raw_kernel<<<h->nblk, TB, 0, s>>>(fa, h->raw, h->part);
   scale_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, n1, h->scale);
-  feat_write_kernel<<<grid_for(n1), 256, 0, s>>>(h->raw, h->geo, h->scale, h->feat, n1);
+  if (h->nc > 0) {
+    // the network also sees the coarse correction; its output is scaled like
+    // that field (the error it refines), else like the input
+    coarse_feat_kernel<<<h->nblk, TB, 0, s>>>(coarse_args(h, label), h->L[1], h->zh, h->part);
+    scale_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, n1, h->scale + 1);
+    HP_CUDA_TRY(cudaMemcpyAsync(h->scale + 2, h->scale + 1, 4, cudaMemcpyDeviceToDevice, s));
+  } else {
+    HP_CUDA_TRY(cudaMemcpyAsync(h->scale + 2, h->scale, 4, cudaMemcpyDeviceToDevice, s));
+  }
+  feat_write_kernel<<<grid_for(n1), 256, 0, s>>>(h->raw, h->geo, h->scale, h->feat, n1,
+                                                 h->nc > 0 ? h->zh : nullptr);
   HP_CUDA_TRY(cudaGetLastError());
   hp_status st;
 #define FW(x) do { st = (x); if (st != HP_OK) return st; } while (0)
@@ -714,12 +1007,14 @@ hp_status precond_forward(HpPrecond* h, const uint8_t* label, const float* invd,
 
 hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
                         float* z, int use_net, cudaStream_t s) {
+  hp_status cst = coarse_solve(h, label, r, s);
+  if (cst != HP_OK) return cst;
   if (use_net) {
     hp_status st = precond_forward(h, label, invd, r, s);
     if (st != HP_OK) return st;
   }
-  ProlongArgs pa{h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y, h->scale, h->omega,
-                 h->L[1], use_net};
+  ProlongArgs pa{coarse_args(h, label), h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y,
+                 h->scale, h->omega, h->L[1], use_net};
   prolong_kernel<<<grid_for(h->ng), 256, 0, s>>>(pa, z);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -739,16 +1034,19 @@ extern "C" hp_status hp_precond_train_step(HpPrecond* h, const uint8_t* label, c
                                            float* loss_out, void* stream) {
   HP_REQUIRE(h && label && invd && r && e, "hp_precond_train_step: null argument");
   cudaStream_t s = (cudaStream_t)stream;
-  hp_status st = precond_forward(h, label, invd, r, s);
+  hp_status st = coarse_solve(h, label, r, s);
+  if (st != HP_OK) return st;
+  st = precond_forward(h, label, invd, r, s);
   if (st != HP_OK) return st;
   const Dims L1 = h->L[1], L2 = h->L[2], L3 = h->L[3];
   const int64_t n1 = L1.n(), n2 = L2.n(), n3 = L3.n();
-  FeatArgs fa{h->pj, h->pk, h->pin, label, invd, r, L1};
-  enorm_kernel<<<h->nblk, TB, 0, s>>>(fa, e, h->ng, h->part);
-  sum_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->enorm);
-  LossArgs la{fa, e, h->y, h->scale, h->omega, h->enorm};
-  loss_kernel<<<h->nblk, TB, 0, s>>>(la, h->gout, h->part);
-  sum_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->loss);
+  ProlongArgs pa{coarse_args(h, label), h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y,
+                 h->scale, h->omega, h->L[1], 1};
+  prolong_kernel<<<grid_for(h->ng), 256, 0, s>>>(pa, h->zbuf);
+  EnergyArgs ea{h->pj, h->pk, h->ng, h->pin, label, h->T32, r, e, h->zbuf, h->az};
+  energy_dots_kernel<<<h->nblk, TB, 0, s>>>(ea, h->part);
+  sum3_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->dots);
+  energy_grad_kernel<<<h->nblk, TB, 0, s>>>(ea, L1, h->dots, h->scale, h->gout, h->loss);
   HP_CUDA_TRY(cudaMemsetAsync(h->grad, 0, h->n_par * 4, s));
 #define BW(x) do { st = (x); if (st != HP_OK) return st; } while (0)
   // OUT (linear, 16 -> 1 padded to 16)
@@ -827,6 +1125,13 @@ extern "C" hp_status hp_precond_output(HpPrecond* h, float* host_y, float* host_
   if (host_scale) HP_CUDA_TRY(cudaMemcpyAsync(host_scale, h->scale, 4, cudaMemcpyDeviceToHost, s));
   if (host_err) HP_CUDA_TRY(cudaMemcpyAsync(host_err, h->err, 4, cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+extern "C" hp_status hp_precond_coarse_info(const HpPrecond* h, int32_t* agg, int32_t* n_coarse) {
+  HP_REQUIRE(h, "hp_precond_coarse_info: null handle");
+  if (agg) *agg = h->nc ? h->ag : 0;
+  if (n_coarse) *n_coarse = h->nc;
   return HP_OK;
 }
 

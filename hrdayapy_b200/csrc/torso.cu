@@ -874,7 +874,7 @@ __global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, floa
 }
 
 static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
-                           HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
+                           int use_net, HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
   TorsoArgs& a = h->a;
   HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol, 8, cudaMemcpyHostToDevice, s));
   int32_t is_init[N_ISCAL] = {0, 0, HP_STOP_REL, fallback_iter, 0, 0};
@@ -897,7 +897,7 @@ static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, i
     int nh = 0;
     while (true) {
       if (restart) {
-        st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, 1, s);
+        st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
         if (st != HP_OK) return st;
         fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
         restart = false;
@@ -928,7 +928,7 @@ static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, i
         continue;
       }
       if (stagnant) { fallback = true; break; }
-      st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, 1, s);
+      st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
       if (st != HP_OK) return st;
       fcg_beta<<<h->nblk, TB, 0, s>>>(a);
       fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
@@ -960,8 +960,8 @@ static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, i
 extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const float* vm,
                                               int32_t vm_on_device, float* out,
                                               int32_t out_on_device, double tol, int32_t max_iter,
-                                              int32_t fallback_iter, HpSolveStats* stats,
-                                              void* stream) {
+                                              int32_t fallback_iter, int32_t use_net,
+                                              HpSolveStats* stats, void* stream) {
   HP_REQUIRE(h && p, "hp_torso_solve_frame_fcg: null handle");
   HP_REQUIRE(max_iter >= 1 && fallback_iter >= 1, "hp_torso_solve_frame_fcg: bad iteration limits");
   HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame_fcg: tol must be positive");
@@ -969,7 +969,7 @@ extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const fl
   hp_status st = build_rhs(h, vm, vm_on_device, s);
   if (st != HP_OK) return st;
   hp_status result = HP_OK;
-  st = fcg_solve(h, p, tol, max_iter, fallback_iter, stats, &result, s);
+  st = fcg_solve(h, p, tol, max_iter, fallback_iter, use_net, stats, &result, s);
   if (st != HP_OK) return st;
   st = readout(h, out, out_on_device, s);
   if (st != HP_OK) return st;

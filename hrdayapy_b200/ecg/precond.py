@@ -33,7 +33,12 @@ def torso_arrays(solver):
 
 
 class LearnedPreconditioner:
-    def __init__(self, solver, labels, n_materials, omega=0.6, seed=0, params=None):
+    """M(r) = omega D^-1 r + Q A_c^-1 Q^T r + P(s CNN(...)) for the torso
+    solve of ``solver`` (a TorsoSolver).  coarse_agg: 0 picks the aggregate
+    size, > 0 fixes it, -1 leaves the coarse level out."""
+
+    def __init__(self, solver, labels, n_materials, omega=0.6, seed=0, params=None,
+                 coarse_agg=0):
         _lib.require_cuda()
         arr = torso_arrays(solver)
         self.solver = solver
@@ -48,11 +53,29 @@ class LearnedPreconditioner:
         d.seed = int(seed)
         self._init = None if params is None else np.ascontiguousarray(params, np.float32)
         d.init_params = _lib.ptr(self._init)
+        self._sigma = np.ascontiguousarray(solver.sigma_table, np.float64)
+        d.sigma = _lib.ptr(self._sigma)
+        d.h_m = float(solver.h_m)
+        d.coarse_agg = int(coarse_agg)
         h = C.c_void_p()
         _lib.check(_lib.lib().hp_precond_create(C.byref(d), C.byref(h), solver.stream),
                    "hp_precond_create")
         self.h = h
         self.stream = solver.stream
+
+    def coarse_info(self):
+        """(aggregate edge length, coarse unknowns); (0, 0) without a coarse level."""
+        ag, nc = C.c_int32(), C.c_int32()
+        _lib.check(_lib.lib().hp_precond_coarse_info(self.h, C.byref(ag), C.byref(nc)),
+                   "hp_precond_coarse_info")
+        return int(ag.value), int(nc.value)
+
+    def apply(self, r_ptr, z_ptr, use_net=True):
+        """z = M(r) on the padded torso grid (device pointers)."""
+        a = self.arrays
+        _lib.check(_lib.lib().hp_precond_apply(self.h, C.c_void_p(a.label), C.c_void_p(a.invd),
+                                               C.c_void_p(r_ptr), C.c_void_p(z_ptr),
+                                               int(use_net), self.stream), "hp_precond_apply")
 
     def params(self):
         n = C.c_int64()
@@ -98,7 +121,10 @@ class LearnedPreconditioner:
             float(lr), float(tol_exact), _lib.ptr(hist), self.stream), "hp_torso_train_precond")
         return hist
 
-    def solve_frame(self, vm, tol=1e-6, max_iter=5000, fallback_iter=200, out=None):
+    def solve_frame(self, vm, tol=1e-6, max_iter=5000, fallback_iter=200, out=None,
+                    use_net=True):
+        """One frame by flexible CG with M (use_net=False: without the
+        network); plain Jacobi-PCG finishes it past fallback_iter."""
         s = self.solver
         st = _lib.HpSolveStats()
         on_dev = 0
@@ -113,7 +139,7 @@ class LearnedPreconditioner:
         _lib.check(_lib.lib().hp_torso_solve_frame_fcg(s.h, self.h, vptr, on_dev, optr,
                                                        int(hasattr(out, "data_ptr")), float(tol),
                                                        int(max_iter), int(fallback_iter),
-                                                       C.byref(st), s.stream),
+                                                       int(use_net), C.byref(st), s.stream),
                    "hp_torso_solve_frame_fcg")
         return out, st
 

@@ -112,6 +112,8 @@ class TorsoSolver:
         h = C.c_void_p()
         _lib.check(L.hp_torso_create(C.byref(d), C.byref(h), self.stream), "hp_torso_create")
         self.h = h
+        self.sigma_table = sig
+        self.h_m = d.h_m
         self.n_read = len(read)
         self.n_heart = len(proj)
         self.n_rows = int(L.hp_torso_rows(h))

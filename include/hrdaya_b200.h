@@ -303,12 +303,18 @@ hp_status hp_conv3_forward(const void *X, const void *Wp, const float *bias, voi
 /* ------------------------------------------------------------------ */
 
 /*
- * M(r) = omega D^-1 r + P(s * CNN([R(D^-1 r) / s, geometry])) on a network
- * grid of half the torso resolution (see csrc/precond.cu).  Torso dims must
- * be multiples of (8, 8, 256).  label: HOST unpadded material labels;
+ * M(r) = omega D^-1 r + Q A_c^-1 Q^T r + P(s * CNN([R(D^-1 r) / s, geometry]))
+ * with Q the aggregation over cubes of coarse_agg^3 voxels and A_c the
+ * Galerkin coarse operator (dense inverse, at most HP_PC_MAX_COARSE
+ * unknowns), and the network on a grid of half the torso resolution (see
+ * csrc/precond.cu).  Torso dims must be multiples of (8, 8, 256).  label:
+ * HOST unpadded material labels; sigma: HOST n_materials conductivities
+ * (S/m, label 0 = air) and h_m the voxel size, as given to hp_torso_create;
  * pin_cell: padded flat index of the pinned voxel; init_params: HOST flat
- * parameter vector or NULL for a seeded random initialisation.
+ * parameter vector or NULL for a seeded random initialisation; coarse_agg:
+ * 0 = automatic aggregate size, > 0 a fixed one, -1 = no coarse level.
  */
+#define HP_PC_MAX_COARSE 2048
 typedef struct {
   int32_t ni, nj, nk;
   const uint8_t *label;
@@ -317,18 +323,22 @@ typedef struct {
   float omega;
   uint64_t seed;
   const float *init_params;
+  const double *sigma;
+  double h_m;
+  int32_t coarse_agg;
 } HpPrecondDesc;
 
 typedef struct HpPrecond HpPrecond;
 
 hp_status hp_precond_create(const HpPrecondDesc *desc, HpPrecond **out, void *stream);
 /* z = M(r) over the padded torso grid (device arrays: label uint8, invd and
- * r fp32, z fp32 out); use_net = 0 applies the Jacobi term only. */
+ * r fp32, z fp32 out); use_net = 0 applies the Jacobi and coarse terms only. */
 hp_status hp_precond_apply(HpPrecond *h, const uint8_t *label, const float *invd, const float *r,
                            float *z, int32_t use_net, void *stream);
-/* One training step on the pair (r, e) (padded device fp32 arrays): forward,
- * loss ||M(r) - e||^2 / ||e||^2, backward, and an Adam step of size lr
- * (lr = 0: gradients only).  *loss_out (host) receives the loss. */
+/* One training step on the pair (r, e) (padded device fp32 arrays, A e = r):
+ * forward, loss L = 1 - (r.z)^2 / ((z.A z)(r.e)) with z = M(r) (the error
+ * energy one optimal step along z leaves), backward, and an Adam step of
+ * size lr (lr = 0: gradients only).  *loss_out (host) receives the loss. */
 hp_status hp_precond_train_step(HpPrecond *h, const uint8_t *label, const float *invd,
                                 const float *r, const float *e, float lr, float *loss_out,
                                 void *stream);
@@ -340,6 +350,8 @@ hp_status hp_precond_params(HpPrecond *h, float *host_params, float *host_grads,
  * input scale s and the device error flag, to host memory. */
 hp_status hp_precond_output(HpPrecond *h, float *host_y, float *host_scale, int32_t *host_err,
                             void *stream);
+/* Aggregate edge length and number of coarse unknowns (0, 0: no coarse level). */
+hp_status hp_precond_coarse_info(const HpPrecond *h, int32_t *agg, int32_t *n_coarse);
 hp_status hp_precond_destroy(HpPrecond *h);
 
 /* Device pointers of a torso handle's padded arrays (for the preconditioner
@@ -356,13 +368,15 @@ typedef struct {
 hp_status hp_torso_arrays(HpTorso *h, HpTorsoArrays *out);
 
 /* Flexible CG with the learned preconditioner for one frame, judged by the
- * same FP64 true relative residual <= tol.  If it has not converged after
- * fallback_iter iterations, or stagnates, the frame is finished by plain
- * Jacobi-PCG (stats->restarts counts the fallback as 1000). */
+ * same FP64 true relative residual <= tol.  use_net = 0 runs the same
+ * solver without the network (Jacobi + coarse level).  If it has not
+ * converged after fallback_iter iterations, or stagnates, the frame is
+ * finished by plain Jacobi-PCG (stats->restarts counts the fallback as
+ * 1000). */
 hp_status hp_torso_solve_frame_fcg(HpTorso *h, HpPrecond *p, const float *vm,
                                    int32_t vm_on_device, float *out, int32_t out_on_device,
                                    double tol, int32_t max_iter, int32_t fallback_iter,
-                                   HpSolveStats *stats, void *stream);
+                                   int32_t use_net, HpSolveStats *stats, void *stream);
 
 /* Trains the preconditioner on residual/error pairs generated by the plain
  * solver: for each of n_frames frames (vm_frames: device fp32, frame f at
