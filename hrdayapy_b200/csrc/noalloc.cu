@@ -71,16 +71,16 @@ residual_kernel(Params p, const uint8_t* __restrict__ label, const double* __res
         atomicAdd(bad, 1u);
       } else {
         const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-        double diag = 0.0, off = 0.0;
+        const double xg = x[g];
+        double ax = 0.0;   // face-flux form, as the solver's true residual
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
           const int ln = label[nb[f]];
           const double t = ln < p.n_materials ? face(p, l, ln) : 0.0;
-          diag += t;
-          off += t * x[nb[f]];
+          ax += t * (xg - x[nb[f]]);
         }
         const double bv = (double)b[g];
-        const double r = bv - (diag * x[g] - off);
+        const double r = bv - ax;
         rr = r * r;
         bb = bv * bv;
       }

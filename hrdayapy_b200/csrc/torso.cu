@@ -161,16 +161,17 @@ __global__ void __launch_bounds__(TB) pcg_k1(TorsoArgs a, int parity) {
     if (alpha_prev != 0.0) a.x[g] += alpha_prev * (double)pold;
     const float pn = a.invd[g] * a.r[g] + betaf * pold;
     const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    float diag = 0.0f, off = 0.0f;
+    // A p as a sum of face fluxes t (p_g - p_n): exact for equal neighbours,
+    // so a smooth p (all that is left late in a solve, after a warm start or
+    // a restart) keeps its small A p instead of a difference of two large sums
+    float ap = 0.0f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const int64_t n = nb[f];
       const float t = c_T32[l * HP_MAX_MATERIALS + a.label[n]];
-      diag += t;
       const float pnn = a.invd[n] * a.r[n] + betaf * pin_[n];
-      off += t * pnn;
+      ap += t * (pn - pnn);
     }
-    const float ap = diag * pn - off;
     pout[g] = pn;
     a.Ap[g] = ap;
     acc[0] += (double)pn * (double)ap;
@@ -251,15 +252,15 @@ __global__ void __launch_bounds__(TB) true_residual(TorsoArgs a, int reset) {
     if (!is_row(a, g)) continue;
     const int l = a.label[g];
     const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    double diag = 0.0, off = 0.0;
+    const double xg = a.x[g];
+    double ax = 0.0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const double t = c_T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
-      diag += t;
-      off += t * a.x[nb[f]];   // x is 0 on air and at the pinned voxel
+      ax += t * (xg - a.x[nb[f]]);   // x is 0 on air and at the pinned voxel
     }
     const double bb = (double)a.b[g];
-    const double rr = bb - (diag * a.x[g] - off);
+    const double rr = bb - ax;
     const float rf = (float)rr;
     if (reset) a.r[g] = rf;
     acc[0] += rr * rr;
@@ -798,15 +799,13 @@ __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
     const int l = a.label[g];
     if (l == 0 || g == a.pin) continue;
     const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    float diag = 0.0f, off = 0.0f;
+    const float pv = a.p0[g];
+    float q = 0.0f;   // face-flux form, as in pcg_k1
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const float t = c_T32[l * HP_MAX_MATERIALS + a.label[nb[f]]];
-      diag += t;
-      off += t * a.p0[nb[f]];
+      q += t * (pv - a.p0[nb[f]]);
     }
-    const float pv = a.p0[g];
-    const float q = diag * pv - off;
     a.Ap[g] = q;
     acc[0] += (double)pv * q;
     acc[1] += (double)pv * a.r[g];
