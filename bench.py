@@ -240,7 +240,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def torso_leg(prob, n_train=4, n_test=5):
+def torso_leg(prob, n_train=8, n_test=5):
     """Torso forward solve (192 x 160 x 256 voxels at 1.5 mm, lungs, blood
     pools, the biventricular shell embedded; 12-lead + 16 x 16 read-out) on
     Vm frames simulated here by the fused monodomain step (1 ms apart).  The
@@ -257,7 +257,7 @@ def torso_leg(prob, n_train=4, n_test=5):
     t_setup = time.perf_counter()
     fs = prob.frame_steps
     first = 20                                   # ms: frames from early activation on
-    last = first + 8 * n_train + n_test + 1
+    last = first + 4 * n_train + n_test + 1
     prob = dataclasses.replace(prob, n_steps=last * fs, vm_every=fs,
                                site_on=np.resize(prob.site_on, last * fs + 1))
     sim = M.MonoHandle(prob)
@@ -283,11 +283,11 @@ def torso_leg(prob, n_train=4, n_test=5):
     pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=5)
     t_setup = time.perf_counter() - t_setup
     t0 = time.perf_counter()
-    hist = pc.train(frames[0:8 * n_train:8].contiguous(), ks=tuple(range(0, 64, 8)), repeats=1,
+    hist = pc.train(frames[0:4 * n_train:4].contiguous(), ks=tuple(range(0, 64, 8)), repeats=1,
                     lr=1e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
-    test0 = 8 * n_train      # frame index (into `frames`) the held-out chain starts from
+    test0 = 4 * n_train      # frame index (into `frames`) the held-out chain starts from
     out = {}
     for name in ("plain_pcg", "two_level_fcg", "learned_fcg"):
         solver.reset()

@@ -872,9 +872,14 @@ __global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, floa
     e[g] = is_row(a, g) ? (float)(xstar[g] - a.x[g]) : 0.0f;
 }
 
-static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
-                           int use_net, HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
+// One flexible-CG run with M (use_net selects the network term) from the
+// current x; returns with *fallback set when it did not converge within
+// fallback_iter iterations, stagnated or broke down.
+static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter, int use_net,
+                         int* it_out, int* restarts_out, double* rel_out, bool* fallback,
+                         cudaStream_t s) {
   TorsoArgs& a = h->a;
+  *fallback = false;
   HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol, 8, cudaMemcpyHostToDevice, s));
   int32_t is_init[N_ISCAL] = {0, 0, HP_STOP_REL, fallback_iter, 0, 0};
   HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_init, sizeof(is_init), cudaMemcpyHostToDevice, s));
@@ -882,69 +887,93 @@ static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, i
   HP_CUDA_TRY(cudaGetLastError());
   hp_status st = read_scalars(h, s);
   if (st != HP_OK) return st;
-  double bb = h->h_scal[SC_BB];
+  const double bb = h->h_scal[SC_BB];
   double rel = bb > 0.0 ? sqrt(h->h_scal[SC_TRUE_RR] / bb) : 0.0;
-  int it = 0, restarts = 0;
-  hp_status result = HP_OK;
-  bool fallback = false;
+  int it = 0;
   if (bb == 0.0) {
     HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, a.ng * 8, s));
-    rel = 0.0;
-  } else if (rel > tol) {
-    bool restart = true;
-    double hist[8];
-    int nh = 0;
-    while (true) {
-      if (restart) {
-        st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
-        if (st != HP_OK) return st;
-        fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
-        restart = false;
-      }
-      fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
-      fcg_update<<<h->nblk, TB, 0, s>>>(a);
-      HP_CUDA_TRY(cudaGetLastError());
-      st = read_scalars(h, s);
-      if (st != HP_OK) return st;
-      it = h->h_iscal[IS_ITER];
-      if (h->h_iscal[IS_NONFINITE] || h->h_iscal[IS_BREAKDOWN]) { fallback = true; break; }
-      const double stat = h->h_scal[SC_STAT];
-      hist[nh % 8] = stat;
-      ++nh;
-      const bool stagnant = nh > 6 && stat > 0.97 * hist[(nh - 6) % 8];
-      if (h->h_iscal[IS_DONE]) {
-        if (it >= fallback_iter) { fallback = true; break; }
-        // recursive residual below tol / 2: the FP64 true residual decides
-        true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
-        st = read_scalars(h, s);
-        if (st != HP_OK) return st;
-        rel = sqrt(h->h_scal[SC_TRUE_RR] / h->h_scal[SC_BB]);
-        if (rel <= tol) break;
-        ++restarts;
-        int32_t is_re[N_ISCAL] = {0, it, HP_STOP_REL, fallback_iter, 0, 0};
-        HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_re, sizeof(is_re), cudaMemcpyHostToDevice, s));
-        restart = true;
-        continue;
-      }
-      if (stagnant) { fallback = true; break; }
+    *rel_out = 0.0;
+    *it_out = 0;
+    return HP_OK;
+  }
+  bool restart = true;
+  double hist[8];
+  int nh = 0;
+  while (rel > tol) {
+    if (restart) {
       st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
       if (st != HP_OK) return st;
-      fcg_beta<<<h->nblk, TB, 0, s>>>(a);
-      fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
+      fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
+      restart = false;
     }
+    fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
+    fcg_update<<<h->nblk, TB, 0, s>>>(a);
+    HP_CUDA_TRY(cudaGetLastError());
+    st = read_scalars(h, s);
+    if (st != HP_OK) return st;
+    it = h->h_iscal[IS_ITER];
+    if (h->h_iscal[IS_NONFINITE] || h->h_iscal[IS_BREAKDOWN]) { *fallback = true; break; }
+    const double stat = h->h_scal[SC_STAT];
+    hist[nh % 8] = stat;
+    ++nh;
+    const bool stagnant = nh > 6 && stat > 0.97 * hist[(nh - 6) % 8];
+    if (h->h_iscal[IS_DONE]) {
+      if (it >= fallback_iter) { *fallback = true; break; }
+      // recursive residual below tol / 2: the FP64 true residual decides
+      true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+      st = read_scalars(h, s);
+      if (st != HP_OK) return st;
+      rel = sqrt(h->h_scal[SC_TRUE_RR] / h->h_scal[SC_BB]);
+      if (rel <= tol) break;
+      ++*restarts_out;
+      int32_t is_re[N_ISCAL] = {0, it, HP_STOP_REL, fallback_iter, 0, 0};
+      HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_re, sizeof(is_re), cudaMemcpyHostToDevice, s));
+      restart = true;
+      continue;
+    }
+    if (stagnant) { *fallback = true; break; }
+    st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
+    if (st != HP_OK) return st;
+    fcg_beta<<<h->nblk, TB, 0, s>>>(a);
+    fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
+  }
+  *it_out = it;
+  *rel_out = rel;
+  return HP_OK;
+}
+
+// Flexible CG with the learned preconditioner.  Safeguards, in order: when
+// the run with the network fails (no convergence within fallback_iter,
+// stagnation or breakdown), FCG restarts from the current iterate without
+// the network (the two-level method, restarts += 100); when that fails too,
+// plain Jacobi-PCG finishes the frame (restarts += 1000).
+static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
+                           int use_net, HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
+  int it_total = 0, restarts = 0;
+  double rel = 0.0;
+  bool fallback = false;
+  hp_status result = HP_OK;
+  for (int net = use_net ? 1 : 0; net >= 0; --net) {
+    int it = 0;
+    const int budget = std::max(1, std::min(fallback_iter, max_iter - it_total));
+    hp_status st = fcg_run(h, p, tol, budget, net, &it, &restarts, &rel, &fallback, s);
+    if (st != HP_OK) return st;
+    it_total += it;
+    if (!fallback) break;
+    if (net == 1) restarts += 100;
   }
   if (fallback) {
     HpSolveStats st2;
     hp_status r2 = HP_OK;
-    st = pcg_solve(h, tol, HP_STOP_REL, std::max(1, max_iter - it), &st2, &r2, s);
+    hp_status st = pcg_solve(h, tol, HP_STOP_REL, std::max(1, max_iter - it_total), &st2, &r2, s);
     if (st != HP_OK) return st;
-    it += st2.iterations;
+    it_total += st2.iterations;
     rel = st2.rel_residual;
     result = r2;
     restarts += 1000;
   }
   if (stats) {
-    stats->iterations = it;
+    stats->iterations = it_total;
     stats->status = result;
     stats->rel_residual = rel;
     stats->stat = rel;

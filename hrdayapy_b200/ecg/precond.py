@@ -35,10 +35,13 @@ def torso_arrays(solver):
 class LearnedPreconditioner:
     """M(r) = omega D^-1 r + Q A_c^-1 Q^T r + P(s CNN(...)) for the torso
     solve of ``solver`` (a TorsoSolver).  coarse_agg: 0 picks the aggregate
-    size, > 0 fixes it, -1 leaves the coarse level out."""
+    size, > 0 fixes it, -1 leaves the coarse level out.  zero_output starts
+    the network with a zero output layer, so that the untrained
+    preconditioner is exactly the method without the network and training
+    only adds corrections to it."""
 
     def __init__(self, solver, labels, n_materials, omega=0.6, seed=0, params=None,
-                 coarse_agg=0):
+                 coarse_agg=0, zero_output=True):
         _lib.require_cuda()
         arr = torso_arrays(solver)
         self.solver = solver
@@ -62,6 +65,11 @@ class LearnedPreconditioner:
                    "hp_precond_create")
         self.h = h
         self.stream = solver.stream
+        if zero_output and params is None:
+            p, _ = self.params()
+            ow, ob = param_offsets()[0][-1]
+            p[ow:ob + LCOUT[-1]] = 0.0
+            self.set_params(p)
 
     def coarse_info(self):
         """(aggregate edge length, coarse unknowns); (0, 0) without a coarse level."""

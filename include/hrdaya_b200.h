@@ -369,10 +369,11 @@ hp_status hp_torso_arrays(HpTorso *h, HpTorsoArrays *out);
 
 /* Flexible CG with the learned preconditioner for one frame, judged by the
  * same FP64 true relative residual <= tol.  use_net = 0 runs the same
- * solver without the network (Jacobi + coarse level).  If it has not
- * converged after fallback_iter iterations, or stagnates, the frame is
- * finished by plain Jacobi-PCG (stats->restarts counts the fallback as
- * 1000). */
+ * solver without the network (Jacobi + coarse level).  If a run with the
+ * network has not converged after fallback_iter iterations, stagnates or
+ * breaks down, FCG restarts from the current iterate without the network
+ * (stats->restarts += 100); if that fails as well, plain Jacobi-PCG
+ * finishes the frame (stats->restarts += 1000). */
 hp_status hp_torso_solve_frame_fcg(HpTorso *h, HpPrecond *p, const float *vm,
                                    int32_t vm_on_device, float *out, int32_t out_on_device,
                                    double tol, int32_t max_iter, int32_t fallback_iter,

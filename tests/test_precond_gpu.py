@@ -45,7 +45,8 @@ def test_forward_and_gradients_vs_torch():
     import torch
     from hrdayapy_b200.ecg.precond import LearnedPreconditioner, param_offsets, LAYERS
     solver, grid, labels, table, dx, vox = _small(shape=(16, 16, 256))
-    pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=3, coarse_agg=-1)
+    pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=3, coarse_agg=-1,
+                               zero_output=False)
     try:
         arr = pc.arrays
         ng = arr.n_cells
@@ -132,12 +133,6 @@ def test_training_and_fcg_on_held_out_frames():
     solver, grid, labels, table, dx, vox = _small(seed=4)
     pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=5)
     try:
-        # start from the method without the network: zero output layer
-        from hrdayapy_b200.ecg.precond import param_offsets
-        p, _ = pc.params()
-        ow, ob = param_offsets()[0][-1]
-        p[ow:ob + 1] = 0.0
-        pc.set_params(p)
         fr = _wave_frames(vox, 16, seed=6)
         vm = torch.from_numpy(fr).cuda().contiguous()
         hist = pc.train(vm[0:16:2], ks=tuple(range(0, 64, 4)), repeats=2, lr=1e-3)
