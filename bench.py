@@ -146,6 +146,105 @@ def build_workload(name, seed=0):
     return out
 
 
+def _build_variant(v):
+    """Worker of the ensemble build (spawned process, no CUDA)."""
+    import pickle
+    from hrdayapy_b200 import synthetic
+    cache = os.environ.get("HP_BENCH_CACHE")
+    path = Path(cache) / f"ensemble_variant_{v}.pkl" if cache else None
+    if path is not None and path.exists():
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    out = synthetic.ensemble_variant(v)
+    if path is not None:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        with open(path, "wb") as f:
+            pickle.dump(out, f, protocol=4)
+    return out
+
+
+def build_ensemble_variants(n_variants=16, workers=8):
+    """The seeded ensemble's variants, built in parallel host processes
+    (spawned, so no process inherits a CUDA context)."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(workers, n_variants)) as pool:
+        return pool.map(_build_variant, range(n_variants))
+
+
+def run_ensemble(args):
+    """16 heart variants of uneven size (0.9M-3.4M voxels, shell scaled by
+    U[0.7, 1.1], sigma_l, g_Ks, g_Kr varied, own Purkinje trees) advanced by
+    one launch per step; brick shape and kernel from the autotuner (tuned on
+    the largest variant); compared with the same steps of the 16 variants run
+    one after another."""
+    import torch
+    from hrdayapy_b200 import monodomain as M
+    from hrdayapy_b200.autotune import relayout, tune
+    from hrdayapy_b200.ensemble import build_ensemble
+    t0 = time.perf_counter()
+    variants = build_ensemble_variants()
+    t_build = time.perf_counter() - t0
+    probs = [v[0] for v in variants]
+    fs = probs[0].frame_steps
+    big = int(np.argmax([p.n_myo for p in probs]))
+    cache = os.environ.get("HP_BENCH_CACHE")
+    best, table = tune(probs[big], steps=100, warmup=20,
+                       cache_path=str(Path(cache) / "autotune.json") if cache else None)
+    brick, kernel = tuple(best.layout.brick), best.kernel
+    n = (args.warmup + args.steps) * fs
+    import dataclasses
+    probs = [dataclasses.replace(relayout(p, brick), kernel=kernel, n_steps=n, vm_every=0,
+                                 frame_every=0, site_on=np.resize(p.site_on, n + 1))
+             for p in probs]
+    ens = build_ensemble(probs, gks=[v[1] for v in variants], gkr=[v[2] for v in variants])
+    ens.problem.kernel = kernel
+    stream = torch.cuda.Stream()
+
+    def timed(prob):
+        with torch.cuda.stream(stream):
+            sim = M.MonoHandle(prob, stream=M._lib.C.c_void_p(stream.cuda_stream))
+            sim.run(args.warmup * fs, graph_chunk=fs)
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.run(args.steps * fs, graph_chunk=fs)
+            e1.record(stream)
+            e1.synchronize()
+            vm = sim.voltage()[0]
+            sim.close()
+        return e0.elapsed_time(e1), vm
+
+    ms_ens, vm = timed(ens.problem)
+    n_vox = ens.problem.n_myo
+    ms_seq = 0.0
+    for p in probs:
+        ms, _ = timed(p)
+        ms_seq += ms
+    steps = args.steps * fs
+    value = n_vox * steps / (ms_ens * 1e-3)
+    line = {"metric": "ensemble voxel-steps/s", "value": value, "unit": "voxel-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_ens / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "ensemble16", "variants": len(probs), "n_voxels": int(n_vox),
+                       "voxels_per_variant": [int(p.n_myo) for p in probs],
+                       "n_purkinje": int(ens.problem.n_pk), "brick": list(brick),
+                       "kernel": {1: "brick", 2: "pipelined", 3: "split"}[kernel],
+                       "time_steps_per_bench_step": fs},
+            "sequential": {"value": n_vox * steps / (ms_seq * 1e-3),
+                           "ms_per_step": ms_seq / args.steps,
+                           "speedup_of_one_launch": ms_seq / ms_ens},
+            "autotune": table[:8], "setup_seconds": t_build,
+            "roofline": {"bound": "hbm", "bytes_per_voxel_step": 177.0,
+                         "achieved": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9,
+                         "peak": peaks()[0], "unit": "GB/s",
+                         "frac": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9 / peaks()[0]},
+            "check": {"vm_finite": bool(np.isfinite(vm).all()),
+                      "vm_range_mV": [float(vm.min()), float(vm.max())]}}
+    print(json.dumps(line), flush=True)
+
+
 def bytes_per_voxel_step(prob):
     """Algorithmic HBM bytes per myocardial voxel-step of the fused kernel:
     18 TTP06 state variables + membrane potential read and written (FP32,
@@ -435,6 +534,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble16":
+        run_ensemble(args)
     else:
         run_ours(args)
 

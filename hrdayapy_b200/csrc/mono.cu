@@ -65,8 +65,9 @@ struct MonoArgs {
   // time stepping
   double dt_d;
   float dt, Cm, dt_over_Cm;
-  float site_amp[HP_MAX_SITES];
-  const uint8_t* site_on;
+  const float* site_amp;     // n_variants x HP_MAX_SITES, uA/mm^2
+  const uint8_t* site_on;    // n_variants x site_stride pulse bitmasks
+  int64_t site_stride;       // n_steps + 1
   const float* var_gks;
   const float* var_gkr;
   // outputs
@@ -108,12 +109,15 @@ __device__ __forceinline__ CellParams pheno_params(int ph, float gks_s, float gk
   return p;
 }
 
-__device__ __forceinline__ float stim_current(const MonoArgs& a, uint32_t bits, int64_t istep) {
-  uint32_t on = bits & (uint32_t)a.site_on[istep];
+// Stimulus current of a cell of variant var at step istep: the sum of the
+// amplitudes of its sites that fire then (each variant has its own sites).
+__device__ __forceinline__ float stim_current(const MonoArgs& a, uint32_t bits, int64_t istep,
+                                              int var) {
+  uint32_t on = bits & (uint32_t)a.site_on[var * a.site_stride + istep];
   float I = 0.0f;
   while (on) {
     int s = __ffs(on) - 1;
-    I += a.site_amp[s];
+    I += a.site_amp[var * HP_MAX_SITES + s];
     on &= on - 1;
   }
   return I;
@@ -202,7 +206,7 @@ __device__ __forceinline__ void purkinje_ionic_state(const MonoArgs& a, int p, f
   const float Iion = ttp06_step(Vn, c, a.dt, cp);
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p] = c.v[v];
-  const float Is = stim_current(a, a.pk_stim[p], istep);
+  const float Is = stim_current(a, a.pk_stim[p], istep, var);
   Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
@@ -320,7 +324,7 @@ __device__ __forceinline__ void voxel_ionic(const MonoArgs& a, int64_t slot, uin
   const float Iion = ttp06_step(Vn, cs, a.dt, cp);
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
-  const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep);
+  const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
   Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
@@ -1045,7 +1049,7 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   HP_REQUIRE(!d->anisotropic || d->n_bricks == 0 || (d->wface && d->doff),
              "hp_mono_create: anisotropic needs wface and doff");
   HP_REQUIRE(d->n_pk == 0 || (d->pk_ptr && d->pk_stim), "hp_mono_create: missing Purkinje arrays");
-  HP_REQUIRE(d->site_on, "hp_mono_create: missing site_on");
+  HP_REQUIRE(d->site_on && (d->n_sites == 0 || d->site_amp), "hp_mono_create: missing site tables");
   HP_REQUIRE(d->n_myo >= 0 && (d->n_myo == 0 || d->slot_of_node), "hp_mono_create: missing slot_of_node");
   HP_REQUIRE(d->kernel >= 0 && d->kernel <= 3, "hp_mono_create: kernel must be 0..3");
 
@@ -1129,8 +1133,17 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   a.dt = (float)d->dt;
   a.Cm = (float)d->Cm;
   a.dt_over_Cm = (float)(d->dt / d->Cm);
-  for (int i = 0; i < d->n_sites; ++i) a.site_amp[i] = d->site_amp[i];
-  HP_TRY(up(h, (uint8_t**)&a.site_on, d->site_on, d->n_steps + 1, s));
+  {
+    // per-variant site tables: amplitudes padded to HP_MAX_SITES per variant
+    std::vector<float> amp((size_t)d->n_variants * HP_MAX_SITES, 0.0f);
+    for (int v = 0; v < d->n_variants; ++v)
+      for (int i = 0; i < d->n_sites; ++i)
+        amp[(size_t)v * HP_MAX_SITES + i] = d->site_amp[(size_t)v * d->n_sites + i];
+    HP_TRY(up(h, (float**)&a.site_amp, amp.data(), amp.size(), s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));  // amp is a stack temporary
+  }
+  a.site_stride = d->n_steps + 1;
+  HP_TRY(up(h, (uint8_t**)&a.site_on, d->site_on, (size_t)d->n_variants * (d->n_steps + 1), s));
   HP_TRY(up(h, (float**)&a.var_gks, d->variant_gks, d->n_variants, s));
   HP_TRY(up(h, (float**)&a.var_gkr, d->variant_gkr, d->n_variants, s));
   // outputs

@@ -183,9 +183,16 @@ class MonoHandle:
         d.Cm = float(prob.Cm)
         d.v0 = float(prob.v0)
         d.n_steps = int(prob.n_steps)
-        d.n_sites = len(prob.site_amp)
-        d.site_amp = k(prob.site_amp if len(prob.site_amp) else np.zeros(1), np.float32)
-        d.site_on = k(prob.site_on, np.uint8)
+        # site tables: (n_sites,) / (n_steps + 1,) for one heart, one row per
+        # variant for an ensemble
+        amp = np.atleast_2d(np.asarray(prob.site_amp, np.float32))
+        on = np.atleast_2d(np.asarray(prob.site_on, np.uint8))
+        if amp.shape[0] != nvar or on.shape != (nvar, prob.n_steps + 1):
+            raise ValueError(f"site tables {amp.shape} / {on.shape} do not match {nvar} variants "
+                             f"and {prob.n_steps} steps")
+        d.n_sites = amp.shape[1]
+        d.site_amp = k(amp if amp.size else np.zeros((nvar, 1)), np.float32)
+        d.site_on = k(on, np.uint8)
         d.n_myo = prob.n_myo
         d.slot_of_node = k(lay.slot_of_node, np.int32)
         d.vm_every = int(prob.vm_every)

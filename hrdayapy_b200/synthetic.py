@@ -330,9 +330,9 @@ def junction_bands(nodes_vox, el, act, S, h, n_bands=7, amp=1.0, dur=2.0):
     return sites
 
 
-def biv_shell_problem(seed=0, **kw_over):
+def biv_shell_problem(seed=0, scale=1.05, n=256, **kw_over):
     from . import monodomain as M
-    args, fib, kw = biv_shell(seed=seed)
+    args, fib, kw = biv_shell(n=n, seed=seed, scale=scale)
     kw.update(kw_over)
     nodes, el, act, S, phi = args
     if kw.get("stim_protocol") is None:
@@ -353,6 +353,21 @@ def biv_shell_problem(seed=0, **kw_over):
                            vm_save_dt=None, save_every=None, **kwp)
     prob.frame_steps = 50
     return prob, info
+
+
+def ensemble_variant(v, seed=0):
+    """Variant v of the seeded 16-heart ensemble: the biventricular shell
+    scaled by s ~ U[0.7, 1.1], longitudinal conductivity ~ U[0.2, 0.4] S/m,
+    g_Ks and g_Kr multipliers ~ U[0.5, 1.5], its own tree / jitter seed.
+    Returns (prepared problem, g_Ks multiplier, g_Kr multiplier)."""
+    rng = np.random.default_rng([seed, v])
+    s = rng.uniform(0.7, 1.1)
+    sigma_l = rng.uniform(0.2, 0.4)
+    gks, gkr = rng.uniform(0.5, 1.5, 2)
+    # the grid grows with the heart (h stays 0.4 mm) so no variant is clipped
+    n = int(np.ceil(256 * max(1.0, s) / 8) * 8)
+    prob, _ = biv_shell_problem(seed=1000 + v, scale=1.05 * s, n=n, sigma_l=sigma_l)
+    return prob, float(gks), float(gkr)
 
 
 # --------------------------------------------------------------------------

@@ -115,14 +115,14 @@ typedef struct {
   const int32_t *pmj_pk;
   const float *pmj_coef;
 
-  /* time stepping and stimulus */
+  /* time stepping and stimulus (each variant has its own n_sites sites) */
   double dt;                    /* ms */
   double Cm;                    /* uF/mm^2 */
   float v0;                     /* initial membrane potential, mV */
   int64_t n_steps;              /* total steps of the run */
   int32_t n_sites;
-  const float *site_amp;        /* n_sites, uA/mm^2 */
-  const uint8_t *site_on;       /* n_steps + 1 bitmasks: sites firing at t = step * dt */
+  const float *site_amp;        /* n_variants x n_sites, uA/mm^2 */
+  const uint8_t *site_on;       /* n_variants x (n_steps + 1) bitmasks: sites firing at t = step * dt */
 
   /* outputs */
   int32_t n_myo;                /* myocardial nodes in reference order */

@@ -1,0 +1,80 @@
+"""Batched ensembles of heart variants (hrdayapy_b200.ensemble): host-side
+concatenation on the CPU, and on the GPU one ensemble run against separate
+runs of its variants -- every variant must evolve bit for bit as it does
+alone."""
+import numpy as np
+import pytest
+
+from tests import cases
+
+
+def _variant(seed, shape, T, brick=(4, 4, 8)):
+    from hrdayapy_b200 import monodomain as M
+    args, fibre, kw = cases.ragged_aniso_case(seed=seed, shape=shape, T=T)
+    nodes, el, act, S, phi = args
+    kwx = dict(kw, A_P=2.0 / kw["R_P"])
+    prob, _ = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=True,
+                        vm_save_dt=kw["dt"], act_threshold=-20.0, deact_threshold=-20.0,
+                        brick=brick, **kwx)
+    return prob
+
+
+def test_concatenation_keeps_variants_apart():
+    from hrdayapy_b200.ensemble import build_ensemble
+    pa = _variant(11, (28, 24, 18), 2.0)
+    pb = _variant(12, (24, 20, 16), 2.0)
+    ens = build_ensemble([pa, pb], gks=[1.0, 1.4], gkr=[1.0, 0.6])
+    p = ens.problem
+    na, nb_ = pa.layout.n_bricks, pb.layout.n_bricks
+    assert p.layout.n_bricks == na + nb_ and p.n_myo == pa.n_myo + pb.n_myo
+    assert p.n_pk == pa.n_pk + pb.n_pk
+    nbr = p.layout.brick_nbr
+    # neighbour tables never cross variants
+    assert ((nbr[:na] < na) | (nbr[:na] < 0)).all()
+    assert ((nbr[na:] >= na) | (nbr[na:] < 0)).all()
+    assert (p.brick_variant[:na] == 0).all() and (p.brick_variant[na:] == 1).all()
+    # Purkinje CSR of variant b points into b's nodes / slots
+    idx = p.pk_idx[p.pk_ptr[pa.n_pk]:]
+    pk = idx[idx >= 0]
+    slots = -idx[idx < 0] - 1
+    assert (pk >= pa.n_pk).all() and (slots >= pa.layout.n_slots).all()
+    assert p.site_amp.shape[0] == 2 and p.site_on.shape == (2, pa.n_steps + 1)
+    np.testing.assert_array_equal(p.site_on[1], pb.site_on)
+    a_part, b_part = ens.split(np.arange(p.n_myo))
+    assert len(a_part) == pa.n_myo and len(b_part) == pb.n_myo
+    with pytest.raises(ValueError):
+        build_ensemble([pa, _variant(12, (24, 20, 16), 2.0, brick=(4, 8, 8))])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_ensemble_matches_separate_runs(kernel):
+    from hrdayapy_b200 import monodomain as M
+    from hrdayapy_b200.ensemble import build_ensemble
+    pa = _variant(11, (28, 24, 18), 20.0)
+    pb = _variant(12, (24, 20, 16), 20.0)
+    gks, gkr = [1.0, 1.4], [1.0, 0.6]
+    ens = build_ensemble([pa, pb], gks=gks, gkr=gkr)
+
+    def run(p):
+        p.kernel = kernel
+        sim = M.MonoHandle(p)
+        sim.run(p.n_steps, graph_chunk=50)
+        vm = sim.vm_frames()
+        a, na, d, nd = sim.events()
+        sim.close()
+        return vm, a, na
+
+    vm_e, act_e, n_e = run(ens.problem)
+    for v, p in enumerate((pa, pb)):
+        p.variant_gks = np.array([gks[v]])
+        p.variant_gkr = np.array([gkr[v]])
+        vm_s, act_s, n_s = run(p)
+        np.testing.assert_array_equal(ens.split(vm_e)[v], vm_s)
+        np.testing.assert_array_equal(ens.split(act_e)[v], act_s)
+        np.testing.assert_array_equal(ens.split(n_e)[v], n_s)
+    # the ionic scaling reaches the second variant: it differs from an unscaled run
+    pb.variant_gks = None
+    pb.variant_gkr = None
+    vm_u, _, _ = run(pb)
+    assert np.abs(ens.split(vm_e)[1] - vm_u).max() > 0.1
