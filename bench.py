@@ -268,8 +268,16 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     prob, info = build_workload(args.workload)
-    prob.kernel = args.kernel
     fs = prob.frame_steps
+    tune_table = None
+    if args.kernel:
+        prob.kernel = args.kernel
+    elif args.autotune:
+        from hrdayapy_b200.autotune import tune
+        cache = os.environ.get("HP_BENCH_CACHE")
+        prob, tune_table = tune(prob, steps=100, warmup=20,
+                                cache_path=str(Path(cache) / "autotune.json") if cache else None)
+        prob.frame_steps = fs
     total_steps = (args.warmup + args.steps) * fs
     prob.n_steps = total_steps
     prob.site_on = np.resize(prob.site_on, total_steps + 1)
@@ -319,6 +327,7 @@ def run_ours(args):
                        "n_purkinje": int(prob.n_pk), "dt_ms": prob.dt,
                        "time_steps_per_bench_step": fs, "brick": list(prob.layout.brick),
                        "kernel": {1: "brick", 2: "pipelined", 3: "split"}[kinfo[0]], "grid": kinfo[1],
+                       "autotuned": tune_table is not None,
                        "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -331,6 +340,8 @@ def run_ours(args):
         }
         if args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(prob, info, args)
+        if tune_table is not None:
+            line["autotune"] = [{k: v for k, v in t.items()} for t in tune_table[:8]]
         if args.torso:
             line["torso"] = torso_leg(prob)
         print(json.dumps(line), flush=True)
@@ -527,6 +538,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-torso", dest="torso", action="store_false",
                     help="skip the torso ms/frame leg (plain PCG vs learned FCG)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default brick shape and kernel instead of timing candidates")
     ap.add_argument("--kernel", type=int, default=0,
                     help="monodomain step kernel: 0 auto, 1 per-brick, 2 pipelined, 3 split")
     args = ap.parse_args()
