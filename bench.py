@@ -1,19 +1,24 @@
-"""Benchmark: monodomain voxel-steps/s of the fused sm_100a time step.
+"""Benchmark: monodomain voxel-steps/s of the sm_100a time step, and torso
+ECG solve ms/frame (plain PCG vs learned FCG at 1e-6).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
-                    [--impl ours|reference]
+                    [--impl ours|reference] [--no-torso] [--no-autotune]
 
 One bench step = one Vm frame of simulated time (frame_steps time steps,
 1 ms at dt = 0.02 ms) of the whole workload, inputs resident in HBM.  The
 per-step working set (19 FP32 state arrays + coefficients, hundreds of MB)
 is larger than the 126 MB L2, so no explicit flush is needed between
-steps.  Prints ONE JSON line (rank 0).
+steps.  Prints ONE JSON line (rank 0); for the default workload it carries a
+"torso" object with the ECG forward solve on frames the step simulated.
 
 Workloads (seeded synthetic inputs, see hrdayapy_b200/synthetic.py):
   biv_shell  -- biventricular shell, ~2.5M voxels in 256^3 at 0.4 mm,
                 helical fibres, endo/M/epi layers, fractal Purkinje tree
                 (the configuration the headline metric is quoted on)
   slab64     -- 64x64x16 isotropic slab at 0.25 mm (the CPU-runnable case)
+  ensemble16 -- 16 shell variants of uneven size in one launch per step
+                against the same variants run one after another
+  torso      -- the torso solve alone (--torso-shape) on seeded frames
 
 --impl reference times the CPU restatement of the reference method (FP64,
 all host threads) on a bounded sample of the same workload.
@@ -243,6 +248,74 @@ def run_ensemble(args):
             "check": {"vm_finite": bool(np.isfinite(vm).all()),
                       "vm_range_mV": [float(vm.min()), float(vm.max())]}}
     print(json.dumps(line), flush=True)
+
+
+def run_torso(args):
+    """Torso forward solve alone: the biventricular shell embedded in an
+    elliptic-cylinder torso of --torso-shape voxels (extent 288 x 240 x 384
+    mm, lungs, blood pools), seeded activation-front Vm frames 1 ms apart,
+    each frame warm-started from the previous one and solved to the FP64
+    true relative residual 1e-6 by plain Jacobi-PCG, by two-level FCG and by
+    learned FCG (network trained for a few seconds on earlier frames)."""
+    import torch
+    from hrdayapy_b200 import synthetic
+    from hrdayapy_b200.ecg import torso as T
+    from hrdayapy_b200.ecg.precond import LearnedPreconditioner
+    from hrdayapy_b200.ecg.torso_grid import torso_grid_from_labels
+    shape = tuple(int(x) for x in args.torso_shape.split(","))
+    dx = 288.0 / shape[0]
+    geo = synthetic.biv_geometry()
+    lab, sm, reg = synthetic.torso_for_heart(geo, shape=shape, dx=dx)
+    grid = torso_grid_from_labels(lab, sm, dx)
+    labels, table = T.labels_from_grid(grid)
+    vox = np.argwhere(geo["S"] == 1)
+    coords = vox[:, [1, 0, 2]].astype(np.float64) * geo["h"]
+    proj, _ = T.projection_map(coords, reg["R"], reg["t"], 1.0, grid["origin_mm"], dx,
+                               grid["active_id_map"], grid["shape"])
+    solver = T.TorsoSolver(labels, table, dx, grid["pin_row"], T.heart_neighbours(vox), proj,
+                           0.2625, geo["h"], grid["surface_rows"][:266])
+    x = vox[:, 0].astype(np.float64) + 0.4 * vox[:, 2]
+    n_fr = 8 + args.warmup + args.steps + 1
+    lo, hi = x.min(), x.max()
+    rng = np.random.default_rng(0)
+    frames = np.stack([(-85.0 + 110.0 / (1.0 + np.exp(-(lo + (hi - lo) * (f + 0.5) / n_fr - x) / 1.5))
+                        + rng.normal(0, 0.3, len(x))) for f in range(n_fr)]).astype(np.float32)
+    fr = torch.from_numpy(frames).cuda()
+    out = {}
+    pc = None
+    for name in ("plain_pcg", "two_level_fcg", "learned_fcg"):
+        if name != "plain_pcg" and pc is None:
+            pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=5)
+            pc.train(fr[0:8].contiguous(), ks=tuple(range(0, 64, 8)), repeats=1, lr=1e-3)
+        solver.reset()
+        its, ms = [], []
+        for f in range(8, n_fr):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            if name == "plain_pcg":
+                _, st = solver.solve_frame(fr[f], 1e-6, "rel", 50000)
+            else:
+                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 2000, use_net=(name == "learned_fcg"))
+            torch.cuda.synchronize()
+            if f >= 8 + 1 + args.warmup:
+                ms.append((time.perf_counter() - t1) * 1e3)
+                its.append(int(st.iterations))
+        out[name] = {"ms_per_frame": float(np.mean(ms)), "iterations": its}
+    rows = solver.n_rows
+    if pc is not None:
+        pc.close()
+    solver.close()
+    p = out["plain_pcg"]
+    t_it = p["ms_per_frame"] * 1e-3 / max(np.mean(p["iterations"]), 1)
+    peak, kind = peaks()
+    print(json.dumps({"metric": "torso solve ms/frame", "value": out["learned_fcg"]["ms_per_frame"],
+                      "unit": "ms/frame", "higher_is_better": False, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "data": "synthetic (seeded)",
+                      "config": {"workload": f"torso {shape} @{dx} mm", "rows": int(rows)}, **out,
+                      "pcg_roofline": {"bound": "hbm", "bytes_per_unknown_per_iteration": 40,
+                                       "achieved": 40.0 * rows / t_it / 1e9, "peak": peak,
+                                       "frac": 40.0 * rows / t_it / 1e9 / peak,
+                                       "peak_source": kind}}), flush=True)
 
 
 def bytes_per_voxel_step(prob):
@@ -536,6 +609,8 @@ def main():
     ap.add_argument("--workload", default="biv_shell")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--torso-shape", default="192,160,256",
+                    help="torso voxels for --workload torso (extent fixed at 288 x 240 x 384 mm)")
     ap.add_argument("--no-torso", dest="torso", action="store_false",
                     help="skip the torso ms/frame leg (plain PCG vs learned FCG)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -549,6 +624,8 @@ def main():
         run_reference(args)
     elif args.workload == "ensemble16":
         run_ensemble(args)
+    elif args.workload == "torso":
+        run_torso(args)
     else:
         run_ours(args)
 
