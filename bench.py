@@ -295,7 +295,7 @@ def run_torso(args):
             if name == "plain_pcg":
                 _, st = solver.solve_frame(fr[f], 1e-6, "rel", 50000)
             else:
-                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 2000, use_net=(name == "learned_fcg"))
+                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 300, use_net=(name == "learned_fcg"))
             torch.cuda.synchronize()
             if f >= 8 + 1 + args.warmup:
                 ms.append((time.perf_counter() - t1) * 1e3)
@@ -482,7 +482,7 @@ def torso_leg(prob, n_train=8, n_test=5):
             if name == "plain_pcg":
                 _, st = solver.solve_frame(frames[f], 1e-6, "rel", 50000)
             else:
-                _, st = pc.solve_frame(frames[f], 1e-6, 50000, 2000,
+                _, st = pc.solve_frame(frames[f], 1e-6, 50000, 300,
                                        use_net=(name == "learned_fcg"))
             torch.cuda.synchronize()
             ms.append((time.perf_counter() - t1) * 1e3)

@@ -142,45 +142,56 @@ __device__ __forceinline__ bool is_row(const TorsoArgs& a, int64_t g) {
   return a.label[g] != 0 && g != a.pin;
 }
 
-// Iteration part 1: pending x update, p <- z + beta p (z = M^-1 r), Ap = A p,
-// partial p.Ap.
-__global__ void __launch_bounds__(TB) pcg_k1(TorsoArgs a, int parity) {
+// Iteration part 1a: pending x update and p <- M^-1 r + beta p, in place
+// (one buffer: every thread reads and writes only its own cells).
+__global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
-  const double beta = a.scal[SC_BETA];
   const double alpha_prev = a.scal[SC_ALPHA_PREV];
-  const float betaf = (float)beta;
-  const float* __restrict__ pin_ = parity ? a.p1 : a.p0;
-  float* __restrict__ pout = parity ? a.p0 : a.p1;
+  const float betaf = (float)a.scal[SC_BETA];
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ invd = a.invd;
+  const float* __restrict__ r = a.r;
+  float* __restrict__ p = a.p0;
+  double* __restrict__ x = a.x;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
+#pragma unroll 4
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
+    if (lab[g] == 0 || g == pin) continue;
+    const float pold = p[g];
+    if (alpha_prev != 0.0) x[g] += alpha_prev * (double)pold;
+    p[g] = invd[g] * r[g] + betaf * pold;
+  }
+}
+
+// Iteration part 1b: Ap = A p as a sum of face fluxes t (p_g - p_n) (exact
+// for equal neighbours, so a smooth p keeps its small A p instead of a
+// difference of two large sums), partial p.Ap; the last block forms alpha
+// and clears the pending x update (part 1a applied it).
+__global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
+  if (a.iscal[IS_DONE]) return;
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ p = a.p0;
+  float* __restrict__ Ap = a.Ap;
   const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[1] = {0.0};
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
-       g += (int64_t)gridDim.x * TB) {
-    const int l = a.label[g];
-    if (l == 0 || g == a.pin) continue;
-    const float pold = pin_[g];
-    if (alpha_prev != 0.0) a.x[g] += alpha_prev * (double)pold;
-    const float pn = a.invd[g] * a.r[g] + betaf * pold;
+#pragma unroll 2
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
+    const int l = lab[g];
+    if (l == 0 || g == pin) continue;
+    const float pg = p[g];
     const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    // A p as a sum of face fluxes t (p_g - p_n): exact for equal neighbours,
-    // so a smooth p (all that is left late in a solve, after a warm start or
-    // a restart) keeps its small A p instead of a difference of two large sums
     float ap = 0.0f;
 #pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      const int64_t n = nb[f];
-      const float t = c_T32[l * HP_MAX_MATERIALS + a.label[n]];
-      const float pnn = a.invd[n] * a.r[n] + betaf * pin_[n];
-      ap += t * (pn - pnn);
-    }
-    pout[g] = pn;
-    a.Ap[g] = ap;
-    acc[0] += (double)pn * (double)ap;
+    for (int f = 0; f < 6; ++f) ap += c_T32[l * HP_MAX_MATERIALS + lab[nb[f]]] * (pg - p[nb[f]]);
+    Ap[g] = ap;
+    acc[0] += (double)pg * (double)ap;
   }
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double pAp = tot[0];
     a.scal[SC_PAP] = pAp;
-    a.scal[SC_ALPHA_PREV] = 0.0;   // every block applied the pending x update
+    a.scal[SC_ALPHA_PREV] = 0.0;   // every block of part 1a applied the pending x update
     if (!(fabs(pAp) >= 1e-30) || !isfinite(pAp)) {   // breakdown, as the reference's |pAp| < 1e-30
       a.iscal[IS_BREAKDOWN] = isfinite(pAp) ? 1 : 0;
       a.iscal[IS_NONFINITE] = isfinite(pAp) ? 0 : 1;
@@ -198,13 +209,18 @@ __global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float alphaf = (float)alpha;
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ invd = a.invd;
+  const float* __restrict__ Ap = a.Ap;
+  float* __restrict__ rv = a.r;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
-       g += (int64_t)gridDim.x * TB) {
-    if (!is_row(a, g)) continue;
-    const float r = a.r[g] - alphaf * a.Ap[g];
-    a.r[g] = r;
-    const float z = a.invd[g] * r;
+#pragma unroll 4
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
+    if (lab[g] == 0 || g == pin) continue;
+    const float r = rv[g] - alphaf * Ap[g];
+    rv[g] = r;
+    const float z = invd[g] * r;
     acc[0] += (double)r * z;
     acc[1] += (double)z * z;
     acc[2] += (double)r * r;
@@ -234,9 +250,9 @@ __global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
 }
 
 // x += alpha_prev * p (the pending update of the last iteration).
-__global__ void __launch_bounds__(TB) pcg_finish_x(TorsoArgs a, int parity) {
+__global__ void __launch_bounds__(TB) pcg_finish_x(TorsoArgs a) {
   const double alpha = a.scal[SC_ALPHA_PREV];
-  const float* __restrict__ p = parity ? a.p1 : a.p0;
+  const float* __restrict__ p = a.p0;
   for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng;
        g += (int64_t)gridDim.x * TB)
     if (is_row(a, g)) a.x[g] += alpha * (double)p[g];
@@ -572,19 +588,19 @@ extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; 
 
 static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
   for (int q = 0; q < n; ++q) {
-    pcg_k1<<<h->nblk, TB, 0, s>>>(h->a, h->parity);
+    pcg_p_update<<<h->nblk, TB, 0, s>>>(h->a);
+    pcg_ap<<<h->nblk, TB, 0, s>>>(h->a);
     pcg_k2<<<h->nblk, TB, 0, s>>>(h->a);
-    h->parity ^= 1;
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
 
-// CG iterations in chunks of `chunk` (a CUDA graph per parity), with the
+// CG iterations in chunks of `chunk` (one CUDA graph), with the
 // host reading the done flag once per chunk.  Kernels after convergence
 // inside a chunk return immediately.
 static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
-  const int chunk = 8;   // even, so the p-buffer parity is the same after every chunk
+  const int chunk = 8;
   if (s == nullptr) {    // the legacy default stream cannot be captured
     for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
       hp_status st = iter_launch(h, chunk, s);
@@ -596,26 +612,21 @@ static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
     return HP_OK;
   }
   if (!h->graph[0] || h->graph_stream != s) {
-    for (int par = 0; par < 2; ++par) {
-      if (h->graph[par]) cudaGraphExecDestroy(h->graph[par]);
-      h->graph[par] = nullptr;
-      const int save = h->parity;
-      h->parity = par;
-      cudaGraph_t g;
-      HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      hp_status st = iter_launch(h, chunk, s);
-      cudaError_t ce = cudaStreamEndCapture(s, &g);
-      h->parity = save;
-      if (st != HP_OK) return st;
-      HP_CUDA_TRY(ce);
-      HP_CUDA_TRY(cudaGraphInstantiate(&h->graph[par], g, 0));
-      cudaGraphDestroy(g);
-    }
+    if (h->graph[0]) cudaGraphExecDestroy(h->graph[0]);
+    h->graph[0] = nullptr;
+    cudaGraph_t g;
+    HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    hp_status st = iter_launch(h, chunk, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (st != HP_OK) return st;
+    HP_CUDA_TRY(ce);
+    HP_CUDA_TRY(cudaGraphInstantiate(&h->graph[0], g, 0));
+    cudaGraphDestroy(g);
     h->graph_chunk = chunk;
     h->graph_stream = s;
   }
   for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
-    HP_CUDA_TRY(cudaGraphLaunch(h->graph[h->parity], s));
+    HP_CUDA_TRY(cudaGraphLaunch(h->graph[0], s));
     HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
     if (h->h_iscal[IS_DONE]) break;
@@ -683,18 +694,14 @@ static hp_status pcg_solve(HpTorso* h, double tol, int rule, int max_iter, HpSol
     if (total_it >= max_iter) { result = HP_ERR_NOT_CONVERGED; break; }
     int32_t is_run[N_ISCAL] = {0, 0, rule, max_iter - total_it, 0, 0};
     HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_run, sizeof(is_run), cudaMemcpyHostToDevice, s));
-    const int par0 = h->parity;
     hp_status st = run_iterations(h, max_iter - total_it, s);
     if (st != HP_OK) return st;
     st = read_scalars(h, s);
     if (st != HP_OK) return st;
     const int its = h->h_iscal[IS_ITER];
     total_it += its;
-    // iteration q (0-based) reads parity par0 ^ (q & 1) and writes the other
-    const int last_out = (par0 ^ ((its - 1) & 1)) ^ 1;
-    h->parity = (par0 ^ (its & 1));
     if (its > 0) {
-      pcg_finish_x<<<h->nblk, TB, 0, s>>>(a, last_out);
+      pcg_finish_x<<<h->nblk, TB, 0, s>>>(a);
       HP_CUDA_TRY(cudaGetLastError());
     }
     if (h->h_iscal[IS_NONFINITE]) { result = HP_ERR_NONFINITE; break; }
