@@ -754,24 +754,36 @@ mono_diffuse_kernel(MonoArgs a, int step_off) {
 
 constexpr int ION_THREADS = 128;
 
-__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+// The split step keeps the 18 TTP06 states in compact tissue order (index
+// i of active_slot, not the slot), so the ionic half's state loads and
+// stores are fully coalesced; tag, V and W stay per slot for the stencil.
+// mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
+__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off,
+                                                                   int mode) {
   const int64_t step = *a.d_step + step_off;
   const bool odd = step & 1;
+  const int64_t istep = mode ? 0 : step + 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < a.n_active) {
     const int64_t slot = a.active_slot[i];
     const uint32_t tag = a.tag[slot];
     const float Vn = a.Vpost[slot];
+    const int64_t na = a.n_active;
     CellState cs;
 #pragma unroll
-    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * a.n_slots + slot];
+    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + i];
     const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
-    voxel_ionic(a, slot, tag, tag & HP_TAG_PHENO_MASK, Vn, cs, step + 1, var,
-                odd ? a.Vs0 : a.Vs1);
+    const CellParams cp = pheno_params(tag & HP_TAG_PHENO_MASK, a.var_gks[var], a.var_gkr[var]);
+    const float Iion = ttp06_step(Vn, cs, a.dt, cp);
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
+    const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
+    float* __restrict__ Wout = mode ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
+    Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
   } else {
     const int p = i - a.n_active_pad;
     if (p >= 0 && p < a.n_pk)
-      purkinje_ionic(a, p, a.pk_Vpost[p], step + 1, odd ? a.pk_Vs0 : a.pk_Vs1);
+      purkinje_ionic(a, p, a.pk_Vpost[p], istep, mode ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
   }
 }
 
@@ -932,7 +944,9 @@ static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) 
   if (grid == 0) return HP_OK;
   if (mode == 0 && h->diff) {
     h->diff<<<h->diff_grid, h->bv, h->diff_smem, s>>>(h->a, step_off);
-    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
+    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off, 0);
+  } else if (mode == 1 && h->diff) {
+    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off, 1);
   } else if (mode == 0 && h->pipe)
     h->pipe<<<h->pipe_grid, h->bv, h->pipe_smem, s>>>(h->a, step_off);
   else
@@ -1000,6 +1014,10 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   h->a.n_active_pad = (int32_t)((act.size() + 31) / 32 * 32);
   h->a.bv_shift = shift;
   h->diff = d->anisotropic ? se->diff_aniso : se->diff_iso;
+  // states in compact tissue order (resting state, as for the slot order)
+  if (!act.empty())
+    init_cells_kernel<<<1024, 256, 0, s>>>(h->a.state, h->a.Vpost, (int64_t)act.size(), d->v0);
+  HP_CUDA_TRY(cudaGetLastError());
   // diffusion half: persistent CTAs over bricks, halo copy table per shape
   const std::vector<uint32_t> tab = se->halo(d->anisotropic != 0);
   if ((int)tab.size() > (d->anisotropic ? se->diff_cap_aniso : se->diff_cap_iso)) {
@@ -1360,9 +1378,25 @@ extern "C" hp_status hp_mono_copy_v(HpMono* h, float* v_myo, float* v_pk, void* 
 extern "C" hp_status hp_mono_copy_state(HpMono* h, float* st_slots, float* st_pk, void* stream) {
   HP_REQUIRE(h, "hp_mono_copy_state: null handle");
   cudaStream_t s = (cudaStream_t)stream;
-  if (st_slots && h->a.n_slots)
+  if (st_slots && h->a.n_slots) {
     HP_CUDA_TRY(cudaMemcpyAsync(st_slots, h->a.state, (size_t)N_STATE * h->a.n_slots * sizeof(float),
                                 cudaMemcpyDeviceToHost, s));
+    if (h->diff) {
+      // the split step stores states in compact tissue order: scatter to slots
+      HP_CUDA_TRY(cudaStreamSynchronize(s));
+      const int64_t ns = h->a.n_slots, na = h->a.n_active;
+      std::vector<int32_t> act(na);
+      if (na) HP_CUDA_TRY(cudaMemcpy(act.data(), h->a.active_slot, na * 4, cudaMemcpyDeviceToHost));
+      std::vector<float> tmp((size_t)N_STATE * na);
+      for (int v = 0; v < N_STATE; ++v)
+        std::copy(st_slots + (size_t)v * na, st_slots + (size_t)(v + 1) * na, tmp.begin() + (size_t)v * na);
+      for (int v = 0; v < N_STATE; ++v) {
+        float* dst = st_slots + (size_t)v * ns;
+        std::fill(dst, dst + ns, 0.0f);
+        for (int64_t i = 0; i < na; ++i) dst[act[i]] = tmp[(size_t)v * na + i];
+      }
+    }
+  }
   if (st_pk && h->a.n_pk)
     HP_CUDA_TRY(cudaMemcpyAsync(st_pk, h->a.pk_state, (size_t)N_STATE * h->a.n_pk * sizeof(float),
                                 cudaMemcpyDeviceToHost, s));

@@ -101,6 +101,27 @@ def test_step_kernels_identical(brick, aniso):
         np.testing.assert_array_equal(res[0][4], r[4])
 
 
+def test_state_readback_same_for_every_kernel():
+    """hp_mono_copy_state reports the 18 TTP06 states in node order whatever
+    the kernel's internal state order (the split step keeps them compact)."""
+    from hrdayapy_b200 import monodomain as M
+    args, fibre, kw = cases.ragged_aniso_case(T=3.0)
+    nodes, el, act, S, phi = args
+    out = []
+    for k in (1, 2, 3):
+        prob, _ = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=True,
+                            vm_save_dt=kw["dt"], **dict(kw, A_P=2.0 / kw["R_P"]))
+        prob.kernel = k
+        sim = M.MonoHandle(prob)
+        sim.run(prob.n_steps)
+        out.append(sim.state())
+        sim.close()
+    for st, sp in out[1:]:
+        np.testing.assert_array_equal(st, out[0][0])
+        np.testing.assert_array_equal(sp, out[0][1])
+    assert np.isfinite(out[0][0]).all() and out[0][0][0].min() > 100.0     # Ki ~ 138 mM
+
+
 def test_graph_and_direct_launch_agree():
     from hrdayapy_b200 import monodomain as M
     args, fibre, kw = cases.aniso_case()
