@@ -168,12 +168,14 @@ def _build_variant(v):
     return out
 
 
-def build_ensemble_variants(n_variants=16, workers=8):
-    """The seeded ensemble's variants, built in parallel host processes
-    (spawned, so no process inherits a CUDA context)."""
+def build_ensemble_variants(which, workers=8):
+    """Variants `which` of the seeded ensemble, built in parallel host
+    processes (spawned, so no process inherits a CUDA context)."""
     import multiprocessing as mp
-    with mp.get_context("spawn").Pool(min(workers, n_variants)) as pool:
-        return pool.map(_build_variant, range(n_variants))
+    if not which:
+        return []
+    with mp.get_context("spawn").Pool(min(workers, len(which))) as pool:
+        return pool.map(_build_variant, which)
 
 
 def run_ensemble(args):
@@ -181,13 +183,30 @@ def run_ensemble(args):
     U[0.7, 1.1], sigma_l, g_Ks, g_Kr varied, own Purkinje trees) advanced by
     one launch per step; brick shape and kernel from the autotuner (tuned on
     the largest variant); compared with the same steps of the 16 variants run
-    one after another."""
+    one after another.  With N ranks the variants are dealt to ranks by
+    longest-processing-time-first on their expected voxel counts (s^3); each
+    rank advances its share as one ensemble, no data-path collective, and
+    the job's time is the slowest rank's."""
     import torch
-    from hrdayapy_b200 import monodomain as M
+    from hrdayapy_b200 import monodomain as M, synthetic
     from hrdayapy_b200.autotune import relayout, tune
     from hrdayapy_b200.ensemble import build_ensemble
+    from hrdayapy_b200.sharding import gather_to_all, lpt_assign, max_over_ranks
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    n_var = 16
+    share = lpt_assign([synthetic.ensemble_params(v)[0] ** 3 for v in range(n_var)],
+                       world)[rank]
     t0 = time.perf_counter()
-    variants = build_ensemble_variants()
+    variants = build_ensemble_variants(share)
     t_build = time.perf_counter() - t0
     probs = [v[0] for v in variants]
     fs = probs[0].frame_steps
@@ -220,20 +239,34 @@ def run_ensemble(args):
             sim.close()
         return e0.elapsed_time(e1), vm
 
+    if dist:
+        dist.barrier()
     ms_ens, vm = timed(ens.problem)
-    n_vox = ens.problem.n_myo
+    n_local = ens.problem.n_myo
     ms_seq = 0.0
     for p in probs:
         ms, _ = timed(p)
         ms_seq += ms
+    ms_ens = max_over_ranks(ms_ens, device="cuda" if dist else None)
+    ms_seq = max_over_ranks(ms_seq, device="cuda" if dist else None)
+    per_rank = gather_to_all({"variants": share, "voxels": int(n_local),
+                              "sizes": [int(p.n_myo) for p in probs]})
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    n_vox = sum(r["voxels"] for r in per_rank)
     steps = args.steps * fs
     value = n_vox * steps / (ms_ens * 1e-3)
     line = {"metric": "ensemble voxel-steps/s", "value": value, "unit": "voxel-steps/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_ens / args.steps, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_ens / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "ensemble16", "variants": len(probs), "n_voxels": int(n_vox),
-                       "voxels_per_variant": [int(p.n_myo) for p in probs],
+            "config": {"workload": "ensemble16", "variants": n_var, "n_voxels": int(n_vox),
+                       "voxels_per_rank": [r["voxels"] for r in per_rank],
+                       "variants_per_rank": [r["variants"] for r in per_rank],
+                       "parallelism": f"variants sharded over {world} rank(s), LPT",
                        "n_purkinje": int(ens.problem.n_pk), "brick": list(brick),
                        "kernel": {1: "brick", 2: "pipelined", 3: "split"}[kernel],
                        "time_steps_per_bench_step": fs},
@@ -242,9 +275,9 @@ def run_ensemble(args):
                            "speedup_of_one_launch": ms_seq / ms_ens},
             "autotune": table[:8], "setup_seconds": t_build,
             "roofline": {"bound": "hbm", "bytes_per_voxel_step": 177.0,
-                         "achieved": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9,
-                         "peak": peaks()[0], "unit": "GB/s",
-                         "frac": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9 / peaks()[0]},
+                         "achieved": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9 / world,
+                         "peak": peaks()[0], "unit": "GB/s (per GPU)",
+                         "frac": n_vox * 177.0 / (ms_ens * 1e-3 / steps) / 1e9 / world / peaks()[0]},
             "check": {"vm_finite": bool(np.isfinite(vm).all()),
                       "vm_range_mV": [float(vm.min()), float(vm.max())]}}
     print(json.dumps(line), flush=True)

@@ -355,15 +355,22 @@ def biv_shell_problem(seed=0, scale=1.05, n=256, **kw_over):
     return prob, info
 
 
-def ensemble_variant(v, seed=0):
-    """Variant v of the seeded 16-heart ensemble: the biventricular shell
-    scaled by s ~ U[0.7, 1.1], longitudinal conductivity ~ U[0.2, 0.4] S/m,
-    g_Ks and g_Kr multipliers ~ U[0.5, 1.5], its own tree / jitter seed.
-    Returns (prepared problem, g_Ks multiplier, g_Kr multiplier)."""
+def ensemble_params(v, seed=0):
+    """(scale s ~ U[0.7, 1.1], sigma_l ~ U[0.2, 0.4] S/m, g_Ks and g_Kr
+    multipliers ~ U[0.5, 1.5]) of variant v of the seeded ensemble."""
     rng = np.random.default_rng([seed, v])
     s = rng.uniform(0.7, 1.1)
     sigma_l = rng.uniform(0.2, 0.4)
     gks, gkr = rng.uniform(0.5, 1.5, 2)
+    return float(s), float(sigma_l), float(gks), float(gkr)
+
+
+def ensemble_variant(v, seed=0):
+    """Variant v of the seeded 16-heart ensemble: the biventricular shell
+    scaled by s, longitudinal conductivity sigma_l, g_Ks / g_Kr multipliers
+    (ensemble_params), its own tree / jitter seed.  Returns (prepared
+    problem, g_Ks multiplier, g_Kr multiplier)."""
+    s, sigma_l, gks, gkr = ensemble_params(v, seed)
     # the grid grows with the heart (h stays 0.4 mm) so no variant is clipped
     n = int(np.ceil(256 * max(1.0, s) / 8) * 8)
     prob, _ = biv_shell_problem(seed=1000 + v, scale=1.05 * s, n=n, sigma_l=sigma_l)
