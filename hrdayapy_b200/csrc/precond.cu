@@ -254,7 +254,7 @@ __global__ void relu_mask_kernel(__nv_bfloat16* __restrict__ g, const __nv_bfloa
 
 // Coarse level: per aggregate the sum of r over its active, unpinned cells.
 struct CoarseArgs {
-  int ni, nj, nk, pj, pk, ag, nbj, nbk, nc;
+  int ni, nj, nk, pj, pk, ag, ag_shift, nbj, nbk, nc;
   int64_t pin;
   const uint8_t* label;
   const int32_t* c_box;   // nc aggregate boxes
@@ -264,31 +264,34 @@ struct CoarseArgs {
   float* zc;
 };
 
+// aggregate edge lengths are powers of two: shifts instead of divisions
 __device__ __forceinline__ int coarse_of(const CoarseArgs& c, int i, int j, int k) {
-  return c.box2c[((i / c.ag) * c.nbj + j / c.ag) * c.nbk + k / c.ag];
+  const int sh = c.ag_shift;
+  return c.box2c[((i >> sh) * c.nbj + (j >> sh)) * c.nbk + (k >> sh)];
 }
 
 __global__ void __launch_bounds__(TB) coarse_restrict_kernel(CoarseArgs c, const float* __restrict__ r) {
   const int I = blockIdx.x;
   const int b = c.c_box[I];
   const int bk = b % c.nbk, bj = (b / c.nbk) % c.nbj, bi = b / (c.nbk * c.nbj);
-  const int n = c.ag * c.ag * c.ag;
+  const int sh = c.ag_shift, m = c.ag - 1;
+  const int n = 1 << (3 * sh);
   double acc = 0.0;
   for (int t = threadIdx.x; t < n; t += TB) {
-    const int i = bi * c.ag + t / (c.ag * c.ag), j = bj * c.ag + (t / c.ag) % c.ag,
-              k = bk * c.ag + t % c.ag;
+    const int i = (bi << sh) + (t >> (2 * sh)), j = (bj << sh) + ((t >> sh) & m),
+              k = (bk << sh) + (t & m);
     if (i >= c.ni || j >= c.nj || k >= c.nk) continue;
     const int64_t g = ((int64_t)(i + 1) * c.pj + (j + 1)) * c.pk + (k + 1);
     if (c.label[g] != 0 && g != c.pin) acc += (double)r[g];
   }
-  __shared__ double sh[TB];
-  sh[threadIdx.x] = acc;
+  __shared__ double red[TB];
+  red[threadIdx.x] = acc;
   __syncthreads();
   for (int st = TB / 2; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
     __syncthreads();
   }
-  if (threadIdx.x == 0) c.rc[I] = sh[0];
+  if (threadIdx.x == 0) c.rc[I] = red[0];
 }
 
 // zc = A_c^-1 rc, one warp per row
@@ -340,18 +343,22 @@ struct ProlongArgs {
   int use_net;
 };
 
-// z = omega * invd * r + s * y[parent] on active fine cells (0 elsewhere)
-__global__ void prolong_kernel(ProlongArgs a, float* __restrict__ z) {
+// z = omega * invd * r + s * y[parent] + zc[aggregate] on active fine cells
+// (0 elsewhere); one block per padded (i, j) row, threads along k, so the
+// coordinates come from the launch shape instead of divisions.
+__global__ void __launch_bounds__(TB) prolong_kernel(ProlongArgs a, float* __restrict__ z) {
   const float s = a.use_net ? a.scale[2] : 0.0f;
-  const int64_t SI = (int64_t)a.pj * a.pk;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
-       g += (int64_t)gridDim.x * blockDim.x) {
+  const int i = blockIdx.y, j = blockIdx.x;
+  const int64_t row = ((int64_t)i * a.pj + j) * a.pk;
+  const bool inner = i > 0 && j > 0 && j < a.pj - 1 && i < (int)(a.ng / ((int64_t)a.pj * a.pk)) - 1;
+  for (int k = threadIdx.x; k < a.pk; k += TB) {
+    const int64_t g = row + k;
     float v = 0.0f;
-    if (a.label[g] != 0 && g != a.pin) {
+    if (inner && a.label[g] != 0 && g != a.pin) {
       v = a.omega * a.invd[g] * a.r[g];
-      const int i = (int)(g / SI) - 1, j = (int)((g / a.pk) % a.pj) - 1, k = (int)(g % a.pk) - 1;
-      if (a.use_net) v += s * a.y[((int64_t)(i / 2) * a.cd.H + j / 2) * a.cd.W + k / 2];
-      if (a.c.nc > 0) v += a.c.zc[coarse_of(a.c, i, j, k)];
+      const int ui = i - 1, uj = j - 1, uk = k - 1;
+      if (a.use_net) v += s * a.y[((int64_t)(ui >> 1) * a.cd.H + (uj >> 1)) * a.cd.W + (uk >> 1)];
+      if (a.c.nc > 0) v += a.c.zc[coarse_of(a.c, ui, uj, uk)];
     }
     z[g] = v;
   }
@@ -703,6 +710,8 @@ static hp_status coarse_setup(HpPrecond* h, const HpPrecondDesc* d, cudaStream_t
   auto unknown = [&](int i, int j, int k) {
     return lab(i, j, k) != 0 && !(i == pin_i && j == pin_j && k == pin_k);
   };
+  HP_REQUIRE(d->coarse_agg <= 0 || (d->coarse_agg & (d->coarse_agg - 1)) == 0,
+             "hp_precond_create: coarse_agg must be a power of two");
   int ag = d->coarse_agg > 0 ? d->coarse_agg : 4;
   std::vector<int32_t> box2c, c_box;
   int nbi = 0, nbj = 0, nbk = 0;
@@ -951,7 +960,9 @@ static void wgrad(HpPrecond* h, int l, const __nv_bfloat16* X, const __nv_bfloat
 static int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)); }
 
 static CoarseArgs coarse_args(const HpPrecond* h, const uint8_t* label) {
-  return CoarseArgs{h->ni, h->nj, h->nk, h->pj, h->pk, h->ag, h->nbj, h->nbk, h->nc, h->pin,
+  int sh = 0;
+  while ((1 << sh) < h->ag) ++sh;
+  return CoarseArgs{h->ni, h->nj, h->nk, h->pj, h->pk, h->ag, sh, h->nbj, h->nbk, h->nc, h->pin,
                     label, h->c_box, h->box2c, h->ainv, h->rc, h->zc};
 }
 
@@ -1015,7 +1026,7 @@ hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, c
   }
   ProlongArgs pa{coarse_args(h, label), h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y,
                  h->scale, h->omega, h->L[1], use_net};
-  prolong_kernel<<<grid_for(h->ng), 256, 0, s>>>(pa, z);
+  prolong_kernel<<<dim3(h->pj, (unsigned)(h->ng / ((int64_t)h->pj * h->pk))), TB, 0, s>>>(pa, z);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
@@ -1042,7 +1053,7 @@ extern "C" hp_status hp_precond_train_step(HpPrecond* h, const uint8_t* label, c
   const int64_t n1 = L1.n(), n2 = L2.n(), n3 = L3.n();
   ProlongArgs pa{coarse_args(h, label), h->pj, h->pk, h->ng, h->pin, label, invd, r, h->y,
                  h->scale, h->omega, h->L[1], 1};
-  prolong_kernel<<<grid_for(h->ng), 256, 0, s>>>(pa, h->zbuf);
+  prolong_kernel<<<dim3(h->pj, (unsigned)(h->ng / ((int64_t)h->pj * h->pk))), TB, 0, s>>>(pa, h->zbuf);
   EnergyArgs ea{h->pj, h->pk, h->ng, h->pin, label, h->T32, r, e, h->zbuf, h->az};
   energy_dots_kernel<<<h->nblk, TB, 0, s>>>(ea, h->part);
   sum3_kernel<<<1, TB, 0, s>>>(h->part, h->nblk, h->dots);

@@ -39,9 +39,11 @@ constexpr int NPART = 4;           // partial sums per block
 
 enum Scal : int {
   SC_RZ = 0, SC_PAP, SC_ALPHA, SC_BETA, SC_ALPHA_PREV, SC_ZZ, SC_ZMAX, SC_RR, SC_BB,
-  SC_TRUE_RR, SC_SRC_MEAN, SC_STAT, SC_TOL, N_SCAL
+  SC_TRUE_RR, SC_SRC_MEAN, SC_STAT, SC_TOL, SC_HIST0, N_SCAL = SC_HIST0 + 8
 };
-enum IScal : int { IS_DONE = 0, IS_ITER, IS_RULE, IS_MAXIT, IS_BREAKDOWN, IS_NONFINITE, N_ISCAL };
+enum IScal : int {
+  IS_DONE = 0, IS_ITER, IS_RULE, IS_MAXIT, IS_BREAKDOWN, IS_NONFINITE, IS_STAGNANT, IS_NH, N_ISCAL
+};
 
 struct TorsoArgs {
   int64_t ng;          // padded grid cells
@@ -391,6 +393,9 @@ struct HpTorso {
   int parity;
   bool have_x;
   cudaGraphExec_t graph[2];
+  cudaGraphExec_t fcg_graph[2];   // FCG chunk without / with the network
+  const void* fcg_graph_pc;       // preconditioner handle the FCG graphs hold
+  cudaStream_t fcg_graph_stream;
   int graph_chunk;
   cudaStream_t graph_stream;
 };
@@ -483,6 +488,9 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   h->graph[0] = h->graph[1] = nullptr;
   h->graph_chunk = 0;
   h->graph_stream = nullptr;
+  h->fcg_graph[0] = h->fcg_graph[1] = nullptr;
+  h->fcg_graph_pc = nullptr;
+  h->fcg_graph_stream = nullptr;
   h->ni = ni; h->nj = nj; h->nk = nk;
   h->n_rows = n_rows;
   h->parity = 0;
@@ -836,12 +844,19 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float af = (float)alpha;
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ p = a.p0;
+  const float* __restrict__ Ap = a.Ap;
+  float* __restrict__ rv = a.r;
+  double* __restrict__ x = a.x;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[1] = {0.0};
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB) {
-    if (!is_row(a, g)) continue;
-    a.x[g] += alpha * (double)a.p0[g];
-    const float r = a.r[g] - af * a.Ap[g];
-    a.r[g] = r;
+#pragma unroll 4
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
+    if (lab[g] == 0 || g == pin) continue;
+    x[g] += alpha * (double)p[g];
+    const float r = rv[g] - af * Ap[g];
+    rv[g] = r;
     acc[0] += (double)r * r;
   }
   double tot[1];
@@ -850,33 +865,82 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
     const double stat = sqrt(tot[0] / fmax(a.scal[SC_BB], 1e-300));
     a.scal[SC_STAT] = stat;
     const int it = ++a.iscal[IS_ITER];
+    // stagnation: less than 3 % progress over the last 5 iterations
+    const int nh = ++a.iscal[IS_NH];
+    a.scal[SC_HIST0 + (nh - 1) % 8] = stat;
+    const bool stagnant = nh > 6 && stat > 0.97 * a.scal[SC_HIST0 + (nh - 6) % 8];
     if (!isfinite(tot[0])) { a.iscal[IS_NONFINITE] = 1; a.iscal[IS_DONE] = 1; }
     else if (stat < 0.5 * a.scal[SC_TOL] || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
+    else if (stagnant) { a.iscal[IS_STAGNANT] = 1; a.iscal[IS_DONE] = 1; }
   }
 }
 
 // partial z.q (z in p1); last block: beta = -z.q / p.q
 __global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a) {
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ z = a.p1;
+  const float* __restrict__ Ap = a.Ap;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[1] = {0.0};
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB)
-    if (is_row(a, g)) acc[0] += (double)a.p1[g] * a.Ap[g];
+#pragma unroll 4
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride)
+    if (lab[g] != 0 && g != pin) acc[0] += (double)z[g] * Ap[g];
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0)
     a.scal[SC_BETA] = -tot[0] / a.scal[SC_PAP];
 }
 
 // p = z + beta p
-__global__ void fcg_p(TorsoArgs a, int first) {
+__global__ void __launch_bounds__(TB) fcg_p(TorsoArgs a, int first) {
   const float beta = first ? 0.0f : (float)a.scal[SC_BETA];
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
-       g += (int64_t)gridDim.x * blockDim.x)
-    if (is_row(a, g)) a.p0[g] = a.p1[g] + beta * a.p0[g];
+  const uint8_t* __restrict__ lab = a.label;
+  const float* __restrict__ z = a.p1;
+  float* __restrict__ p = a.p0;
+  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
+#pragma unroll 4
+  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride)
+    if (lab[g] != 0 && g != pin) p[g] = z[g] + beta * p[g];
 }
 
 __global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, float* __restrict__ e) {
   for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < a.ng;
        g += (int64_t)gridDim.x * blockDim.x)
     e[g] = is_row(a, g) ? (float)(xstar[g] - a.x[g]) : 0.0f;
+}
+
+constexpr int FCG_CHUNK = 4;
+
+// The FCG iteration body (A p, x / r update and stopping tests, z = M(r),
+// beta, p) for FCG_CHUNK iterations, captured once per network setting,
+// stream and preconditioner handle.
+static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s) {
+  const int q = use_net ? 1 : 0;
+  if (h->fcg_graph[q] && h->fcg_graph_stream == s && h->fcg_graph_pc == (const void*)p)
+    return HP_OK;
+  if (h->fcg_graph_stream != s || h->fcg_graph_pc != (const void*)p) {
+    for (int k = 0; k < 2; ++k)
+      if (h->fcg_graph[k]) { cudaGraphExecDestroy(h->fcg_graph[k]); h->fcg_graph[k] = nullptr; }
+  }
+  TorsoArgs& a = h->a;
+  cudaGraph_t g;
+  HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  hp_status st = HP_OK;
+  for (int it = 0; it < FCG_CHUNK && st == HP_OK; ++it) {
+    fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
+    fcg_update<<<h->nblk, TB, 0, s>>>(a);
+    st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
+    if (st != HP_OK) break;
+    fcg_beta<<<h->nblk, TB, 0, s>>>(a);
+    fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
+  }
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (st != HP_OK) return st;
+  HP_CUDA_TRY(ce);
+  HP_CUDA_TRY(cudaGraphInstantiate(&h->fcg_graph[q], g, 0));
+  cudaGraphDestroy(g);
+  h->fcg_graph_stream = s;
+  h->fcg_graph_pc = (const void*)p;
+  return HP_OK;
 }
 
 // One flexible-CG run with M (use_net selects the network term) from the
@@ -903,9 +967,17 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
     *it_out = 0;
     return HP_OK;
   }
-  bool restart = true;
-  double hist[8];
-  int nh = 0;
+  // chunks of FCG_CHUNK iterations replayed from a CUDA graph; kernels of a
+  // chunk after the device-side done flag return at once (the
+  // preconditioner's then only writes its own scratch and z)
+  // z = M(r0), p = z (this first application also sets up anything the
+  // preconditioner initialises lazily, before the capture)
+  st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
+  if (st != HP_OK) return st;
+  fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
+  st = fcg_graph(h, p, use_net, s);
+  if (st != HP_OK) return st;
+  bool restart = false;
   while (rel > tol) {
     if (restart) {
       st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
@@ -913,19 +985,16 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
       fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
       restart = false;
     }
-    fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
-    fcg_update<<<h->nblk, TB, 0, s>>>(a);
-    HP_CUDA_TRY(cudaGetLastError());
+    HP_CUDA_TRY(cudaGraphLaunch(h->fcg_graph[use_net ? 1 : 0], s));
     st = read_scalars(h, s);
     if (st != HP_OK) return st;
     it = h->h_iscal[IS_ITER];
-    if (h->h_iscal[IS_NONFINITE] || h->h_iscal[IS_BREAKDOWN]) { *fallback = true; break; }
-    const double stat = h->h_scal[SC_STAT];
-    hist[nh % 8] = stat;
-    ++nh;
-    const bool stagnant = nh > 6 && stat > 0.97 * hist[(nh - 6) % 8];
+    if (h->h_iscal[IS_NONFINITE] || h->h_iscal[IS_BREAKDOWN] || h->h_iscal[IS_STAGNANT]) {
+      *fallback = true;
+      break;
+    }
     if (h->h_iscal[IS_DONE]) {
-      if (it >= fallback_iter) { *fallback = true; break; }
+      if (h->h_scal[SC_STAT] >= 0.5 * tol) { *fallback = true; break; }   // iteration budget
       // recursive residual below tol / 2: the FP64 true residual decides
       true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
       st = read_scalars(h, s);
@@ -936,13 +1005,7 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
       int32_t is_re[N_ISCAL] = {0, it, HP_STOP_REL, fallback_iter, 0, 0};
       HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_re, sizeof(is_re), cudaMemcpyHostToDevice, s));
       restart = true;
-      continue;
     }
-    if (stagnant) { *fallback = true; break; }
-    st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
-    if (st != HP_OK) return st;
-    fcg_beta<<<h->nblk, TB, 0, s>>>(a);
-    fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
   }
   *it_out = it;
   *rel_out = rel;
@@ -1098,8 +1161,10 @@ extern "C" hp_status hp_torso_reset(HpTorso* h) {
 
 extern "C" hp_status hp_torso_destroy(HpTorso* h) {
   if (!h) return HP_OK;
-  for (int q = 0; q < 2; ++q)
+  for (int q = 0; q < 2; ++q) {
     if (h->graph[q]) cudaGraphExecDestroy(h->graph[q]);
+    if (h->fcg_graph[q]) cudaGraphExecDestroy(h->fcg_graph[q]);
+  }
   for (void* p : h->allocs) cudaFree(p);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->h_iscal) cudaFreeHost(h->h_iscal);
