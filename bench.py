@@ -448,12 +448,50 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_baseline(prob, info, args)
         if tune_table is not None:
             line["autotune"] = [{k: v for k, v in t.items()} for t in tune_table[:8]]
+        if args.theta:
+            line["theta_scheme"] = theta_leg(prob)
         if args.torso:
             line["torso"] = torso_leg(prob)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def theta_leg(prob, n_steps=100, warm=20, theta=0.5, cg_tol=1e-5):
+    """The reference's default diffusion half (theta = 0.5, Crank-Nicolson,
+    relative tolerance 1e-5) on the same heart: ms per time step including
+    the per-step convergence test on the host, CG iterations per step, and
+    the split into stencil passes and vector kernels."""
+    import dataclasses
+    import torch
+    from hrdayapy_b200 import monodomain as M
+    n = warm + n_steps
+    p = dataclasses.replace(prob, theta=theta, cn_tol=cg_tol, cn_max_iter=100, kernel=0,
+                            n_steps=n, site_on=np.resize(prob.site_on, n + 1), vm_every=0,
+                            frame_every=0)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        sim = M.MonoHandle(p, stream=M._lib.C.c_void_p(stream.cuda_stream))
+        sim.run(warm)
+        it0, s0, _, _ = sim.cn_stats()
+        stream.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim.run(n_steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        it1, s1, unconv, brk = sim.cn_stats()
+        vm = sim.voltage()[0]
+        sim.close()
+    return {"theta": theta, "cg_tol": cg_tol, "steps": n_steps,
+            "ms_per_step": ms / n_steps,
+            "voxel_steps_per_s": prob.n_myo * n_steps / (ms * 1e-3),
+            "cg_iters_per_step": (it1 - it0) / max(1, s1 - s0),
+            "unconverged": unconv, "breakdowns": brk,
+            "vm_finite": bool(np.isfinite(vm).all())}
 
 
 def torso_leg(prob, n_train=8, n_test=5):
@@ -644,6 +682,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--torso-shape", default="192,160,256",
                     help="torso voxels for --workload torso (extent fixed at 288 x 240 x 384 mm)")
+    ap.add_argument("--no-theta", dest="theta", action="store_false",
+                    help="skip the theta = 0.5 (Crank-Nicolson) leg")
     ap.add_argument("--no-torso", dest="torso", action="store_false",
                     help="skip the torso ms/frame leg (plain PCG vs learned FCG)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",

@@ -45,6 +45,8 @@ class HpMonoDesc(C.Structure):
         ("n_surf", C.c_int32), ("surf_of_slot", P), ("frame_every", C.c_int64),
         ("act_threshold", C.c_float), ("deact_threshold", C.c_float), ("max_events", C.c_int32),
         ("kernel", C.c_int32),
+        ("theta", C.c_double), ("cn_tol", C.c_double), ("cn_max_iter", C.c_int32),
+        ("pk_weight", C.c_float),
     ]
 
 
@@ -66,6 +68,7 @@ def lib():
     L.hp_mono_run.argtypes = [P, C.c_int64, C.c_int32, P]
     L.hp_mono_steps_done.argtypes = [P]
     L.hp_mono_steps_done.restype = C.c_int64
+    L.hp_mono_cn_stats.argtypes = [P, P, P, P, P]
     L.hp_mono_copy_vm.argtypes = [P, C.c_int64, C.c_int64, P, C.c_int32, P]
     L.hp_mono_copy_frames.argtypes = [P, C.c_int64, C.c_int64, P, P, C.c_int32, P]
     L.hp_mono_copy_events.argtypes = [P, P, P, P, P, P]

@@ -4,7 +4,8 @@ the signatures of the reference's hrdayapy/anisotropic_simulation/coupled.py
 purkinje_myocardium_anisotropic_solver.py:1308-1360.
 
 A_P is derived as 2 / R_P and passing it raises TypeError, as in the
-reference (:1519-1526).  Only theta = 0 is accepted (fused explicit step).
+reference (:1519-1526).  theta = 0 runs the fused explicit step, 0 < theta
+<= 1 (default 0.5) the theta-scheme with a CG solve per step.
 """
 from __future__ import annotations
 

@@ -178,17 +178,33 @@ __device__ __forceinline__ void load_region(float* __restrict__ tile,
 // junction edges to myocardial slots), same skewed step as the voxels.
 // Diffusion half: V_{i+1} of node p from W_i, stored in pk_Vpost (and the
 // animation frame of step i).
+// Row sum of Purkinje node p: sum_q coef_q (W_j - W_p) over its cable and
+// junction edges (Purkinje potentials in Wpk, myocardial ones in Wmyo).
+// DIAG: the diagonal of the row instead (every difference reads -1).
+template <bool DIAG = false>
+__device__ __forceinline__ float purkinje_acc(const MonoArgs& a, int p,
+                                              const float* __restrict__ Wpk,
+                                              const float* __restrict__ Wmyo) {
+  const float Vc = DIAG ? 0.0f : Wpk[p];
+  float acc = 0.0f;
+  for (int q = a.pk_ptr[p]; q < a.pk_ptr[p + 1]; ++q) {
+    if constexpr (DIAG) {
+      acc += a.pk_coef[q] * -1.0f;
+    } else {
+      const int j = a.pk_idx[q];
+      const float Vj = j >= 0 ? Wpk[j] : Wmyo[-(int64_t)j - 1];
+      acc += a.pk_coef[q] * (Vj - Vc);
+    }
+  }
+  return acc;
+}
+
 __device__ __forceinline__ float purkinje_diffuse(const MonoArgs& a, int p, int64_t step) {
   const bool odd = step & 1;
   const float* __restrict__ Win = odd ? a.pk_Vs1 : a.pk_Vs0;
   const float* __restrict__ Wmyo = odd ? a.Vs1 : a.Vs0;
   const float Vc = Win[p];
-  float acc = 0.0f;
-  for (int q = a.pk_ptr[p]; q < a.pk_ptr[p + 1]; ++q) {
-    const int j = a.pk_idx[q];
-    const float Vj = j >= 0 ? Win[j] : Wmyo[-(int64_t)j - 1];
-    acc += a.pk_coef[q] * (Vj - Vc);
-  }
+  const float acc = purkinje_acc(a, p, Win, Wmyo);
   const float Vn = fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
   a.pk_Vpost[p] = Vn;
   if (a.frame_every > 0 && step % a.frame_every == 0)
@@ -228,35 +244,38 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   }
 }
 
-// Diffusion half of one voxel: V_{i+1} = clamp(W + sum coef (W_j - W), ...)
-// from shared tiles with strides SI (i), SJ (j), 1 (k); face weights and
-// off-diagonal tensor components are three tiles each, NS floats apart.
-template <int SI, int SJ, int NS, bool ANISO>
-__device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, const float* tW,
-                                         const float* tD, int c, uint32_t tag, int64_t slot,
-                                         bool odd) {
-  const float Vc = tV[c];
+// Stencil sum of one voxel, sum_j coef_ij (W_j - W_i) including its junction
+// currents (Purkinje potentials from Wpk), from shared tiles with strides SI
+// (i), SJ (j), 1 (k); face weights and off-diagonal tensor components are
+// three tiles each, NS floats apart.
+template <int SI, int SJ, int NS, bool ANISO, bool DIAG = false>
+__device__ __forceinline__ float stencil_acc(const MonoArgs& a, const float* tV, const float* tW,
+                                             const float* tD, int c, uint32_t tag, int64_t slot,
+                                             const float* __restrict__ Wpk) {
+  // DIAG: every difference reads -1, so the sum is the operator's diagonal
+#define HP_DV(x) (DIAG ? -1.0f : ((x) - Vc))
+  const float Vc = DIAG ? 0.0f : tV[c];
   float acc = 0.0f;
   const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
   if constexpr (!ANISO) {
     float s = 0.0f;
-    if (fb & 1u) s += tV[c + SI] - Vc;
-    if (fb & 2u) s += tV[c - SI] - Vc;
-    if (fb & 4u) s += tV[c + SJ] - Vc;
-    if (fb & 8u) s += tV[c - SJ] - Vc;
-    if (fb & 16u) s += tV[c + 1] - Vc;
-    if (fb & 32u) s += tV[c - 1] - Vc;
+    if (fb & 1u) s += HP_DV(tV[c + SI]);
+    if (fb & 2u) s += HP_DV(tV[c - SI]);
+    if (fb & 4u) s += HP_DV(tV[c + SJ]);
+    if (fb & 8u) s += HP_DV(tV[c - SJ]);
+    if (fb & 16u) s += HP_DV(tV[c + 1]);
+    if (fb & 32u) s += HP_DV(tV[c - 1]);
     acc = a.iso_coef * s;
   } else {
     const float* tWx = tW;
     const float* tWy = tW + NS;
     const float* tWz = tW + 2 * NS;
-    if (fb & 1u) acc += tWx[c] * (tV[c + SI] - Vc);
-    if (fb & 2u) acc += tWx[c - SI] * (tV[c - SI] - Vc);
-    if (fb & 4u) acc += tWy[c] * (tV[c + SJ] - Vc);
-    if (fb & 8u) acc += tWy[c - SJ] * (tV[c - SJ] - Vc);
-    if (fb & 16u) acc += tWz[c] * (tV[c + 1] - Vc);
-    if (fb & 32u) acc += tWz[c - 1] * (tV[c - 1] - Vc);
+    if (fb & 1u) acc += tWx[c] * HP_DV(tV[c + SI]);
+    if (fb & 2u) acc += tWx[c - SI] * HP_DV(tV[c - SI]);
+    if (fb & 4u) acc += tWy[c] * HP_DV(tV[c + SJ]);
+    if (fb & 8u) acc += tWy[c - SJ] * HP_DV(tV[c - SJ]);
+    if (fb & 16u) acc += tWz[c] * HP_DV(tV[c + 1]);
+    if (fb & 32u) acc += tWz[c - 1] * HP_DV(tV[c - 1]);
     const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
     const float* t01 = tD;
     const float* t02 = tD + NS;
@@ -264,7 +283,7 @@ __device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, con
     // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
 #define HP_DIAG(bit, T, OFF, SGN)                                            \
   if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
-                                 (tV[c + (OFF)] - Vc);
+                                 HP_DV(tV[c + (OFF)]);
     HP_DIAG(0, t01, SI + SJ, 1.0f)
     HP_DIAG(1, t01, -SI - SJ, 1.0f)
     HP_DIAG(2, t01, SI - SJ, -1.0f)
@@ -280,12 +299,22 @@ __device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, con
 #undef HP_DIAG
   }
   if (tag & HP_TAG_PMJ) {
-    const float* __restrict__ Wpk = odd ? a.pk_Vs1 : a.pk_Vs0;
     const int r = a.pmj_row[slot];
     for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
-      acc += a.pmj_coef[q] * (Wpk[a.pmj_pk[q]] - Vc);
+      acc += a.pmj_coef[q] * HP_DV(Wpk[a.pmj_pk[q]]);
   }
-  return fminf(fmaxf(Vc + acc, -150.0f), 80.0f);
+#undef HP_DV
+  return acc;
+}
+
+// Diffusion half of one voxel (explicit step): V = clamp(W + sum coef (W_j - W)).
+template <int SI, int SJ, int NS, bool ANISO>
+__device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, const float* tW,
+                                         const float* tD, int c, uint32_t tag, int64_t slot,
+                                         bool odd) {
+  const float acc = stencil_acc<SI, SJ, NS, ANISO>(a, tV, tW, tD, c, tag, slot,
+                                                   odd ? a.pk_Vs1 : a.pk_Vs0);
+  return fminf(fmaxf(tV[c] + acc, -150.0f), 80.0f);
 }
 
 // Outputs of a tissue voxel once V_{i+1} = Vn is known: the
@@ -787,6 +816,286 @@ __global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Crank-Nicolson diffusion half (theta > 0).
+//
+// The reference solves (Cm/dt) V_{i+1} - theta L V_{i+1} = (Cm/dt) W_i +
+// (1 - theta) L W_i by Jacobi-preconditioned BiCGSTAB from V_{i+1} = W_i
+// (purkinje_myocardium_pipeline.py:662-754, :1383-1391; anisotropic solver
+// :1784-1790), then clamps to [-150, 80].  With the coefficients pre-scaled
+// by dt / (Cm Ai) the system is M x = W + (1 - theta) Lh W, M = I - theta Lh.
+// Lh = D^-1 K with K symmetric and D = diag(Ai) (Ai_M on tissue, Ai_P on
+// Purkinje nodes), so M is self-adjoint in the inner product weighted by
+// Ai / Ai_M: this solver runs Jacobi-preconditioned CG in that inner product
+// (weight 1 on tissue slots, pk_weight = Ai_P / Ai_M on Purkinje nodes).
+// The stopping rule is the reference's: unweighted ||r|| <= tol ||rhs||.
+//
+// CG vectors are [slots | Purkinje nodes] of length n_slots + n_pk, FP32;
+// dot products are FP64 with deterministic last-block grid reductions.  The
+// warm-start residual rhs - M W equals Lh W, so one stencil pass gives the
+// initial residual, the norm of the right-hand side and the first direction.
+// Every iteration kernel returns at once when the done flag is set, so the
+// host may enqueue iterations in chunks and test the flag between chunks.
+enum CnScal : int { CN_BB = 0, CN_RZ, CN_PQ, CN_ALPHA, CN_BETA, CN_RR, N_CN_SCAL };
+enum CnIScal : int { CI_DONE = 0, CI_ITER, CI_TOTAL, CI_SOLVES, CI_UNCONV, CI_BREAK, N_CN_ISCAL };
+constexpr int CN_TB = 256;   // threads of the vector kernels
+constexpr int CN_NPART = 4;  // partials per block
+
+struct CnArgs {
+  int64_t n;             // n_slots + n_pk
+  float theta, omt;      // theta and 1 - theta
+  float pk_weight;       // Ai_P / Ai_M
+  double tol2;           // squared relative tolerance
+  int32_t max_iter;
+  float* x;
+  float* r;
+  float* p;
+  float* q;
+  float* dinv;           // 1 / diag(M); 0 on padding slots
+  double* part;          // grid x CN_NPART partial sums
+  double* scal;
+  int32_t* iscal;
+  unsigned int* ticket;
+};
+
+// Block-reduces NV sums into part[blockIdx.x]; true in the last block to
+// arrive, whose threads then all hold the grid totals in tot (summed in
+// block order, so the result does not depend on scheduling).
+template <int NT, int NV>
+__device__ bool cn_reduce_last(double (&v)[NV], const CnArgs& c, double (&tot)[NV]) {
+  __shared__ double sh[NT / 32][NV];
+  __shared__ double sh2[NT][NV];
+  __shared__ bool am_last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double w = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (lane == 0) sh[wid][k] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = sh[0][k];
+      for (int w = 1; w < NT / 32; ++w) s += sh[w][k];
+      c.part[(int64_t)blockIdx.x * CN_NPART + k] = s;
+    }
+    __threadfence();
+    am_last = atomicAdd(c.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += NT) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] += ((volatile double*)c.part)[(int64_t)b * CN_NPART + k];
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) sh2[threadIdx.x][k] = v[k];
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) sh2[threadIdx.x][k] += sh2[threadIdx.x + s][k];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) tot[k] = sh2[0][k];
+  if (threadIdx.x == 0) *c.ticket = 0u;
+  return true;
+}
+
+// Stencil pass of the CN solve, persistent CTAs over bricks then chunks of
+// BV Purkinje nodes.
+//   mode 0 (start of a step): x = W, r = Lh W, p = Dinv r; sums
+//          ||W + (1 - theta) Lh W||^2, ||r||^2, <r, Dinv r>_w;
+//   mode 1 (iteration): q = p - theta Lh p; sum <p, q>_w, alpha = rz / pq;
+//   mode 2 (set-up): dinv = 1 / (1 - theta diag Lh).
+template <int BI, int BJ, int BK, bool ANISO>
+__global__ void __launch_bounds__(BI * BJ * BK)
+cn_stencil_kernel(MonoArgs a, CnArgs c, int mode) {
+  using G = TileGeom<BI, BJ, BK>;
+  constexpr int BV = G::BV, SI = G::SI, SJ = G::SJ;
+  if (mode == 1 && c.iscal[CI_DONE]) return;
+  const int64_t step = *a.d_step;
+  const bool odd = step & 1;
+  const int64_t ns = a.n_slots;
+  const float* __restrict__ Smyo = mode == 0 ? (odd ? a.Vs1 : a.Vs0) : c.p;
+  const float* __restrict__ Spk = mode == 0 ? (odd ? a.pk_Vs1 : a.pk_Vs0) : c.p + ns;
+  __shared__ int nb27[27];
+  __shared__ float tV[G::N];
+  __shared__ float tW[ANISO ? 3 * G::N : 1];
+  __shared__ float tD[ANISO ? 3 * G::N : 1];
+  const int tid = threadIdx.x;
+  const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
+  const int cc = (li + 1) * SI + (lj + 1) * SJ + (lk + 1);
+  const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    if (it >= a.n_bricks) {
+      const int pn = (it - a.n_bricks) * BV + tid;
+      if (pn >= a.n_pk) continue;
+      const int64_t e = ns + pn;
+      const float w = c.pk_weight;
+      if (mode == 2) {
+        c.dinv[e] = 1.0f / (1.0f - c.theta * purkinje_acc<true>(a, pn, Spk, Smyo));
+        continue;
+      }
+      const float acc = purkinje_acc(a, pn, Spk, Smyo);
+      if (mode == 0) {
+        const float Wi = Spk[pn], z = c.dinv[e] * acc, b = Wi + c.omt * acc;
+        c.x[e] = Wi;
+        c.r[e] = acc;
+        c.p[e] = z;
+        v[0] += (double)b * b;
+        v[1] += (double)acc * acc;
+        v[2] += (double)w * acc * z;
+      } else {
+        const float pi = Spk[pn], qi = pi - c.theta * acc;
+        c.q[e] = qi;
+        v[0] += (double)w * pi * qi;
+      }
+      continue;
+    }
+    __syncthreads();  // the previous brick's tiles are no longer read
+    if (tid < 27) nb27[tid] = a.nbr[(int64_t)it * 27 + tid];
+    __syncthreads();
+    if (mode != 2) load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, -1, BK + 1>(tV, Smyo, nb27, tid);
+    if constexpr (ANISO) {
+      load_region<BI, BJ, BK, -1, BI, 0, BJ, 0, BK>(tW, a.wface, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, -1, BJ, 0, BK>(tW + G::N, a.wface + ns, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, 0, BJ, -1, BK>(tW + 2 * G::N, a.wface + 2 * ns, nb27, tid);
+      load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, 0, BK>(tD, a.doff, nb27, tid);
+      load_region<BI, BJ, BK, -1, BI + 1, 0, BJ, -1, BK + 1>(tD + G::N, a.doff + ns, nb27, tid);
+      load_region<BI, BJ, BK, 0, BI, -1, BJ + 1, -1, BK + 1>(tD + 2 * G::N, a.doff + 2 * ns, nb27, tid);
+    }
+    __syncthreads();
+    const int64_t slot = (int64_t)it * BV + tid;
+    const uint32_t tag = a.tag[slot];
+    if (!(tag & HP_TAG_PHENO_MASK)) {  // padding: keeps every vector at 0
+      if (mode == 2) c.dinv[slot] = 0.0f;
+      else if (mode == 0) c.x[slot] = c.r[slot] = c.p[slot] = 0.0f;
+      else c.q[slot] = 0.0f;
+      continue;
+    }
+    if (mode == 2) {
+      c.dinv[slot] = 1.0f / (1.0f - c.theta * stencil_acc<SI, SJ, G::N, ANISO, true>(
+                                                 a, tV, tW, tD, cc, tag, slot, Spk));
+      continue;
+    }
+    const float acc = stencil_acc<SI, SJ, G::N, ANISO>(a, tV, tW, tD, cc, tag, slot, Spk);
+    if (mode == 0) {
+      const float Wi = tV[cc], z = c.dinv[slot] * acc, b = Wi + c.omt * acc;
+      c.x[slot] = Wi;
+      c.r[slot] = acc;
+      c.p[slot] = z;
+      v[0] += (double)b * b;
+      v[1] += (double)acc * acc;
+      v[2] += (double)acc * z;
+    } else {
+      const float pi = tV[cc], qi = pi - c.theta * acc;
+      c.q[slot] = qi;
+      v[0] += (double)pi * qi;
+    }
+  }
+  if (mode == 2) return;
+  double tot[3];
+  if (!cn_reduce_last<BV, 3>(v, c, tot)) return;
+  if (threadIdx.x != 0) return;
+  if (mode == 0) {
+    c.scal[CN_BB] = tot[0];
+    c.scal[CN_RR] = tot[1];
+    c.scal[CN_RZ] = tot[2];
+    c.iscal[CI_ITER] = 0;
+    c.iscal[CI_SOLVES] += 1;
+    // converged at the warm start (also a zero right-hand side)
+    c.iscal[CI_DONE] = (tot[1] <= c.tol2 * tot[0] || tot[0] == 0.0) ? 1 : 0;
+  } else {
+    const double pq = tot[0];
+    if (!(pq > 0.0) || !isfinite(pq)) {  // breakdown: keep the current x
+      c.iscal[CI_BREAK] += 1;
+      c.iscal[CI_DONE] = 1;
+    } else {
+      c.scal[CN_PQ] = pq;
+      c.scal[CN_ALPHA] = c.scal[CN_RZ] / pq;
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q; sums ||r||^2 and <r, Dinv r>_w; the last block
+// takes beta and the stopping decision.
+__global__ void __launch_bounds__(CN_TB) cn_update_kernel(CnArgs c, int64_t ns) {
+  if (c.iscal[CI_DONE]) return;
+  const float alpha = (float)c.scal[CN_ALPHA];
+  double v[2] = {0.0, 0.0};
+  for (int64_t e = blockIdx.x * (int64_t)CN_TB + threadIdx.x; e < c.n;
+       e += (int64_t)gridDim.x * CN_TB) {
+    const float xi = c.x[e] + alpha * c.p[e];
+    const float ri = c.r[e] - alpha * c.q[e];
+    c.x[e] = xi;
+    c.r[e] = ri;
+    const float z = c.dinv[e] * ri;
+    v[0] += (double)ri * ri;
+    v[1] += (double)(e < ns ? 1.0f : c.pk_weight) * ri * z;
+  }
+  double tot[2];
+  if (!cn_reduce_last<CN_TB, 2>(v, c, tot)) return;
+  if (threadIdx.x != 0) return;
+  const int it = c.iscal[CI_ITER] + 1;
+  c.iscal[CI_ITER] = it;
+  c.iscal[CI_TOTAL] += 1;
+  c.scal[CN_RR] = tot[0];
+  const double rz_old = c.scal[CN_RZ];
+  c.scal[CN_BETA] = rz_old > 0.0 ? tot[1] / rz_old : 0.0;
+  c.scal[CN_RZ] = tot[1];
+  if (tot[0] <= c.tol2 * c.scal[CN_BB]) {
+    c.iscal[CI_DONE] = 1;
+  } else if (it >= c.max_iter || !isfinite(tot[0])) {
+    c.iscal[CI_UNCONV] += 1;
+    c.iscal[CI_DONE] = 1;
+  }
+}
+
+// p = Dinv r + beta p.
+__global__ void __launch_bounds__(CN_TB) cn_dir_kernel(CnArgs c) {
+  if (c.iscal[CI_DONE]) return;
+  const float beta = (float)c.scal[CN_BETA];
+  for (int64_t e = blockIdx.x * (int64_t)CN_TB + threadIdx.x; e < c.n;
+       e += (int64_t)gridDim.x * CN_TB)
+    c.p[e] = c.dinv[e] * c.r[e] + beta * c.p[e];
+}
+
+// End of the CN diffusion half: V_{i+1} = clamp(x), then the outputs of step
+// i exactly as the explicit step records them (threads as the ionic launch:
+// compact tissue list, then Purkinje nodes from n_active_pad).
+__global__ void __launch_bounds__(ION_THREADS) cn_finish_kernel(MonoArgs a, CnArgs c) {
+  __shared__ int64_t s_vm_frame, s_anim_frame;
+  const int64_t step = *a.d_step;
+  if (threadIdx.x == 0) {
+    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+  }
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n_active) {
+    const int64_t slot = a.active_slot[i];
+    const float Vn = fminf(fmaxf(c.x[slot], -150.0f), 80.0f);
+    voxel_outputs(a, slot, a.tag[slot], Vn, a.Vpost[slot], step, s_vm_frame, s_anim_frame);
+  } else {
+    const int p = i - a.n_active_pad;
+    if (p >= 0 && p < a.n_pk) {
+      const float Vn = fminf(fmaxf(c.x[a.n_slots + p], -150.0f), 80.0f);
+      a.pk_Vpost[p] = Vn;
+      if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p] = Vn;
+    }
+  }
+}
+
 // Host: halo copy table of the pipelined and split-diffusion kernels for
 // one brick shape: the union of the tile elements the stencil reads, minus
 // the brick's own voxels (the 7-point operator reads face neighbours only,
@@ -860,6 +1169,7 @@ __global__ void fill_kernel(float* p, int64_t n, float v) {
 __global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
 
 typedef void (*StepFn)(MonoArgs, int, int);
+typedef void (*CnFn)(MonoArgs, CnArgs, int);
 typedef void (*PipeFn)(MonoArgs, int);  // also the diffusion half of the split step
 typedef std::vector<uint32_t> (*HaloFn)(bool);
 
@@ -872,6 +1182,7 @@ struct ShapeEntry {
   int stage_floats_iso, stage_floats_aniso;
   int diff_cap_iso, diff_cap_aniso;  // halo entries the diffusion kernel holds
   int diff_floats_iso, diff_floats_aniso;
+  CnFn cn_iso, cn_aniso;
 };
 
 #define HP_SHAPE(I, J, K)                                                                    \
@@ -880,7 +1191,8 @@ struct ShapeEntry {
    mono_diffuse_kernel<I, J, K, false>, mono_diffuse_kernel<I, J, K, true>, pipe_halo_table<I, J, K>, \
    PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS,                      \
    DiffHalo<I, J, K, false>::PER_THREAD * I * J * K, DiffHalo<I, J, K, true>::PER_THREAD * I * J * K, \
-   DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS}
+   DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS,                      \
+   cn_stencil_kernel<I, J, K, false>, cn_stencil_kernel<I, J, K, true>}
 static const ShapeEntry kShapes[] = {HP_SHAPE(4, 4, 8), HP_SHAPE(4, 8, 8), HP_SHAPE(2, 4, 16),
                                      HP_SHAPE(8, 8, 8)};
 #undef HP_SHAPE
@@ -899,6 +1211,12 @@ struct HpMono {
   int diff_grid;     // its persistent grid
   int ion_grid;      // grid of the ionic half
   size_t diff_smem;  // and dynamic shared memory per CTA
+  CnFn cn;           // theta > 0: stencil pass of the CN solve, or null
+  CnArgs cn_a;
+  int cn_grid;       // persistent grid of the stencil pass
+  int cn_vgrid;      // grid of the vector kernels
+  int cn_chunk;      // iterations enqueued before the next flag test
+  int32_t* cn_host;  // pinned copy of the done flag and iteration count
   int bv;
   int64_t n_steps, steps_done;
   int64_t n_vm_frames, n_anim_frames;
@@ -1045,6 +1363,82 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   return HP_OK;
 }
 
+// Theta-scheme diffusion half: CG vectors, the persistent grid of the
+// stencil pass and the Jacobi diagonal (one stencil pass in mode 2).
+static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, cudaStream_t s) {
+  CnArgs& c = h->cn_a;
+  memset(&c, 0, sizeof(c));
+  const int64_t n = h->a.n_slots + h->a.n_pk;
+  c.n = n;
+  c.theta = (float)d->theta;
+  c.omt = (float)(1.0 - d->theta);
+  c.pk_weight = d->pk_weight;
+  // the vectors are FP32: a tighter relative tolerance than ~1e-7 is not
+  // reachable by the recursive residual
+  const double tol = std::max(d->cn_tol, 1e-7);
+  c.tol2 = tol * tol;
+  c.max_iter = d->cn_max_iter;
+  h->cn = d->anisotropic ? se->cn_aniso : se->cn_iso;
+  int dev = 0, n_sm = 0, per_sm = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->cn, h->bv, 0));
+  const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
+  h->cn_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
+  h->cn_vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + CN_TB - 1) / CN_TB, 8 * n_sm));
+  h->cn_chunk = 4;
+  HP_TRY_NODESTROY(al(h, &c.x, n));
+  HP_TRY_NODESTROY(al(h, &c.r, n));
+  HP_TRY_NODESTROY(al(h, &c.p, n));
+  HP_TRY_NODESTROY(al(h, &c.q, n));
+  HP_TRY_NODESTROY(al(h, &c.dinv, n));
+  HP_TRY_NODESTROY(al(h, &c.part, (size_t)std::max(h->cn_grid, h->cn_vgrid) * CN_NPART));
+  HP_TRY_NODESTROY(al(h, &c.scal, N_CN_SCAL));
+  HP_TRY_NODESTROY(al(h, &c.iscal, N_CN_ISCAL));
+  HP_TRY_NODESTROY(al(h, &c.ticket, 1));
+  HP_CUDA_TRY(cudaMemsetAsync(c.scal, 0, N_CN_SCAL * sizeof(double), s));
+  HP_CUDA_TRY(cudaMemsetAsync(c.iscal, 0, N_CN_ISCAL * sizeof(int32_t), s));
+  HP_CUDA_TRY(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned int), s));
+  HP_CUDA_TRY(cudaMemsetAsync(c.p, 0, n * sizeof(float), s));
+  HP_CUDA_TRY(cudaMallocHost((void**)&h->cn_host, 2 * sizeof(int32_t)));
+  h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 2);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// One theta-scheme step: the stencil pass that starts the solve, CG
+// iterations in chunks (sized by the previous step's count) until the done
+// flag, the outputs of V_{i+1} = clamp(x), the ionic half and the step count.
+static hp_status cn_step(HpMono* h, cudaStream_t s) {
+  const CnArgs& c = h->cn_a;
+  h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 0);
+  HP_CUDA_TRY(cudaGetLastError());
+  int launched = 0;
+  while (launched < c.max_iter) {
+    const int k = std::min(h->cn_chunk, c.max_iter - launched);
+    for (int j = 0; j < k; ++j) {
+      h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 1);
+      cn_update_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c, h->a.n_slots);
+      cn_dir_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c);
+    }
+    HP_CUDA_TRY(cudaGetLastError());
+    launched += k;
+    HP_CUDA_TRY(cudaMemcpyAsync(h->cn_host, c.iscal + CI_DONE, 2 * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h->cn_host[0]) break;
+  }
+  // next step: enqueue this step's count (+1) before the first test
+  h->cn_chunk = std::max(1, std::min(h->cn_host[1] + 1, 64));
+  if (h->ion_grid > 0) {
+    cn_finish_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, c);
+    mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0, 0);
+  }
+  advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, 1);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* stream) {
   HP_REQUIRE(d && out, "hp_mono_create: null argument");
   *out = nullptr;
@@ -1070,6 +1464,12 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   HP_REQUIRE(d->site_on && (d->n_sites == 0 || d->site_amp), "hp_mono_create: missing site tables");
   HP_REQUIRE(d->n_myo >= 0 && (d->n_myo == 0 || d->slot_of_node), "hp_mono_create: missing slot_of_node");
   HP_REQUIRE(d->kernel >= 0 && d->kernel <= 3, "hp_mono_create: kernel must be 0..3");
+  HP_REQUIRE(d->theta >= 0.0 && d->theta <= 1.0, "hp_mono_create: theta must be in [0, 1]");
+  HP_REQUIRE(d->theta == 0.0 ||
+                 (d->cn_tol > 0.0 && d->cn_max_iter >= 1 && (d->n_pk == 0 || d->pk_weight > 0.0f)),
+             "hp_mono_create: theta > 0 needs cn_tol > 0, cn_max_iter >= 1 and pk_weight > 0");
+  HP_REQUIRE(d->theta == 0.0 || d->kernel == HP_MONO_KERNEL_AUTO || d->kernel == HP_MONO_KERNEL_SPLIT,
+             "hp_mono_create: theta > 0 runs on the split step (kernel AUTO or SPLIT)");
 
   HpMono* h = new HpMono();
   h->graph = nullptr;
@@ -1088,6 +1488,8 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   h->diff_grid = 0;
   h->diff_smem = 0;
   h->ion_grid = 0;
+  h->cn = nullptr;
+  h->cn_host = nullptr;
   h->anisotropic = d->anisotropic;
   h->n_steps = d->n_steps;
   h->steps_done = 0;
@@ -1227,9 +1629,10 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
     HP_CUDA_TRY(cudaMemsetAsync(a.pk_Vs1, 0, d->n_pk * sizeof(float), s));
   }
   HP_CUDA_TRY(cudaGetLastError());
-  if (d->kernel == HP_MONO_KERNEL_SPLIT ||
+  if (d->kernel == HP_MONO_KERNEL_SPLIT || d->theta > 0.0 ||
       (d->kernel == HP_MONO_KERNEL_AUTO && d->n_bricks > 0)) {
     HP_TRY(setup_split(h, se, d, s));
+    if (d->theta > 0.0) HP_TRY(setup_cn(h, se, d, s));
   } else if (d->kernel != HP_MONO_KERNEL_BRICK && d->n_bricks > 0) {
     HP_TRY(setup_pipe(h, se, d->anisotropic, d->kernel == HP_MONO_KERNEL_PIPELINED, s));
   }
@@ -1246,6 +1649,14 @@ extern "C" hp_status hp_mono_run(HpMono* h, int64_t n, int32_t graph_chunk, void
              "hp_mono_run: %lld steps requested, %lld remain", (long long)n,
              (long long)(h->n_steps - h->steps_done));
   cudaStream_t s = (cudaStream_t)stream;
+  if (h->cn) {  // theta-scheme: the host tests convergence between chunks
+    for (int64_t o = 0; o < n; ++o) {
+      hp_status st = cn_step(h, s);
+      if (st != HP_OK) return st;
+      h->steps_done += 1;
+    }
+    return HP_OK;
+  }
   int64_t left = n;
   // the legacy default stream cannot be captured: launch directly there
   if (graph_chunk > 0 && left >= graph_chunk && s != nullptr) {
@@ -1404,9 +1815,22 @@ extern "C" hp_status hp_mono_copy_state(HpMono* h, float* st_slots, float* st_pk
   return HP_OK;
 }
 
+extern "C" hp_status hp_mono_cn_stats(HpMono* h, int64_t* iterations, int64_t* solves,
+                                      int64_t* unconverged, int64_t* breakdowns) {
+  HP_REQUIRE(h, "hp_mono_cn_stats: null handle");
+  int32_t v[N_CN_ISCAL] = {0};
+  if (h->cn) HP_CUDA_TRY(cudaMemcpy(v, h->cn_a.iscal, sizeof(v), cudaMemcpyDeviceToHost));
+  if (iterations) *iterations = v[CI_TOTAL];
+  if (solves) *solves = v[CI_SOLVES];
+  if (unconverged) *unconverged = v[CI_UNCONV];
+  if (breakdowns) *breakdowns = v[CI_BREAK];
+  return HP_OK;
+}
+
 extern "C" hp_status hp_mono_destroy(HpMono* h) {
   if (!h) return HP_OK;
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->cn_host) cudaFreeHost(h->cn_host);
   for (void* p : h->allocs) cudaFree(p);
   delete h;
   return HP_OK;

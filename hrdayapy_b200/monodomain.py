@@ -5,9 +5,11 @@ Set-up follows simulation/functions/purkinje_myocardium_pipeline.py:1030-1345
 and anisotropic_simulation/functions/purkinje_myocardium_anisotropic_solver.py
 :1308-1745 (tree discretisation, root stimulus zone, membrane loading, PMJ
 mapping, phenotype assignment, stimulus sites); the time loop (:1347-1420 /
-:1746-1820) is hp_mono_run.  Only theta = 0 (the explicit method the fused
-kernel implements) is accepted; see DESIGN notes in the repository for the
-scheme gap to the reference's default theta = 0.5.
+:1746-1820) is hp_mono_run.  theta = 0 is the explicit update of the
+fused step kernels; 0 < theta <= 1 (the reference's default is 0.5) solves
+the theta-scheme diffusion half on the GPU each step by preconditioned CG
+(stopping rule and iteration cap as the reference's BiCGSTAB: cg_tol,
+cg_max_iter).
 """
 from __future__ import annotations
 
@@ -126,7 +128,11 @@ class MonoProblem:
     pk_variant: np.ndarray | None = None
     variant_gks: np.ndarray | None = None
     variant_gkr: np.ndarray | None = None
-    kernel: int = 0          # HP_MONO_KERNEL_AUTO / _BRICK (1) / _PIPELINED (2)
+    kernel: int = 0          # HP_MONO_KERNEL_AUTO / _BRICK (1) / _PIPELINED (2) / _SPLIT (3)
+    theta: float = 0.0       # 0 explicit diffusion half, (0, 1] theta-scheme (CG)
+    cn_tol: float = 1e-5     # relative residual of the theta-scheme solve
+    cn_max_iter: int = 100
+    pk_weight: float = 1.0   # Ai_P / Ai_M
 
     @property
     def n_pk(self):
@@ -203,6 +209,10 @@ class MonoHandle:
         d.deact_threshold = float(prob.deact_threshold)
         d.max_events = int(prob.max_events)
         d.kernel = int(prob.kernel)
+        d.theta = float(prob.theta)
+        d.cn_tol = float(prob.cn_tol)
+        d.cn_max_iter = int(prob.cn_max_iter)
+        d.pk_weight = float(prob.pk_weight)
         self._desc = d
         if stream is None:
             # a dedicated stream: CUDA graphs cannot capture the legacy stream
@@ -222,6 +232,14 @@ class MonoHandle:
     def run(self, n: int, graph_chunk: int = 50):
         _lib.check(_lib.lib().hp_mono_run(self.h, int(n), int(graph_chunk), self.stream),
                    "hp_mono_run")
+
+    def cn_stats(self):
+        """Theta-scheme counters: (CG iterations, solves, solves stopped by
+        the iteration cap, breakdowns); zeros at theta = 0."""
+        v = [C.c_int64() for _ in range(4)]
+        _lib.check(_lib.lib().hp_mono_cn_stats(self.h, *[C.byref(x) for x in v]),
+                   "hp_mono_cn_stats")
+        return tuple(int(x.value) for x in v)
 
     def kernel_info(self):
         """(kernel id, grid CTAs, dynamic shared memory bytes) of the step."""
@@ -309,8 +327,11 @@ def prepare(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None,
             ectopic_region=None, stim_regions=None, stim_len_mm=2.0, c_pmj=0.05,
             n_pmj=1, phi_endo_max=0.35, phi_epi_min=0.65, vm_save_dt=None,
             save_every=None, act_threshold=-40.0, deact_threshold=-40.0,
-            max_events=4, brick=None, verbose=False):
+            max_events=4, brick=None, theta=0.0, cg_tol=1e-5, cg_max_iter=100,
+            verbose=False):
     """Builds the MonoProblem and the bookkeeping the result dict needs."""
+    if not 0.0 <= float(theta) <= 1.0:
+        raise ValueError(f"theta={theta} must lie in [0, 1]")
     h = float(voxel_size)
     S = np.asarray(S)
     Z = np.asarray(Z) if Z is not None else S
@@ -472,7 +493,8 @@ def prepare(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None,
         dt=dt, Cm=Cm, n_steps=n_steps, site_amp=np.array([s["amp"] for s in sites], np.float32),
         site_on=site_on, vm_every=vm_every, frame_every=frame_every, surf_nodes=surf,
         surf_of_slot=lay.to_slots(surf_of_node, -1, np.int32), act_threshold=act_threshold,
-        deact_threshold=deact_threshold, max_events=max_events)
+        deact_threshold=deact_threshold, max_events=max_events, theta=float(theta),
+        cn_tol=float(cg_tol), cn_max_iter=int(cg_max_iter), pk_weight=float(Ai_P / Ai_M))
     info = dict(comp_nodes=comp, comp_edges_full=cedges,
                 comp_edges=clip_purkinje_outside_Z(comp, cedges, Z, h), branch_map=bmaps,
                 vox_idx=vox, nodes_mm=myo_xyz, Np=Np, pmj_ids=pmj_ids,
@@ -524,11 +546,9 @@ def run(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None, anisotr
         theta=0.0, dtype=None, device=None, n_frames=100, frame_save_dt=None,
         out_npz=None, out_vm_npz=None, vm_save_dt=None, vm_tmp_dir=None, anim_tmp_dir=None,
         cg_tol=None, cg_max_iter=None, graph_chunk=50, verbose=False, **kw):
-    """Full run with the reference's return dict, plus activation events."""
-    if theta != 0.0:
-        raise ValueError(
-            f"theta={theta}: the fused GPU time step is the explicit (theta = 0) method; "
-            "pass theta=0.0")
+    """Full run with the reference's return dict, plus activation events.
+    theta = 0 runs the fused explicit step; 0 < theta <= 1 the theta-scheme
+    with its CG solve (cg_tol, cg_max_iter as the reference's defaults)."""
     if device is not None and not str(device).startswith("cuda"):
         raise ValueError(f"device={device!r}: this implementation runs on CUDA only")
     T = kw.get("T", 400.0)
@@ -539,9 +559,12 @@ def run(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None, anisotr
     else:
         save_every = max(1, n_steps // max(1, int(n_frames)))
     run_vm = vm_save_dt is not None and out_vm_npz is not None
+    cn = {} if float(theta) == 0.0 else dict(
+        theta=float(theta), cg_tol=1e-5 if cg_tol is None else float(cg_tol),
+        cg_max_iter=100 if cg_max_iter is None else int(cg_max_iter))
     prob, info = prepare(nodes, elements, activation_times, S, Z, phi, fibre_dir=fibre_dir,
                          anisotropic=anisotropic, vm_save_dt=vm_save_dt if run_vm else None,
-                         save_every=save_every, **kw)
+                         save_every=save_every, **cn, **kw)
     sim = MonoHandle(prob)
     try:
         sim.run(n_steps, graph_chunk)

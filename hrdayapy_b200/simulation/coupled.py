@@ -2,8 +2,9 @@
 hrdayapy/simulation/coupled.py:33-131 and
 simulation/functions/purkinje_myocardium_pipeline.py:1030-1069.
 
-The time loop runs on the GPU (libhrdaya_b200, fused explicit step); only
-theta = 0 is accepted.  Extra keyword arguments act_threshold /
+The time loop runs on the GPU (libhrdaya_b200): theta = 0 the fused explicit
+step, 0 < theta <= 1 (default 0.5, as the reference) the theta-scheme with a
+CG solve per step (cg_tol, cg_max_iter).  Extra keyword arguments act_threshold /
 deact_threshold / max_events control the in-loop activation recording whose
 tables are added to the returned dict ("activation_times", ...).
 """

@@ -138,6 +138,20 @@ typedef struct {
   /* step kernel (all give bit-identical results): HP_MONO_KERNEL_AUTO is
    * the split step, the fastest on B200 for every compiled brick shape */
   int32_t kernel;
+
+  /* diffusion half: theta = 0 is the explicit update above; 0 < theta <= 1
+   * solves (I - theta Lh) V_{i+1} = W_i + (1 - theta) Lh W_i each step by
+   * Jacobi-preconditioned CG from V_{i+1} = W_i (reference: BiCGSTAB on the
+   * same system, pipeline.py:662-754 and :1383-1391), stopping when
+   * ||r|| <= cn_tol ||rhs|| (cn_tol below 1e-7 is raised to 1e-7, FP32
+   * vectors) or after cn_max_iter iterations.  pk_weight = Ai_P / Ai_M, the
+   * Purkinje over the tissue membrane loading (the inner product that makes
+   * the operator symmetric).  Needs the split step (kernel AUTO or SPLIT);
+   * CUDA-graph chunks are not used (the host tests convergence). */
+  double theta;
+  double cn_tol;
+  int32_t cn_max_iter;
+  float pk_weight;
 } HpMonoDesc;
 
 #define HP_MONO_KERNEL_AUTO 0
@@ -156,6 +170,11 @@ hp_status hp_mono_create(const HpMonoDesc *desc, HpMono **out, void *stream);
 hp_status hp_mono_run(HpMono *h, int64_t n, int32_t graph_chunk, void *stream);
 /* Steps done so far. */
 int64_t hp_mono_steps_done(const HpMono *h);
+/* Theta-scheme solver counters since creation: CG iterations, solves (one
+ * per step), solves stopped by cn_max_iter, and breakdowns (<p, Ap> <= 0).
+ * All zero at theta = 0.  Any output may be NULL; synchronises the device. */
+hp_status hp_mono_cn_stats(HpMono *h, int64_t *iterations, int64_t *solves,
+                           int64_t *unconverged, int64_t *breakdowns);
 /* Step kernel in use (HP_MONO_KERNEL_BRICK, _PIPELINED or _SPLIT), its grid size
  * and dynamic shared memory per CTA; any output may be NULL. */
 hp_status hp_mono_kernel_info(const HpMono *h, int32_t *kernel, int32_t *grid, int64_t *smem_bytes);

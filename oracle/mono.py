@@ -1,6 +1,6 @@
 """ORACLE -- test infrastructure, not product code.
 
-FP64 CPU restatement of HrdayaPy's monodomain path (theta = 0), used only by
+FP64 CPU restatement of HrdayaPy's monodomain path, used only by
 tests/, by ``__graft_entry__.smoke()`` as the checker and by ``bench.py``'s
 CPU-baseline leg.  The product package never imports this module.
 
@@ -18,8 +18,10 @@ upstream project root):
   purkinje_myocardium_anisotropic_solver.py:1204-1300
 * :func:`phenotypes`        -- ionic_models/hetero_solver.py:74-128
 * :func:`run`               -- run_coupled (pipeline.py:1030-1420) and the
-  anisotropic solver (..._anisotropic_solver.py:1308-1820) at theta = 0; the
-  time loop itself runs in C (ttp06_oracle.c, orc_mono_run)
+  anisotropic solver (..._anisotropic_solver.py:1308-1820); the time loop
+  itself runs in C (ttp06_oracle.c): orc_mono_run at theta = 0,
+  orc_mono_run_cn (the reference's BiCGSTAB, pipeline.py:662-754) at
+  theta > 0
 * :func:`activation_maps`   -- simulation/functions/activation_maps.py:63-116,295-350
 
 Parity is pinned by tests/test_oracle_golden.py against fixtures produced by
@@ -57,6 +59,9 @@ def lib():
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int64,
                                    ctypes.c_int, P, P, P, P, P, P, ctypes.c_int64, P, P]
         L.orc_mono_run.restype = ctypes.c_int
+        L.orc_mono_run_cn.argtypes = L.orc_mono_run.argtypes + [
+            ctypes.c_double, ctypes.c_double, ctypes.c_int64, P]
+        L.orc_mono_run_cn.restype = ctypes.c_int
         L.orc_num_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -285,9 +290,11 @@ def setup(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
           Cm=0.01, A_P=133.33, A_M=140.0, R_P=0.015, dt=0.02, T=10.0,
           stim_protocol=None, ectopic_region=None, stim_regions=None,
           stim_len_mm=2.0, c_pmj=0.05, n_pmj=1, phi_endo_max=0.35, phi_epi_min=0.65,
-          vm_save_dt=None, gks_scale=1.0, gkr_scale=1.0, anisotropic=False):
-    """Set-up of the reference method (theta = 0): assembled L, phenotypes,
-    stimulus schedule, resting state.  ``anisotropic=True`` follows the
+          vm_save_dt=None, gks_scale=1.0, gkr_scale=1.0, anisotropic=False,
+          theta=0.0, cg_tol=1e-5, cg_max_iter=100):
+    """Set-up of the reference method (theta = 0 the explicit update, theta >
+    0 the theta-scheme): assembled L, phenotypes, stimulus schedule, resting
+    state.  ``anisotropic=True`` follows the
     anisotropic solver (A_P = 2/R_P, fibre tensor, 18-connected mesh);
     otherwise run_coupled (A_P argument, uniform sigma_M)."""
     h = float(voxel_size)
@@ -340,7 +347,9 @@ def setup(nodes, elements, act_times, S, phi, *, fibre_dir=None, voxel_size=0.4,
                 dt=float(dt), Cm=float(Cm), n_steps=n_steps, snap_every=snap_every,
                 V=np.full(N, V0), state=np.tile(TTP06_INIT, (N, 1)),
                 gks=np.full(N, float(gks_scale)), gkr=np.full(N, float(gkr_scale)),
-                step=0, vox_idx=vox, comp_nodes=comp, comp_edges=cedges, branch_map=bmaps,
+                step=0, theta=float(theta), cg_tol=float(cg_tol), cg_max_iter=int(cg_max_iter),
+                cg_iters=0, Ai_P=Ai_P, Ai_M=Ai_M,
+                vox_idx=vox, comp_nodes=comp, comp_edges=cedges, branch_map=bmaps,
                 pmj_ids=pmj_ids, pmj_patches=patches)
 
 
@@ -369,11 +378,18 @@ def advance(ctx, n_steps, snapshots=True):
     psnaps = np.zeros((max(n_snap, 1), Np), np.float32)
     if snapshots and k0 % se != 0 and n_snap:
         raise ValueError("advance() must start on a snapshot boundary when snapshots are on")
-    rc = lib().orc_mono_run(N, Np, _p(ctx["ptr"]), _p(ctx["idx"]), _p(ctx["val"]),
-                            _p(ctx["pheno"]), _p(ctx["gks"]), _p(ctx["gkr"]), dt, ctx["Cm"],
-                            n_steps, nS, _p(site_ptr), _p(site_nodes), _p(site_amp), _p(on),
-                            _p(ctx["V"]), _p(ctx["state"]), se if snapshots else 0,
-                            _p(snaps), _p(psnaps))
+    args = (N, Np, _p(ctx["ptr"]), _p(ctx["idx"]), _p(ctx["val"]),
+            _p(ctx["pheno"]), _p(ctx["gks"]), _p(ctx["gkr"]), dt, ctx["Cm"],
+            n_steps, nS, _p(site_ptr), _p(site_nodes), _p(site_amp), _p(on),
+            _p(ctx["V"]), _p(ctx["state"]), se if snapshots else 0,
+            _p(snaps), _p(psnaps))
+    if ctx.get("theta", 0.0) == 0.0:
+        rc = lib().orc_mono_run(*args)
+    else:
+        it = np.zeros(1, np.int64)
+        rc = lib().orc_mono_run_cn(*args, ctx["theta"], ctx["cg_tol"], ctx["cg_max_iter"],
+                                   _p(it))
+        ctx["cg_iters"] += int(it[0])
     if rc != 0:
         raise RuntimeError(f"orc_mono_run failed ({rc})")
     ctx["step"] = k0 + n_steps
@@ -382,7 +398,7 @@ def advance(ctx, n_steps, snapshots=True):
 
 
 def run(nodes, elements, act_times, S, phi, **kw):
-    """Full theta = 0 FP64 run of the reference method from rest.  Returns
+    """Full FP64 run of the reference method from rest.  Returns
     ``Vm`` (n_snap, N_myo) float32, ``time_vm``, ``Vp`` Purkinje snapshots,
     final ``V``/``state`` and the set-up bookkeeping."""
     ctx = setup(nodes, elements, act_times, S, phi, **kw)

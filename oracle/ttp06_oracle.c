@@ -404,3 +404,142 @@ int orc_mono_run(int64_t N, int64_t n_skip,
     free(c.Istim); free(c.Vs); free(c.mark);
     return 0;
 }
+
+/*
+ * Theta-scheme (Crank-Nicolson at theta = 0.5) monodomain time loop: the
+ * reference's default diffusion half (pipeline.py:1383-1391, anisotropic
+ * solver :1784-1790).  Per step: ionic step on V^n, V* as orc_mono_run, then
+ * A V^{n+1} = b with A = (Cm/dt) I - theta L, b = (Cm/dt) V* + (1 - theta)
+ * L V*, solved by the reference's Jacobi-preconditioned BiCGSTAB from x0 = V*
+ * (_build_cn_matrix pipeline.py:662-688, _bicgstab :691-754, restated
+ * below step by step), clamped to [-150, 80].  Serial.  iters (may be NULL)
+ * receives the BiCGSTAB iteration count summed over the steps.
+ */
+static void cn_apply(int64_t N, const int64_t *Lp, const int32_t *Li, const double *Lv,
+                     double scale, double theta, const double *x, double *y) {
+    for (int64_t i = 0; i < N; ++i) {
+        double acc = 0.0;
+        for (int64_t q = Lp[i]; q < Lp[i + 1]; ++q) acc += Lv[q] * x[Li[q]];
+        y[i] = scale * x[i] - theta * acc;
+    }
+}
+static double dotv(int64_t N, const double *a, const double *b) {
+    double s = 0.0;
+    for (int64_t i = 0; i < N; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* _bicgstab (pipeline.py:691-754); x holds x0 on entry.  Returns iterations. */
+static int64_t cn_bicgstab(int64_t N, const int64_t *Lp, const int32_t *Li, const double *Lv,
+                           double scale, double theta, const double *Minv, const double *b,
+                           double *x, double tol, int64_t maxiter, double *w) {
+    double *r = w, *rh = w + N, *v = w + 2 * N, *p = w + 3 * N, *ph = w + 4 * N,
+           *s = w + 5 * N, *sh = w + 6 * N, *t = w + 7 * N;
+    cn_apply(N, Lp, Li, Lv, scale, theta, x, t);
+    for (int64_t i = 0; i < N; ++i) { r[i] = b[i] - t[i]; rh[i] = r[i]; v[i] = 0.0; p[i] = 0.0; }
+    double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+    const double b_norm = sqrt(dotv(N, b, b));
+    if (b_norm == 0.0) return 0;
+    int64_t it = 0;
+    for (; it < maxiter; ++it) {
+        double rho = dotv(N, rh, r);
+        if (fabs(rho) < 1e-300) {
+            for (int64_t i = 0; i < N; ++i) rh[i] = r[i];
+            rho = dotv(N, rh, r);
+        }
+        if (it == 0) {
+            for (int64_t i = 0; i < N; ++i) p[i] = r[i];
+        } else {
+            const double beta = (rho / rho_prev) * (alpha / omega);
+            for (int64_t i = 0; i < N; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        }
+        for (int64_t i = 0; i < N; ++i) ph[i] = Minv[i] * p[i];
+        cn_apply(N, Lp, Li, Lv, scale, theta, ph, v);
+        const double da = dotv(N, rh, v);
+        if (fabs(da) < 1e-300) break;
+        alpha = rho / da;
+        for (int64_t i = 0; i < N; ++i) s[i] = r[i] - alpha * v[i];
+        if (sqrt(dotv(N, s, s)) < tol * b_norm) {
+            for (int64_t i = 0; i < N; ++i) x[i] += alpha * ph[i];
+            ++it;
+            break;
+        }
+        for (int64_t i = 0; i < N; ++i) sh[i] = Minv[i] * s[i];
+        cn_apply(N, Lp, Li, Lv, scale, theta, sh, t);
+        const double dw = dotv(N, t, t);
+        omega = fabs(dw) > 1e-300 ? dotv(N, t, s) / dw : 0.0;
+        for (int64_t i = 0; i < N; ++i) {
+            x[i] += alpha * ph[i] + omega * sh[i];
+            r[i] = s[i] - omega * t[i];
+        }
+        rho_prev = rho;
+        if (sqrt(dotv(N, r, r)) / b_norm < tol) { ++it; break; }
+        if (fabs(omega) < 1e-300) { ++it; break; }
+    }
+    return it;
+}
+
+int orc_mono_run_cn(int64_t N, int64_t n_skip,
+                    const int64_t *L_ptr, const int32_t *L_idx, const double *L_val,
+                    const int8_t *pheno, const double *gks_s, const double *gkr_s,
+                    double dt, double Cm, int64_t n_steps,
+                    int n_sites, const int64_t *site_ptr, const int32_t *site_nodes,
+                    const double *site_amp, const uint8_t *site_on,
+                    double *V, double *state,
+                    int64_t snap_every, float *snaps, float *psnaps,
+                    double theta, double tol, int64_t maxiter, int64_t *iters) {
+    const double scale = Cm / dt;
+    double *Istim = (double *)calloc(N, sizeof(double));
+    double *Vs = (double *)malloc(sizeof(double) * N);
+    double *b = (double *)malloc(sizeof(double) * N);
+    double *Minv = (double *)malloc(sizeof(double) * N);
+    double *w = (double *)malloc(sizeof(double) * 8 * N);
+    unsigned char *mark = (unsigned char *)calloc(N, 1);
+    if (!Istim || !Vs || !b || !Minv || !w || !mark) {
+        free(Istim); free(Vs); free(b); free(Minv); free(w); free(mark);
+        return -2;
+    }
+    /* M_inv = 1 / (scale - theta diag L), pipeline.py:686-687 */
+    for (int64_t i = 0; i < N; ++i) {
+        double dl = 0.0;
+        for (int64_t q = L_ptr[i]; q < L_ptr[i + 1]; ++q)
+            if (L_idx[q] == i) dl += L_val[q];
+        double da = scale - theta * dl;
+        Minv[i] = 1.0 / (da > 1e-30 ? da : 1e-30);
+    }
+    int64_t snap_i = 0, it_sum = 0;
+    for (int64_t step = 0; step < n_steps; ++step) {
+        memset(Istim, 0, sizeof(double) * N);
+        for (int s = 0; s < n_sites; ++s) {
+            if (!site_on[step * n_sites + s]) continue;
+            for (int64_t q = site_ptr[s]; q < site_ptr[s + 1]; ++q) mark[site_nodes[q]] = 1;
+            for (int64_t q = site_ptr[s]; q < site_ptr[s + 1]; ++q) {
+                int32_t nd = site_nodes[q];
+                if (mark[nd]) { Istim[nd] += site_amp[s]; mark[nd] = 0; }
+            }
+        }
+        for (int64_t i = 0; i < N; ++i) {
+            double ii = orc_ttp06_cell(V[i], state + i * NSTATE, dt, pheno[i],
+                                       gks_s ? gks_s[i] : 1.0, gkr_s ? gkr_s[i] : 1.0);
+            Vs[i] = V[i] + (dt / Cm) * (-(ii * Cm) + Istim[i]);
+        }
+        for (int64_t i = 0; i < N; ++i) {
+            double acc = 0.0;
+            for (int64_t q = L_ptr[i]; q < L_ptr[i + 1]; ++q) acc += L_val[q] * Vs[L_idx[q]];
+            b[i] = scale * Vs[i] + (1.0 - theta) * acc;
+        }
+        memcpy(V, Vs, sizeof(double) * N);
+        it_sum += cn_bicgstab(N, L_ptr, L_idx, L_val, scale, theta, Minv, b, V, tol, maxiter, w);
+        for (int64_t i = 0; i < N; ++i) V[i] = V[i] < -150.0 ? -150.0 : (V[i] > 80.0 ? 80.0 : V[i]);
+        if (snap_every > 0 && step % snap_every == 0) {
+            if (snaps)
+                for (int64_t i = n_skip; i < N; ++i) snaps[snap_i * (N - n_skip) + i - n_skip] = (float)V[i];
+            if (psnaps)
+                for (int64_t i = 0; i < n_skip; ++i) psnaps[snap_i * n_skip + i] = (float)V[i];
+            ++snap_i;
+        }
+    }
+    if (iters) *iters = it_sum;
+    free(Istim); free(Vs); free(b); free(Minv); free(w); free(mark);
+    return 0;
+}

@@ -1,6 +1,7 @@
 """FP64 numpy emulation of the fused monodomain kernel's algorithm, run on
 the product's MonoProblem (brick slots, tag bits, coefficient arrays, the
-half-step skew and in-loop event recording).  Used by CPU tests to check the
+half-step skew and in-loop event recording, the theta-scheme's weighted
+CG solve).  Used by CPU tests to check the
 host-side preparation and the kernel's step logic against the oracle without
 a GPU.  The ionic half uses the oracle's TTP06 (FP64)."""
 from __future__ import annotations
@@ -94,11 +95,49 @@ def emulate(prob, n_steps=None):
             Is += np.where((on >> s) & 1, amp[s], 0.0)
         return V + (dt / Cm) * (-(I * Cm) + Is)
 
+    Lh = (Cmat - sp.diags(deg)).tocsr()
+    wgt = np.concatenate([np.full(Np, prob.pk_weight), np.ones(N)])
+    dinv = 1.0 / (1.0 + prob.theta * deg)
+
+    def cn_solve(W):
+        """The GPU theta-scheme solve: Jacobi-preconditioned CG in the
+        inner product weighted by wgt, from x = W (rhs - M W = Lh W)."""
+        th = prob.theta
+        tol2 = max(prob.cn_tol, 1e-7) ** 2
+        LW = Lh @ W
+        x, r = W.copy(), LW.copy()
+        p = dinv * r
+        bb = float(np.sum((W + (1.0 - th) * LW) ** 2))
+        rz = float(np.sum(wgt * r * p))
+        if float(r @ r) <= tol2 * bb or bb == 0.0:
+            return x, 0
+        for it in range(1, prob.cn_max_iter + 1):
+            q = p - th * (Lh @ p)
+            pq = float(np.sum(wgt * p * q))
+            if not pq > 0.0:
+                return x, it
+            alpha = rz / pq
+            x += alpha * p
+            r -= alpha * q
+            z = dinv * r
+            rz_new = float(np.sum(wgt * r * z))
+            if float(r @ r) <= tol2 * bb:
+                return x, it
+            p = z + (rz_new / rz) * p
+            rz = rz_new
+        return x, prob.cn_max_iter
+
     W = ionic(Vpost, 0)
     snaps, psnaps = [], []
     act = np.full(N, np.nan)
+    iters = []
     for step in range(n_steps):
-        Vn = np.clip(W + (Cmat @ W - deg * W), -150.0, 80.0)
+        if prob.theta == 0.0:
+            Vn = np.clip(W + (Cmat @ W - deg * W), -150.0, 80.0)
+        else:
+            x, it = cn_solve(W)
+            iters.append(it)
+            Vn = np.clip(x, -150.0, 80.0)
         if step >= 1:
             Vp = Vpost[Np:]
             thr = prob.act_threshold
@@ -111,4 +150,5 @@ def emulate(prob, n_steps=None):
             snaps.append(Vn[Np:].astype(np.float32))
             psnaps.append(Vn[:Np].astype(np.float32))
         W = ionic(Vn, step + 1)
+    emulate.cn_iters = iters
     return np.array(snaps), np.array(psnaps), act

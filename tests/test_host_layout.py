@@ -2,6 +2,7 @@
 junction CSR, stimulus schedule) checked on the CPU against the oracle's
 assembled global Laplacian and time loop."""
 import numpy as np
+import scipy.sparse as sp
 import pytest
 
 from hrdayapy_b200 import layout as L
@@ -109,6 +110,41 @@ def test_kernel_algorithm_emulation_matches_oracle():
         np.testing.assert_allclose(a_em, a[:, 0], atol=1e-4, equal_nan=True)
 
 
+@pytest.mark.parametrize("aniso", [False, True])
+def test_theta_scheme_emulation_matches_oracle(aniso):
+    """The GPU theta-scheme algorithm (weighted Jacobi-CG from the warm start
+    x = W, reference stopping rule) against the oracle's restatement of the
+    reference's BiCGSTAB at theta = 0.5.  The operator the kernels apply is
+    self-adjoint in the Ai-weighted inner product the CG uses."""
+    if aniso:
+        args, fibre, kw = cases.aniso_case()
+        extra = dict(fibre_dir=fibre, anisotropic=True)
+        kw = dict(kw, A_P=2.0 / kw["R_P"])
+    else:
+        args, kw = cases.iso_case()
+        extra = {}
+    nodes, el, act, S, phi = args
+    kw = dict(kw, T=6.0)
+    prob, info = M.prepare(nodes, el, act, S, S, phi, vm_save_dt=0.02, act_threshold=-20.0,
+                           theta=0.5, cg_tol=1e-7, cg_max_iter=100, **extra, **kw)
+    C = coefficient_matrix(prob)
+    Lh = C - sp.diags(np.asarray(C.sum(axis=1)).ravel())
+    w = np.concatenate([np.full(prob.n_pk, prob.pk_weight), np.ones(C.shape[0] - prob.n_pk)])
+    WL = sp.diags(w) @ Lh
+    assert abs(WL - WL.T).max() <= 1e-6 * abs(WL).max()
+    snaps, psnaps, a_em = emulate(prob)
+    assert max(emulate.cn_iters) < 100
+    kwo = {k: v for k, v in kw.items() if k != "A_P"} if aniso else kw
+    r = orc.run(nodes, el, act, S, phi, vm_save_dt=0.02, theta=0.5, cg_tol=1e-10,
+                cg_max_iter=200, **extra, **kwo)
+    np.testing.assert_allclose(snaps, r["Vm"], atol=2e-3)
+    if prob.n_pk and aniso:
+        np.testing.assert_allclose(psnaps, r["Vp"], atol=2e-3)
+    a = orc.activation_maps(r["Vm"], r["time_vm"], -20.0, -20.0)["activation_times"]
+    if a.shape[1]:
+        np.testing.assert_allclose(a_em, a[:, 0], atol=1e-4, equal_nan=True)
+
+
 def test_bad_arguments():
     args, kw = cases.iso_case()
     nodes, el, act, S, phi = args
@@ -124,6 +160,12 @@ def test_bad_arguments():
                                                np.zeros(S.shape + (3,)), A_P=1.0)
     from hrdayapy_b200 import monodomain
     with pytest.raises(ValueError):
-        monodomain.run(nodes, el, act, S, S, phi, theta=0.5, **kw)
+        monodomain.run(nodes, el, act, S, S, phi, theta=1.5, **kw)
+    prob, _ = M.prepare(nodes, el, act, S, S, phi, theta=0.5, cg_tol=1e-6, cg_max_iter=50, **kw)
+    assert (prob.theta, prob.cn_tol, prob.cn_max_iter) == (0.5, 1e-6, 50)
+    S_P = np.pi * kw.get("R_P", 0.015) ** 2
+    ai_p = kw.get("A_P", 133.33) * S_P * kw.get("dx_p", 0.2)
+    ai_m = kw.get("A_M", 0.14) * kw["voxel_size"] ** 3
+    assert prob.pk_weight == pytest.approx(ai_p / ai_m)
     with pytest.raises(ValueError):
         monodomain.run(nodes, el, act, S, S, phi, theta=0.0, device="cpu", **kw)

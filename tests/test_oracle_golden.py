@@ -62,6 +62,27 @@ def test_mono_aniso(golden):
     np.testing.assert_allclose(a["activation_times"], g["act"], atol=1e-5)
 
 
+@pytest.mark.parametrize("name", ["iso", "aniso"])
+def test_oracle_theta_scheme_vs_upstream(golden, name):
+    """The oracle's restatement of the reference's theta = 0.5 step
+    (BiCGSTAB on (Cm/dt) I - theta L) reproduces the upstream code's own
+    activation map."""
+    from oracle import mono as orc
+    g = golden(f"mono_{name}.npz")
+    if name == "iso":
+        args, kw = cases.iso_case()
+        extra = {}
+    else:
+        args, fibre, kw = cases.aniso_case()
+        extra = dict(fibre_dir=fibre, anisotropic=True)
+    nodes, el, act, S, phi = args
+    r = orc.run(nodes, el, act, S, phi, vm_save_dt=kw["dt"], theta=0.5, cg_tol=1e-12,
+                cg_max_iter=200, **extra, **kw)
+    a = orc.activation_maps(r["Vm"], r["time_vm"], -20.0, -20.0)["activation_times"]
+    assert a.shape == g["act_cn"].shape
+    np.testing.assert_allclose(a, g["act_cn"], atol=1e-5)
+
+
 def test_scheme_gap_is_reported(golden):
     """theta=0 (the method built here) vs the upstream default theta=0.5: the
     gap is a property of the scheme, recorded for the documentation."""
