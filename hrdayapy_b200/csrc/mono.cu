@@ -631,192 +631,6 @@ mono_pipe_kernel(MonoArgs a, int step_off) {
 }
 
 // ---------------------------------------------------------------------------
-// Split step: two launches per step over the same arrays.
-//
-// mono_diffuse_kernel (one CTA per brick, plus CTAs of BV Purkinje nodes)
-// forms V_{i+1} from W_i and its halo, records the crossings and snapshots of
-// step i and stores V_{i+1} in Vpost.  mono_ionic_kernel then runs the ionic
-// half of step i+1 with one thread per tissue slot, taken from the compact
-// list active_slot, so padding slots of partially filled bricks occupy no
-// lane, and without shared memory or barriers, so it runs at full occupancy.
-// Both do the fused kernels' arithmetic in the same order: results are
-// bit-identical to theirs.
-// Halo copy-table entries per thread of the diffusion kernel (held in
-// registers for the whole launch).  Rows of a face or ij-edge outside the
-// brick in i or j move as BK/4 16-byte chunks, k-face and k-edge elements
-// one by one.
-template <int BI, int BJ, int BK, bool ANISO>
-struct DiffHalo {
-  static constexpr int BV = BI * BJ * BK, Q = BK / 4;
-  static constexpr int W = ANISO ? 2 * (BI + BJ + 2) * Q + 2 * BI * BJ + 4 * (BI + BJ)
-                                 : 2 * (BI + BJ) * Q + 2 * BI * BJ;
-  // face weights (-i, -j, -k faces) and the three off-diagonal tiles
-  static constexpr int A = (BJ + BI) * Q + BI * BJ + (2 * BJ + 2 * BI + 4) * Q +
-                           (2 * BJ * Q + 2 * BI * BJ + 4 * BJ) + (2 * BI * Q + 2 * BI * BJ + 4 * BI);
-  static constexpr int N = ANISO ? W + A : W;
-  static constexpr int PER_THREAD = (N + BV - 1) / BV;
-};
-
-// Shared-memory stage of the diffusion kernel: the staged tiles, then the
-// brick's tags and V_i.
-template <int BI, int BJ, int BK, bool ANISO>
-struct DiffStage {
-  using G = PipeGeom<BI, BJ, BK>;
-  static constexpr int NF = ANISO ? 7 : 1;
-  static constexpr int TAG = NF * G::NT;
-  static constexpr int VP = TAG + G::BV;
-  static constexpr int FLOATS = VP + G::BV;
-  static constexpr int NCHUNK = (NF + 2) * G::BV / 4;  // 16-byte own-brick copies
-};
-
-template <int BI, int BJ, int BK, bool ANISO>
-__global__ void __launch_bounds__(BI * BJ * BK)
-mono_diffuse_kernel(MonoArgs a, int step_off) {
-  using G = PipeGeom<BI, BJ, BK>;
-  using H = DiffHalo<BI, BJ, BK, ANISO>;
-  using D = DiffStage<BI, BJ, BK, ANISO>;
-  constexpr int BV = G::BV, NF = D::NF, PT = H::PER_THREAD;
-  constexpr int QB = BV / 4;  // 16-byte chunks per brick row of one field
-  extern __shared__ __align__(16) float smem[];
-  float* stages = smem;                     // 2 x FLOATS
-  int* ring = (int*)(smem + 2 * D::FLOATS);  // 2 x 27 neighbour lists
-  __shared__ int64_t s_vm_frame, s_anim_frame;
-  const int64_t step = *a.d_step + step_off;
-  const bool odd = step & 1;
-  const float* __restrict__ Win = odd ? a.Vs1 : a.Vs0;
-  const int tid = threadIdx.x;
-  const int64_t ns = a.n_slots;
-  // this thread's halo copies for the whole launch: stage offset (field tile
-  // + position), neighbour direction, source (array + offset in the brick)
-  uint32_t hpos[PT], hdir[PT];
-  const float* hsrc[PT];
-#pragma unroll
-  for (int q = 0; q < PT; ++q) {
-    const int e = tid + q * BV;
-    const uint32_t t = e < a.n_halo ? a.halo_tab[e] : 0u;
-    const int f = (t >> 11) & 7;
-    hpos[q] = e < a.n_halo ? (uint32_t)(f * G::NT + (int)(t & ((1u << HALO_POS_BITS) - 1)))
-                           : 0xFFFFFFFFu;
-    hdir[q] = ((t >> 14) & 31) | ((t & HALO_CHUNK) ? 32u : 0u);
-    hsrc[q] = e >= a.n_halo ? Win
-                            : (f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)) +
-                                  ((t >> 19) & 0xFFFu);
-  }
-  auto issue = [&](float* st, const int* nb27, int b) {
-    const int64_t base = (int64_t)b * BV;
-#pragma unroll
-    for (int k = 0; k < (D::NCHUNK + BV - 1) / BV; ++k) {
-      const int q = tid + k * BV;
-      if (q < D::NCHUNK) {
-        const int f = q / QB, o = (q % QB) * 4;
-        const float* src = f == 0    ? Win
-                           : f < NF  ? (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)
-                           : f == NF ? (const float*)a.tag
-                                     : a.Vpost;
-        float* dst = f < NF ? st + f * G::NT + G::pos(o / (BJ * BK), (o / BK) % BJ, o % BK)
-                            : st + D::TAG + (f - NF) * BV + o;
-        cp_async16(dst, src + base + o);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < PT; ++q) {
-      if (hpos[q] != 0xFFFFFFFFu) {
-        const int nb = nb27[hdir[q] & 31];
-        const bool chunk = hdir[q] & 32;
-        if (nb >= 0) {
-          if (chunk)
-            cp_async16(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
-          else
-            cp_async4(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
-        } else if (chunk) {
-          *(float4*)(st + hpos[q]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        } else {
-          st[hpos[q]] = 0.0f;
-        }
-      }
-    }
-  };
-  const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
-  const int c = G::pos(li, lj, lk);
-  const int G_ = gridDim.x;
-  const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
-  if (tid == 0) {
-    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
-    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
-  }
-  int cur = blockIdx.x;
-  if (cur < a.n_bricks && tid < 27) ring[tid] = a.nbr[(int64_t)cur * 27 + tid];
-  __syncthreads();
-  if (cur < a.n_bricks) {
-    issue(stages, ring, cur);
-    const int nx = cur + G_;
-    if (nx < a.n_bricks && tid < 27) cp_async4(ring + 27 + tid, a.nbr + (int64_t)nx * 27 + tid);
-  }
-  cp_async_commit();
-  for (int n = 0; cur < n_items; ++n, cur += G_) {
-    cp_async_wait_all();
-    __syncthreads();
-    const int nxt = cur + G_;
-    if (nxt < a.n_bricks) {
-      issue(stages + ((n + 1) & 1) * D::FLOATS, ring + ((n + 1) & 1) * 27, nxt);
-      const int nn = nxt + G_;
-      if (nn < a.n_bricks && tid < 27) cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
-    }
-    cp_async_commit();
-    if (cur < a.n_bricks) {
-      const float* st = stages + (n & 1) * D::FLOATS;
-      const uint32_t tag = ((const uint32_t*)(st + D::TAG))[tid];
-      if (tag & HP_TAG_PHENO_MASK) {
-        const int64_t slot = (int64_t)cur * BV + tid;
-        const float Vn = diffuse<G::SI, G::SJ, G::NT, ANISO>(
-            a, st, ANISO ? st + G::NT : st, ANISO ? st + 4 * G::NT : st, c, tag, slot, odd);
-        voxel_outputs(a, slot, tag, Vn, st[D::VP + tid], step, s_vm_frame, s_anim_frame);
-      }
-    } else {
-      const int p = (cur - a.n_bricks) * BV + tid;
-      if (p < a.n_pk) purkinje_diffuse(a, p, step);
-    }
-    __syncthreads();
-  }
-  cp_async_wait_all();
-}
-
-constexpr int ION_THREADS = 128;
-
-// The split step keeps the 18 TTP06 states in compact tissue order (index
-// i of active_slot, not the slot), so the ionic half's state loads and
-// stores are fully coalesced; tag, V and W stay per slot for the stencil.
-// mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
-__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off,
-                                                                   int mode) {
-  const int64_t step = *a.d_step + step_off;
-  const bool odd = step & 1;
-  const int64_t istep = mode ? 0 : step + 1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < a.n_active) {
-    const int64_t slot = a.active_slot[i];
-    const uint32_t tag = a.tag[slot];
-    const float Vn = a.Vpost[slot];
-    const int64_t na = a.n_active;
-    CellState cs;
-#pragma unroll
-    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + i];
-    const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
-    const CellParams cp = pheno_params(tag & HP_TAG_PHENO_MASK, a.var_gks[var], a.var_gkr[var]);
-    const float Iion = ttp06_step(Vn, cs, a.dt, cp);
-#pragma unroll
-    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
-    const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
-    float* __restrict__ Wout = mode ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
-    Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
-  } else {
-    const int p = i - a.n_active_pad;
-    if (p >= 0 && p < a.n_pk)
-      purkinje_ionic(a, p, a.pk_Vpost[p], istep, mode ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Crank-Nicolson diffusion half (theta > 0).
 //
 // The reference solves (Cm/dt) V_{i+1} - theta L V_{i+1} = (Cm/dt) W_i +
@@ -837,7 +651,8 @@ __global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, 
 // Every iteration kernel returns at once when the done flag is set, so the
 // host may enqueue iterations in chunks and test the flag between chunks.
 enum CnScal : int { CN_BB = 0, CN_RZ, CN_PQ, CN_ALPHA, CN_BETA, CN_RR, N_CN_SCAL };
-enum CnIScal : int { CI_DONE = 0, CI_ITER, CI_TOTAL, CI_SOLVES, CI_UNCONV, CI_BREAK, N_CN_ISCAL };
+enum CnIScal : int { CI_DONE = 0, CI_ITER, CI_TOTAL, CI_SOLVES, CI_UNCONV, CI_BREAK, CI_LOOP,
+                     N_CN_ISCAL };
 constexpr int CN_TB = 256;   // threads of the vector kernels
 constexpr int CN_NPART = 4;  // partials per block
 
@@ -910,8 +725,291 @@ __device__ bool cn_reduce_last(double (&v)[NV], const CnArgs& c, double (&tot)[N
   return true;
 }
 
-// Stencil pass of the CN solve, persistent CTAs over bricks then chunks of
-// BV Purkinje nodes.
+// ---------------------------------------------------------------------------
+// Split step: two launches per step over the same arrays.
+//
+// mono_diffuse_kernel (one CTA per brick, plus CTAs of BV Purkinje nodes)
+// forms V_{i+1} from W_i and its halo, records the crossings and snapshots of
+// step i and stores V_{i+1} in Vpost.  mono_ionic_kernel then runs the ionic
+// half of step i+1 with one thread per tissue slot, taken from the compact
+// list active_slot, so padding slots of partially filled bricks occupy no
+// lane, and without shared memory or barriers, so it runs at full occupancy.
+// Both do the fused kernels' arithmetic in the same order: results are
+// bit-identical to theirs.
+// Halo copy-table entries per thread of the diffusion kernel (held in
+// registers for the whole launch).  Rows of a face or ij-edge outside the
+// brick in i or j move as BK/4 16-byte chunks, k-face and k-edge elements
+// one by one.
+template <int BI, int BJ, int BK, bool ANISO>
+struct DiffHalo {
+  static constexpr int BV = BI * BJ * BK, Q = BK / 4;
+  static constexpr int W = ANISO ? 2 * (BI + BJ + 2) * Q + 2 * BI * BJ + 4 * (BI + BJ)
+                                 : 2 * (BI + BJ) * Q + 2 * BI * BJ;
+  // face weights (-i, -j, -k faces) and the three off-diagonal tiles
+  static constexpr int A = (BJ + BI) * Q + BI * BJ + (2 * BJ + 2 * BI + 4) * Q +
+                           (2 * BJ * Q + 2 * BI * BJ + 4 * BJ) + (2 * BI * Q + 2 * BI * BJ + 4 * BI);
+  static constexpr int N = ANISO ? W + A : W;
+  static constexpr int PER_THREAD = (N + BV - 1) / BV;
+};
+
+// Shared-memory stage of the diffusion kernel: the staged tiles, then the
+// brick's tags and V_i.
+template <int BI, int BJ, int BK, bool ANISO>
+struct DiffStage {
+  using G = PipeGeom<BI, BJ, BK>;
+  static constexpr int NF = ANISO ? 7 : 1;
+  static constexpr int TAG = NF * G::NT;
+  static constexpr int VP = TAG + G::BV;
+  static constexpr int FLOATS = VP + G::BV;
+  static constexpr int NCHUNK = (NF + 2) * G::BV / 4;  // 16-byte own-brick copies
+};
+
+// CN operations of the diffusion pass (OP template argument; 0 is the
+// explicit step).
+constexpr int OP_STEP = 0, OP_CN_START = 1, OP_CN_APPLY = 2;
+
+// Last-block scalars of a CN stencil pass (mode OP_CN_START or OP_CN_APPLY)
+// from the grid totals: the start of a solve records ||rhs||^2, ||r||^2 and
+// <r, z>_w and tests the warm start; an application forms alpha.
+__device__ __forceinline__ void cn_pass_scalars(const CnArgs& c, int op, const double (&tot)[3]) {
+  if (op == OP_CN_START) {
+    c.scal[CN_BB] = tot[0];
+    c.scal[CN_RR] = tot[1];
+    c.scal[CN_RZ] = tot[2];
+    c.iscal[CI_ITER] = 0;
+    c.iscal[CI_SOLVES] += 1;
+    // converged at the warm start (also a zero right-hand side)
+    c.iscal[CI_DONE] = (tot[1] <= c.tol2 * tot[0] || tot[0] == 0.0) ? 1 : 0;
+  } else {
+    const double pq = tot[0];
+    if (!(pq > 0.0) || !isfinite(pq)) {  // breakdown: keep the current x
+      c.iscal[CI_BREAK] += 1;
+      c.iscal[CI_DONE] = 1;
+    } else {
+      c.scal[CN_PQ] = pq;
+      c.scal[CN_ALPHA] = c.scal[CN_RZ] / pq;
+    }
+  }
+}
+
+// Persistent diffusion pass over bricks (then chunks of BV Purkinje nodes),
+// tiles double-buffered with cp.async.  OP_STEP: the explicit diffusion half
+// of the split step (V_{i+1} from W_i, outputs of step i).  OP_CN_START: the
+// start of a theta-scheme solve on W_i (x = W, r = Lh W, p = Dinv r and
+// their sums).  OP_CN_APPLY: q = p - theta Lh p and <p, q>_w.  The CN
+// passes write tissue entries only: padding entries of the CG vectors are
+// zero from set-up and stay zero.
+template <int BI, int BJ, int BK, bool ANISO, int OP>
+__device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, int step_off) {
+  using G = PipeGeom<BI, BJ, BK>;
+  using H = DiffHalo<BI, BJ, BK, ANISO>;
+  using D = DiffStage<BI, BJ, BK, ANISO>;
+  constexpr int BV = G::BV, NF = D::NF, PT = H::PER_THREAD;
+  constexpr int QB = BV / 4;  // 16-byte chunks per brick row of one field
+  // per-slot fields after the tiles: tag, then V_i (step) or Dinv (start)
+  constexpr int NCHUNK = OP == OP_CN_APPLY ? (NF + 1) * BV / 4 : D::NCHUNK;
+  extern __shared__ __align__(16) float smem[];
+  float* stages = smem;                     // 2 x FLOATS
+  int* ring = (int*)(smem + 2 * D::FLOATS);  // 2 x 27 neighbour lists
+  __shared__ int64_t s_vm_frame, s_anim_frame;
+  if (OP == OP_CN_APPLY && cn.iscal[CI_DONE]) return;
+  const int64_t step = *a.d_step + step_off;
+  const bool odd = step & 1;
+  const float* __restrict__ Win = OP == OP_CN_APPLY ? cn.p : (odd ? a.Vs1 : a.Vs0);
+  const float* __restrict__ Wpk = OP == OP_CN_APPLY ? cn.p + a.n_slots : (odd ? a.pk_Vs1 : a.pk_Vs0);
+  const float* __restrict__ Xtra = OP == OP_STEP ? a.Vpost : cn.dinv;
+  const int tid = threadIdx.x;
+  const int64_t ns = a.n_slots;
+  // this thread's halo copies for the whole launch: stage offset (field tile
+  // + position), neighbour direction, source (array + offset in the brick)
+  uint32_t hpos[PT], hdir[PT];
+  const float* hsrc[PT];
+#pragma unroll
+  for (int q = 0; q < PT; ++q) {
+    const int e = tid + q * BV;
+    const uint32_t t = e < a.n_halo ? a.halo_tab[e] : 0u;
+    const int f = (t >> 11) & 7;
+    hpos[q] = e < a.n_halo ? (uint32_t)(f * G::NT + (int)(t & ((1u << HALO_POS_BITS) - 1)))
+                           : 0xFFFFFFFFu;
+    hdir[q] = ((t >> 14) & 31) | ((t & HALO_CHUNK) ? 32u : 0u);
+    hsrc[q] = e >= a.n_halo ? Win
+                            : (f == 0 ? Win : (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)) +
+                                  ((t >> 19) & 0xFFFu);
+  }
+  auto issue = [&](float* st, const int* nb27, int b) {
+    const int64_t base = (int64_t)b * BV;
+#pragma unroll
+    for (int k = 0; k < (NCHUNK + BV - 1) / BV; ++k) {
+      const int q = tid + k * BV;
+      if (q < NCHUNK) {
+        const int f = q / QB, o = (q % QB) * 4;
+        const float* src = f == 0    ? Win
+                           : f < NF  ? (f < 4 ? a.wface + (f - 1) * ns : a.doff + (f - 4) * ns)
+                           : f == NF ? (const float*)a.tag
+                                     : Xtra;
+        float* dst = f < NF ? st + f * G::NT + G::pos(o / (BJ * BK), (o / BK) % BJ, o % BK)
+                            : st + D::TAG + (f - NF) * BV + o;
+        cp_async16(dst, src + base + o);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      if (hpos[q] != 0xFFFFFFFFu) {
+        const int nb = nb27[hdir[q] & 31];
+        const bool chunk = hdir[q] & 32;
+        if (nb >= 0) {
+          if (chunk)
+            cp_async16(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
+          else
+            cp_async4(st + hpos[q], hsrc[q] + (int64_t)nb * BV);
+        } else if (chunk) {
+          *(float4*)(st + hpos[q]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+          st[hpos[q]] = 0.0f;
+        }
+      }
+    }
+  };
+  const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
+  const int c = G::pos(li, lj, lk);
+  const int G_ = gridDim.x;
+  const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
+  if (tid == 0) {
+    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+  }
+  double v[3] = {0.0, 0.0, 0.0};  // CN sums
+  int cur = blockIdx.x;
+  if (cur < a.n_bricks && tid < 27) ring[tid] = a.nbr[(int64_t)cur * 27 + tid];
+  __syncthreads();
+  if (cur < a.n_bricks) {
+    issue(stages, ring, cur);
+    const int nx = cur + G_;
+    if (nx < a.n_bricks && tid < 27) cp_async4(ring + 27 + tid, a.nbr + (int64_t)nx * 27 + tid);
+  }
+  cp_async_commit();
+  for (int n = 0; cur < n_items; ++n, cur += G_) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int nxt = cur + G_;
+    if (nxt < a.n_bricks) {
+      issue(stages + ((n + 1) & 1) * D::FLOATS, ring + ((n + 1) & 1) * 27, nxt);
+      const int nn = nxt + G_;
+      if (nn < a.n_bricks && tid < 27) cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
+    }
+    cp_async_commit();
+    if (cur < a.n_bricks) {
+      const float* st = stages + (n & 1) * D::FLOATS;
+      const uint32_t tag = ((const uint32_t*)(st + D::TAG))[tid];
+      if (tag & HP_TAG_PHENO_MASK) {
+        const int64_t slot = (int64_t)cur * BV + tid;
+        const float* tW = ANISO ? st + G::NT : st;
+        const float* tD = ANISO ? st + 4 * G::NT : st;
+        if constexpr (OP == OP_STEP) {
+          const float Vn = diffuse<G::SI, G::SJ, G::NT, ANISO>(a, st, tW, tD, c, tag, slot, odd);
+          voxel_outputs(a, slot, tag, Vn, st[D::VP + tid], step, s_vm_frame, s_anim_frame);
+        } else {
+          const float acc = stencil_acc<G::SI, G::SJ, G::NT, ANISO>(a, st, tW, tD, c, tag, slot, Wpk);
+          if constexpr (OP == OP_CN_START) {
+            const float Wi = st[c], z = st[D::VP + tid] * acc, b = Wi + cn.omt * acc;
+            cn.x[slot] = Wi;
+            cn.r[slot] = acc;
+            cn.p[slot] = z;
+            v[0] += (double)b * b;
+            v[1] += (double)acc * acc;
+            v[2] += (double)acc * z;
+          } else {
+            const float pi = st[c], qi = pi - cn.theta * acc;
+            cn.q[slot] = qi;
+            v[0] += (double)pi * qi;
+          }
+        }
+      }
+    } else {
+      const int p = (cur - a.n_bricks) * BV + tid;
+      if (p < a.n_pk) {
+        if constexpr (OP == OP_STEP) {
+          purkinje_diffuse(a, p, step);
+        } else {
+          const float acc = purkinje_acc(a, p, Wpk, Win);
+          const int64_t e = a.n_slots + p;
+          const float w = cn.pk_weight;
+          if constexpr (OP == OP_CN_START) {
+            const float Wi = Wpk[p], z = cn.dinv[e] * acc, b = Wi + cn.omt * acc;
+            cn.x[e] = Wi;
+            cn.r[e] = acc;
+            cn.p[e] = z;
+            v[0] += (double)b * b;
+            v[1] += (double)acc * acc;
+            v[2] += (double)w * acc * z;
+          } else {
+            const float pi = Wpk[p], qi = pi - cn.theta * acc;
+            cn.q[e] = qi;
+            v[0] += (double)w * pi * qi;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
+  if constexpr (OP != OP_STEP) {
+    double tot[3];
+    if (cn_reduce_last<BV, 3>(v, cn, tot) && threadIdx.x == 0) cn_pass_scalars(cn, OP, tot);
+  }
+}
+
+template <int BI, int BJ, int BK, bool ANISO>
+__global__ void __launch_bounds__(BI * BJ * BK)
+mono_diffuse_kernel(MonoArgs a, int step_off) {
+  CnArgs none{};
+  diffuse_pass<BI, BJ, BK, ANISO, OP_STEP>(a, none, step_off);
+}
+
+// The two CN passes on the persistent diffusion kernel's tiles.
+template <int BI, int BJ, int BK, bool ANISO, int OP>
+__global__ void __launch_bounds__(BI * BJ * BK) cn_pass_kernel(MonoArgs a, CnArgs c) {
+  diffuse_pass<BI, BJ, BK, ANISO, OP>(a, c, 0);
+}
+
+constexpr int ION_THREADS = 128;
+
+// The split step keeps the 18 TTP06 states in compact tissue order (index
+// i of active_slot, not the slot), so the ionic half's state loads and
+// stores are fully coalesced; tag, V and W stay per slot for the stencil.
+// mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
+__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off,
+                                                                   int mode) {
+  const int64_t step = *a.d_step + step_off;
+  const bool odd = step & 1;
+  const int64_t istep = mode ? 0 : step + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n_active) {
+    const int64_t slot = a.active_slot[i];
+    const uint32_t tag = a.tag[slot];
+    const float Vn = a.Vpost[slot];
+    const int64_t na = a.n_active;
+    CellState cs;
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + i];
+    const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
+    const CellParams cp = pheno_params(tag & HP_TAG_PHENO_MASK, a.var_gks[var], a.var_gkr[var]);
+    const float Iion = ttp06_step(Vn, cs, a.dt, cp);
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
+    const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
+    float* __restrict__ Wout = mode ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
+    Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+  } else {
+    const int p = i - a.n_active_pad;
+    if (p >= 0 && p < a.n_pk)
+      purkinje_ionic(a, p, a.pk_Vpost[p], istep, mode ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
+  }
+}
+
+// Stencil pass of the CN solve with plain halo loads, persistent CTAs over
+// bricks then chunks of BV Purkinje nodes (the set-up pass, and the whole
+// solve where the persistent diffusion kernel is not used).
 //   mode 0 (start of a step): x = W, r = Lh W, p = Dinv r; sums
 //          ||W + (1 - theta) Lh W||^2, ||r||^2, <r, Dinv r>_w;
 //   mode 1 (iteration): q = p - theta Lh p; sum <p, q>_w, alpha = rz / pq;
@@ -1005,26 +1103,8 @@ cn_stencil_kernel(MonoArgs a, CnArgs c, int mode) {
   }
   if (mode == 2) return;
   double tot[3];
-  if (!cn_reduce_last<BV, 3>(v, c, tot)) return;
-  if (threadIdx.x != 0) return;
-  if (mode == 0) {
-    c.scal[CN_BB] = tot[0];
-    c.scal[CN_RR] = tot[1];
-    c.scal[CN_RZ] = tot[2];
-    c.iscal[CI_ITER] = 0;
-    c.iscal[CI_SOLVES] += 1;
-    // converged at the warm start (also a zero right-hand side)
-    c.iscal[CI_DONE] = (tot[1] <= c.tol2 * tot[0] || tot[0] == 0.0) ? 1 : 0;
-  } else {
-    const double pq = tot[0];
-    if (!(pq > 0.0) || !isfinite(pq)) {  // breakdown: keep the current x
-      c.iscal[CI_BREAK] += 1;
-      c.iscal[CI_DONE] = 1;
-    } else {
-      c.scal[CN_PQ] = pq;
-      c.scal[CN_ALPHA] = c.scal[CN_RZ] / pq;
-    }
-  }
+  if (cn_reduce_last<BV, 3>(v, c, tot) && threadIdx.x == 0)
+    cn_pass_scalars(c, mode == 0 ? OP_CN_START : OP_CN_APPLY, tot);
 }
 
 // x += alpha p, r -= alpha q; sums ||r||^2 and <r, Dinv r>_w; the last block
@@ -1094,6 +1174,19 @@ __global__ void __launch_bounds__(ION_THREADS) cn_finish_kernel(MonoArgs a, CnAr
       if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p] = Vn;
     }
   }
+}
+
+// Loop condition of a solve captured in a CUDA graph (a conditional WHILE
+// node): before the loop (init) "not yet converged", after each iteration
+// "not converged and fewer than max_iter iterations".  Its own counter
+// bounds the loop whatever the other kernels do.
+__global__ void cn_cond_kernel(cudaGraphConditionalHandle hd, CnArgs c, int init) {
+  int n = 0;
+  if (init)
+    c.iscal[CI_LOOP] = 0;
+  else
+    n = ++c.iscal[CI_LOOP];
+  cudaGraphSetConditional(hd, (!c.iscal[CI_DONE] && n < c.max_iter) ? 1u : 0u);
 }
 
 // Host: halo copy table of the pipelined and split-diffusion kernels for
@@ -1170,6 +1263,7 @@ __global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
 
 typedef void (*StepFn)(MonoArgs, int, int);
 typedef void (*CnFn)(MonoArgs, CnArgs, int);
+typedef void (*CnPassFn)(MonoArgs, CnArgs);
 typedef void (*PipeFn)(MonoArgs, int);  // also the diffusion half of the split step
 typedef std::vector<uint32_t> (*HaloFn)(bool);
 
@@ -1183,6 +1277,7 @@ struct ShapeEntry {
   int diff_cap_iso, diff_cap_aniso;  // halo entries the diffusion kernel holds
   int diff_floats_iso, diff_floats_aniso;
   CnFn cn_iso, cn_aniso;
+  CnPassFn start_iso, start_aniso, apply_iso, apply_aniso;
 };
 
 #define HP_SHAPE(I, J, K)                                                                    \
@@ -1192,7 +1287,9 @@ struct ShapeEntry {
    PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS,                      \
    DiffHalo<I, J, K, false>::PER_THREAD * I * J * K, DiffHalo<I, J, K, true>::PER_THREAD * I * J * K, \
    DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS,                      \
-   cn_stencil_kernel<I, J, K, false>, cn_stencil_kernel<I, J, K, true>}
+   cn_stencil_kernel<I, J, K, false>, cn_stencil_kernel<I, J, K, true>,                      \
+   cn_pass_kernel<I, J, K, false, OP_CN_START>, cn_pass_kernel<I, J, K, true, OP_CN_START>,  \
+   cn_pass_kernel<I, J, K, false, OP_CN_APPLY>, cn_pass_kernel<I, J, K, true, OP_CN_APPLY>}
 static const ShapeEntry kShapes[] = {HP_SHAPE(4, 4, 8), HP_SHAPE(4, 8, 8), HP_SHAPE(2, 4, 16),
                                      HP_SHAPE(8, 8, 8)};
 #undef HP_SHAPE
@@ -1211,12 +1308,18 @@ struct HpMono {
   int diff_grid;     // its persistent grid
   int ion_grid;      // grid of the ionic half
   size_t diff_smem;  // and dynamic shared memory per CTA
-  CnFn cn;           // theta > 0: stencil pass of the CN solve, or null
+  CnFn cn;           // theta > 0: set-up stencil pass (Jacobi diagonal), or null
+  CnPassFn cn_start, cn_apply;  // tiled passes: start of a solve, A p
   CnArgs cn_a;
-  int cn_grid;       // persistent grid of the stencil pass
+  int cn_grid;       // persistent grid of the set-up pass
+  int cn_pgrid;      // persistent grid of the tiled passes
   int cn_vgrid;      // grid of the vector kernels
   int cn_chunk;      // iterations enqueued before the next flag test
   int32_t* cn_host;  // pinned copy of the done flag and iteration count
+  cudaStream_t cn_body_stream;  // captures the bodies of the solve loops
+  cudaGraphExec_t cn_graph;     // steps with device-side solve loops
+  int cn_graph_steps;
+  cudaStream_t cn_graph_stream;
   int bv;
   int64_t n_steps, steps_done;
   int64_t n_vm_frames, n_anim_frames;
@@ -1379,12 +1482,23 @@ static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, 
   c.tol2 = tol * tol;
   c.max_iter = d->cn_max_iter;
   h->cn = d->anisotropic ? se->cn_aniso : se->cn_iso;
-  int dev = 0, n_sm = 0, per_sm = 0;
+  h->cn_start = d->anisotropic ? se->start_aniso : se->start_iso;
+  h->cn_apply = d->anisotropic ? se->apply_aniso : se->apply_iso;
+  int dev = 0, n_sm = 0, per_sm = 0, per_sm_s = 0, per_sm_a = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
   HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
   HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->cn, h->bv, 0));
   const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   h->cn_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
+  // the tiled passes use the split diffusion kernel's shared-memory stages
+  for (CnPassFn f : {h->cn_start, h->cn_apply})
+    HP_CUDA_TRY(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)h->diff_smem));
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s, (const void*)h->cn_start,
+                                                            h->bv, h->diff_smem));
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_a, (const void*)h->cn_apply,
+                                                            h->bv, h->diff_smem));
+  h->cn_pgrid = std::max(1, std::min(n_items, std::max(std::min(per_sm_s, per_sm_a), 1) * n_sm));
   h->cn_vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + CN_TB - 1) / CN_TB, 8 * n_sm));
   h->cn_chunk = 4;
   HP_TRY_NODESTROY(al(h, &c.x, n));
@@ -1392,18 +1506,31 @@ static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, 
   HP_TRY_NODESTROY(al(h, &c.p, n));
   HP_TRY_NODESTROY(al(h, &c.q, n));
   HP_TRY_NODESTROY(al(h, &c.dinv, n));
-  HP_TRY_NODESTROY(al(h, &c.part, (size_t)std::max(h->cn_grid, h->cn_vgrid) * CN_NPART));
+  HP_TRY_NODESTROY(al(h, &c.part,
+                       (size_t)std::max({h->cn_grid, h->cn_pgrid, h->cn_vgrid}) * CN_NPART));
   HP_TRY_NODESTROY(al(h, &c.scal, N_CN_SCAL));
   HP_TRY_NODESTROY(al(h, &c.iscal, N_CN_ISCAL));
   HP_TRY_NODESTROY(al(h, &c.ticket, 1));
   HP_CUDA_TRY(cudaMemsetAsync(c.scal, 0, N_CN_SCAL * sizeof(double), s));
   HP_CUDA_TRY(cudaMemsetAsync(c.iscal, 0, N_CN_ISCAL * sizeof(int32_t), s));
   HP_CUDA_TRY(cudaMemsetAsync(c.ticket, 0, sizeof(unsigned int), s));
-  HP_CUDA_TRY(cudaMemsetAsync(c.p, 0, n * sizeof(float), s));
+  // padding entries of the CG vectors stay zero (the passes skip them)
+  for (float* v : {c.x, c.r, c.p, c.q}) HP_CUDA_TRY(cudaMemsetAsync(v, 0, n * sizeof(float), s));
   HP_CUDA_TRY(cudaMallocHost((void**)&h->cn_host, 2 * sizeof(int32_t)));
+  HP_CUDA_TRY(cudaStreamCreateWithFlags(&h->cn_body_stream, cudaStreamNonBlocking));
   h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 2);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
+}
+
+// One CG iteration of the theta-scheme solve: q = M p (tiled pass, alpha),
+// x and r updates (beta, stopping test), new direction.  Every kernel
+// returns at once once the done flag is set.
+static void cn_iteration(HpMono* h, cudaStream_t s) {
+  const CnArgs& c = h->cn_a;
+  h->cn_apply<<<h->cn_pgrid, h->bv, h->diff_smem, s>>>(h->a, c);
+  cn_update_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c, h->a.n_slots);
+  cn_dir_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c);
 }
 
 // One theta-scheme step: the stencil pass that starts the solve, CG
@@ -1411,16 +1538,12 @@ static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, 
 // flag, the outputs of V_{i+1} = clamp(x), the ionic half and the step count.
 static hp_status cn_step(HpMono* h, cudaStream_t s) {
   const CnArgs& c = h->cn_a;
-  h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 0);
+  h->cn_start<<<h->cn_pgrid, h->bv, h->diff_smem, s>>>(h->a, c);
   HP_CUDA_TRY(cudaGetLastError());
   int launched = 0;
   while (launched < c.max_iter) {
     const int k = std::min(h->cn_chunk, c.max_iter - launched);
-    for (int j = 0; j < k; ++j) {
-      h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 1);
-      cn_update_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c, h->a.n_slots);
-      cn_dir_kernel<<<h->cn_vgrid, CN_TB, 0, s>>>(c);
-    }
+    for (int j = 0; j < k; ++j) cn_iteration(h, s);
     HP_CUDA_TRY(cudaGetLastError());
     launched += k;
     HP_CUDA_TRY(cudaMemcpyAsync(h->cn_host, c.iscal + CI_DONE, 2 * sizeof(int32_t),
@@ -1436,6 +1559,78 @@ static hp_status cn_step(HpMono* h, cudaStream_t s) {
   }
   advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, 1);
   HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// Captures n theta-scheme steps on s (which is capturing): per step the
+// start pass, the loop-condition kernel and a conditional WHILE node whose
+// body (captured on cn_body_stream) is one CG iteration plus the condition
+// update, then the outputs, the ionic half and the step count.  No host
+// round trip per step.
+static hp_status cn_capture_steps(HpMono* h, int n, cudaStream_t s) {
+  const CnArgs& c = h->cn_a;
+  cudaStream_t sb = h->cn_body_stream;
+  for (int k = 0; k < n; ++k) {
+    h->cn_start<<<h->cn_pgrid, h->bv, h->diff_smem, s>>>(h->a, c);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    HP_CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle hd;
+    HP_CUDA_TRY(cudaGraphConditionalHandleCreate(&hd, g, 0, 0));
+    cn_cond_kernel<<<1, 1, 0, s>>>(hd, c, 1);
+    HP_CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = hd;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    HP_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    HP_CUDA_TRY(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed));
+    cn_iteration(h, sb);
+    cn_cond_kernel<<<1, 1, 0, sb>>>(hd, c, 0);
+    cudaGraph_t bo = nullptr;
+    HP_CUDA_TRY(cudaStreamEndCapture(sb, &bo));
+    HP_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    if (h->ion_grid > 0) {
+      cn_finish_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, c);
+      mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0, 0);
+    }
+    advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, 1);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  return HP_OK;
+}
+
+// (Re)builds the graph of n theta-scheme steps for stream s.
+static hp_status cn_build_graph(HpMono* h, int n, cudaStream_t s) {
+  if (h->cn_graph) {
+    cudaGraphExecDestroy(h->cn_graph);
+    h->cn_graph = nullptr;
+  }
+  HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const hp_status st = cn_capture_steps(h, n, s);
+  cudaStreamCaptureStatus bs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->cn_body_stream, &bs) == cudaSuccess &&
+      bs != cudaStreamCaptureStatusNone) {
+    cudaGraph_t dead = nullptr;
+    cudaStreamEndCapture(h->cn_body_stream, &dead);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (st != HP_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  HP_CUDA_TRY(ce);
+  const cudaError_t ie = cudaGraphInstantiate(&h->cn_graph, g, 0);
+  cudaGraphDestroy(g);
+  HP_CUDA_TRY(ie);
+  h->cn_graph_steps = n;
+  h->cn_graph_stream = s;
   return HP_OK;
 }
 
@@ -1490,6 +1685,10 @@ extern "C" hp_status hp_mono_create(const HpMonoDesc* d, HpMono** out, void* str
   h->ion_grid = 0;
   h->cn = nullptr;
   h->cn_host = nullptr;
+  h->cn_body_stream = nullptr;
+  h->cn_graph = nullptr;
+  h->cn_graph_steps = 0;
+  h->cn_graph_stream = nullptr;
   h->anisotropic = d->anisotropic;
   h->n_steps = d->n_steps;
   h->steps_done = 0;
@@ -1649,8 +1848,22 @@ extern "C" hp_status hp_mono_run(HpMono* h, int64_t n, int32_t graph_chunk, void
              "hp_mono_run: %lld steps requested, %lld remain", (long long)n,
              (long long)(h->n_steps - h->steps_done));
   cudaStream_t s = (cudaStream_t)stream;
-  if (h->cn) {  // theta-scheme: the host tests convergence between chunks
-    for (int64_t o = 0; o < n; ++o) {
+  if (h->cn) {
+    // theta-scheme: graphs of up to 16 steps whose solve loops run on the
+    // device (conditional nodes); the remainder, and the legacy default
+    // stream that cannot be captured, test convergence on the host
+    int64_t left = n;
+    const int gs = (int)std::min<int64_t>(graph_chunk, 16);
+    if (gs > 0 && left >= gs && s != nullptr) {
+      if (!h->cn_graph || h->cn_graph_steps != gs || h->cn_graph_stream != s)
+        HP_TRY_NODESTROY(cn_build_graph(h, gs, s));
+      while (left >= gs) {
+        HP_CUDA_TRY(cudaGraphLaunch(h->cn_graph, s));
+        left -= gs;
+        h->steps_done += gs;
+      }
+    }
+    for (; left > 0; --left) {
       hp_status st = cn_step(h, s);
       if (st != HP_OK) return st;
       h->steps_done += 1;
@@ -1830,6 +2043,8 @@ extern "C" hp_status hp_mono_cn_stats(HpMono* h, int64_t* iterations, int64_t* s
 extern "C" hp_status hp_mono_destroy(HpMono* h) {
   if (!h) return HP_OK;
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->cn_graph) cudaGraphExecDestroy(h->cn_graph);
+  if (h->cn_body_stream) cudaStreamDestroy(h->cn_body_stream);
   if (h->cn_host) cudaFreeHost(h->cn_host);
   for (void* p : h->allocs) cudaFree(p);
   delete h;

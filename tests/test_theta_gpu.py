@@ -96,3 +96,24 @@ def test_theta_public_api(tmp_path, golden):
     assert (tmp_path / "c.npz").exists() and (tmp_path / "vm.npz").exists()
     assert np.isfinite(res["vm_snapshots"]).all()
     assert np.max(np.abs(res["activation_times"][:, 0] - g["act_cn"][:, 0])) <= ACT_TOL
+
+
+def test_theta_graph_and_host_loop_agree():
+    """Device-side solve loops (conditional graph nodes) and the host-tested
+    chunks run the same kernels in the same order: bit-identical results,
+    same iteration counts."""
+    from hrdayapy_b200 import monodomain as M
+    args, fibre, kw = cases.aniso_case()
+    nodes, el, act, S, phi = args
+    out = []
+    for chunk in (0, 16):
+        prob, _ = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=True,
+                            vm_save_dt=kw["dt"], theta=0.5, cg_tol=1e-6,
+                            **dict(kw, A_P=2.0 / kw["R_P"], T=4.0))
+        sim = M.MonoHandle(prob)
+        sim.run(prob.n_steps, graph_chunk=chunk)
+        out.append((sim.vm_frames(), sim.voltage()[1], sim.cn_stats()))
+        sim.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
