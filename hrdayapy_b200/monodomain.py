@@ -582,6 +582,10 @@ def run(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None, anisotr
                    branch_map=info["branch_map"], branch_frames_p=branch_frames,
                    surf_verts=sv, surf_faces=sf, vert_to_surf_node=vs, frames_surf=surf,
                    times=times)
+    # node bookkeeping of the snapshot / activation-map files
+    results["node_ids"] = np.arange(len(info["vox_idx"]), dtype=np.int32) + Np
+    results["coords_mm"] = info["nodes_mm"]
+    results["vox_idx"] = info["vox_idx"]
     me = prob.max_events
     results["activation_times"] = _events_table(act, nact, me)
     results["n_activations"] = nact
@@ -594,6 +598,7 @@ def run(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None, anisotr
                           info["nodes_mm"], info["vox_idx"], vm, tv, dt, ve * dt)
         results["vm_snapshots"] = vm
         results["time_vm"] = tv
+        results["vm_snapshots_path"] = str(Path(out_vm_npz).with_suffix(".npz"))
     if out_npz is not None:
         save_npz(results, out_npz)
     return results

@@ -18,6 +18,10 @@ Fixtures (all seeded, small enough to commit):
                        coupled Purkinje tree (root stimulus, c_pmj=0.01 mS)
                        and a myocardial focus stimulated at t = 1 ms.
                        Also the theta=0.5 activation map for the scheme gap.
+* act_maps_iso.npz  -- compute_activation_maps + save_activation_maps on the
+                       snapshots (every 0.5 ms) of a 340 ms run_coupled on
+                       the isotropic slab (activation and repolarisation),
+                       and on a seeded chattering trace with debounce.
 * torso.npz         -- _assemble_stiffness / _find_surface_ids on a small
                        synthetic torso, build_heart_laplacian /
                        build_projection_map, and solve_frame on one Vm frame.
@@ -263,10 +267,58 @@ def torso():
         phi_full_ref=phi_full, ref_iters=n_it)
 
 
+def act_maps():
+    """The upstream activation-map writer on upstream snapshots; keys are
+    prefixed "slab_" (340 ms isotropic run, thresholds -20 / -60 mV) and
+    "chatter_" (synthetic trace, debounce 3 ms, whose input is stored)."""
+    nx, ny, nz = 16, 16, 4
+    h, dt, T, vdt = 0.25, 0.02, 340.0, 0.5
+    S = np.ones((nx, ny, nz), np.uint8)
+    phi = np.ones(S.shape, np.float32)
+    ect = np.zeros(S.shape, bool)
+    ect[:4, :4, :] = True
+    nodes, el, act = _stub(nx, ny, nz)
+    prot = [dict(name="corner", target="ectopic", amp=0.52, dur=1.0, onset=0.0)]
+    am = ref.activation_maps
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        vm_path = Path(td) / "vm.npz"
+        quiet(ref.pipeline.run_coupled, nodes, el, act, S, S.copy(), phi,
+              voxel_size=h, dx_p=0.25, sigma_P=0.0, sigma_M=0.13, Cm=0.01, A_P=133.33,
+              A_M=140.0, R_P=0.015, dt=dt, T=T, theta=0.0, stim_protocol=prot,
+              ectopic_region=ect, stim_len_mm=1.0, c_pmj=0.0, n_pmj=1,
+              cg_tol=1e-12, cg_max_iter=200, n_frames=10, device="cpu",
+              dtype=torch.float64, vm_save_dt=vdt, out_vm_npz=vm_path)
+        snap = quiet(ref.load_vm_snapshots.load_vm_snapshots, vm_path)
+        mp = Path(td) / "maps.npz"
+        quiet(am.compute_activation_maps, snap, S, act_threshold=-20.0, deact_threshold=-60.0,
+              save_path=mp)
+        z = np.load(mp)
+        out.update({"slab_" + k: z[k] for k in z.files if k != "source_vm_path"})
+        # chattering synthetic trace: every crossing kept, then debounced
+        rng = np.random.default_rng(11)
+        t = np.arange(120, dtype=np.float32) * 0.5
+        Vm = (-40.0 + 25.0 * np.sin(t[:, None] / 3.0 + rng.uniform(0, 6, 6)[None, :])
+              + rng.normal(0, 6.0, (120, 6))).astype(np.float32)
+        vs = ref.load_vm_snapshots.VmSnapshots(
+            node_ids=np.arange(6, dtype=np.int32), coords_mm=rng.uniform(0, 5, (6, 3)).astype(np.float32),
+            vox_idx=np.stack([np.arange(6), np.zeros(6, int), np.zeros(6, int)], 1).astype(np.int32),
+            Vm=Vm, time_vm=t, dt_solver=0.5, vm_save_dt=0.5, path=Path("chatter.npz"))
+        cp = Path(td) / "chatter.npz"
+        quiet(am.compute_activation_maps, vs, None, act_threshold=-40.0, deact_threshold=-45.0,
+              min_event_gap_ms=3.0, save_path=cp)
+        z = np.load(cp)
+        out.update({"chatter_" + k: z[k] for k in z.files if k != "source_vm_path"})
+        out.update(chatter_in_Vm=Vm, chatter_in_t=t, chatter_in_coords=vs.coords_mm,
+                   chatter_in_vox=vs.vox_idx)
+    out.update(h=h, dt=dt, T=T, vm_save_dt=vdt)
+    np.savez_compressed(HERE / "act_maps_iso.npz", **out)
+
+
 if __name__ == "__main__":
     torch.set_num_threads(8)
-    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "torso"]
+    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "torso"]
     for w in which:
         print("generating", w, flush=True)
         {"cells": ttp06_cells, "pacing": ttp06_pacing, "iso": mono_iso,
-         "aniso": mono_aniso, "torso": torso}[w]()
+         "aniso": mono_aniso, "maps": act_maps, "torso": torso}[w]()

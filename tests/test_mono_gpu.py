@@ -185,3 +185,22 @@ def test_public_api_writes_reference_schema(tmp_path):
     c = np.load(tmp_path / "c.npz")
     assert "surf_frames" in c.files and "branch_0" in c.files
     assert res["activation_times"].shape[0] == S.size
+
+
+def test_activation_map_file_from_gpu_events(golden, tmp_path):
+    """The in-loop GPU event tables written as the upstream activation-map
+    file: loadable, and the activation times match the upstream map."""
+    from hrdayapy_b200.simulation import (activation_maps_from_run, load_activation_maps,
+                                          run_coupled)
+    g = golden("mono_iso.npz")
+    args, kw = cases.iso_case()
+    nodes, el, act, S, phi = args
+    res = run_coupled(nodes, el, act, S, S, phi, theta=0.0, act_threshold=-20.0,
+                      deact_threshold=-20.0, **kw)
+    activation_maps_from_run(res, S, act_threshold=-20.0, deact_threshold=-20.0,
+                             save_path=tmp_path / "maps.npz")
+    m = load_activation_maps(tmp_path / "maps.npz")
+    assert tuple(m.grid_shape) == S.shape
+    np.testing.assert_array_equal(m.vox_idx, g["vox_idx"])
+    assert np.max(np.abs(m.activation_map(1) - g["act"][:, 0])) <= ACT_TOL
+    assert (m.n_activations == 1).all()
