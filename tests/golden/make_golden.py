@@ -22,6 +22,10 @@ Fixtures (all seeded, small enough to commit):
                        snapshots (every 0.5 ms) of a 340 ms run_coupled on
                        the isotropic slab (activation and repolarisation),
                        and on a seeded chattering trace with debounce.
+* pmj_exp4.npz      -- the upstream Experiment 4 core
+                       (experiments/experiment_3/experiment_common.py
+                       run_directional) on its slab + fibre at dx 0.25 mm:
+                       orthodromic capture and block, antidromic capture.
 * torso.npz         -- _assemble_stiffness / _find_surface_ids on a small
                        synthetic torso, build_heart_laplacian /
                        build_projection_map, and solve_frame on one Vm frame.
@@ -315,10 +319,54 @@ def act_maps():
     np.savez_compressed(HERE / "act_maps_iso.npz", **out)
 
 
+PMJ_CASES = (  # (tag, direction, c_pmj, T)
+    ("ortho", "orthodromic", 5.0, 80.0),
+    ("ortho_block", "orthodromic", 1e-5, 40.0),
+    ("anti", "antidromic", 5.0, 100.0))
+PMJ_GRID = dict(dx_m=0.25, dx_p=0.25, dt=0.05, n_pmj=1)
+
+
+def pmj_exp4():
+    """Runs the upstream experiment core unchanged: its package imports are
+    served by the upstream modules loaded by path."""
+    import types
+    hp = _refload.REF_ROOT / "hrdayapy"
+    exp = _refload.REF_ROOT / "experiments" / "experiment_3"
+    afn = sys.modules["hrdayapy.anisotropic_simulation.functions"]
+    afn.purkinje_myocardium_anisotropic_solver = ref.aniso.purkinje_myocardium_anisotropic_solver
+    afn.load_vm_snapshots = _refload._load(
+        "hrdayapy.anisotropic_simulation.functions.load_vm_snapshots",
+        hp / "anisotropic_simulation" / "functions" / "load_vm_snapshots.py").load_vm_snapshots
+    afn.compute_activation_maps = _refload._load(
+        "hrdayapy.anisotropic_simulation.functions.activation_maps",
+        hp / "anisotropic_simulation" / "functions" / "activation_maps.py").compute_activation_maps
+    _refload._load("hrdayapy._spacing_resolve", hp / "_spacing_resolve.py")
+    coupled = _refload._load("hrdayapy.anisotropic_simulation.coupled",
+                             hp / "anisotropic_simulation" / "coupled.py")
+    sys.modules["hrdayapy.anisotropic_simulation"].compute_anisotropic_coupled = \
+        coupled.compute_anisotropic_coupled
+    sys.modules["hrdayapy.simulation.functions"].activation_maps = ref.activation_maps
+    sys.path.insert(0, str(exp))
+    ec = _refload._load("experiment_common", exp / "experiment_common.py")
+    out = dict(PMJ_GRID)
+    g = PMJ_GRID
+    for tag, direction, c_pmj, T in PMJ_CASES:
+        with tempfile.TemporaryDirectory() as td:
+            r = quiet(ec.run_directional, ec.SIGMA_L, ec.SIGMA_T, ec.SIGMA_P, g["dt"], g["dx_p"],
+                      g["dx_m"], T, tag, c_pmj, g["n_pmj"], direction, Path(td))
+        for k in ("myo_act", "p_act", "p_arc_length", "pmj_junction_capture_fraction",
+                  "pmj_propagating_capture", "pmj_n_myo_activated", "pmj_delay_ms",
+                  "pmj_coupled_myo_idx"):
+            out[f"{tag}_{k}"] = np.asarray(r[k])
+        out[f"{tag}_T"] = T
+        out[f"{tag}_c_pmj"] = c_pmj
+    np.savez_compressed(HERE / "pmj_exp4.npz", **out)
+
+
 if __name__ == "__main__":
     torch.set_num_threads(8)
-    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "torso"]
+    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso"]
     for w in which:
         print("generating", w, flush=True)
         {"cells": ttp06_cells, "pacing": ttp06_pacing, "iso": mono_iso,
-         "aniso": mono_aniso, "maps": act_maps, "torso": torso}[w]()
+         "aniso": mono_aniso, "maps": act_maps, "pmj": pmj_exp4, "torso": torso}[w]()
