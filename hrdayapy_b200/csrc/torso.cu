@@ -62,6 +62,11 @@ struct TorsoArgs {
   int32_t* iscal;
   double* part;        // gridDim x NPART
   unsigned int* ticket;
+  // tissue lines: the k-run from the first to the last tissue cell of every
+  // (i, j) line that has one (air inside a run is allowed)
+  int32_t n_lines;
+  const int64_t* line_g0;
+  const int32_t* line_len;
 };
 
 __constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
@@ -144,50 +149,104 @@ __device__ __forceinline__ bool is_row(const TorsoArgs& a, int64_t g) {
   return a.label[g] != 0 && g != a.pin;
 }
 
+// The PCG vector kernels walk tissue lines, one warp per line (lanes over
+// consecutive k, coalesced rows), loading a batch of LB chunks of 32 cells
+// before any arithmetic so every thread has several independent loads in
+// flight.  Air lines are never touched; inside a line the vectors are zero
+// on air cells and at the pinned voxel (r, p, x start at 0 and only row
+// cells are ever written non-zero; invd is 0 there), so no labels are read.
+template <int LB, class Load, class Apply>
+__device__ __forceinline__ void for_line_batches(const TorsoArgs& a, Load&& load, Apply&& apply) {
+  const int lane = threadIdx.x & 31;
+  const int n_warps = gridDim.x * (TB / 32);
+  for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
+    const int64_t g0 = a.line_g0[L];
+    const int len = a.line_len[L];
+    for (int k0 = lane; k0 < len; k0 += 32 * LB) {
+#pragma unroll
+      for (int u = 0; u < LB; ++u)
+        if (k0 + 32 * u < len) load(u, g0 + k0 + 32 * u);
+#pragma unroll
+      for (int u = 0; u < LB; ++u)
+        if (k0 + 32 * u < len) apply(u, g0 + k0 + 32 * u);
+    }
+  }
+}
+
 // Iteration part 1a: pending x update and p <- M^-1 r + beta p, in place
-// (one buffer: every thread reads and writes only its own cells).
+// (every thread reads and writes only its own cells).
 __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha_prev = a.scal[SC_ALPHA_PREV];
   const float betaf = (float)a.scal[SC_BETA];
-  const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ invd = a.invd;
   const float* __restrict__ r = a.r;
   float* __restrict__ p = a.p0;
   double* __restrict__ x = a.x;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
-#pragma unroll 4
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
-    if (lab[g] == 0 || g == pin) continue;
-    const float pold = p[g];
-    if (alpha_prev != 0.0) x[g] += alpha_prev * (double)pold;
-    p[g] = invd[g] * r[g] + betaf * pold;
+  constexpr int LB = 4;
+  float pv[LB], zv[LB];
+  if (alpha_prev != 0.0) {
+    double xv[LB];
+    for_line_batches<LB>(
+        a, [&](int u, int64_t g) { pv[u] = p[g]; zv[u] = invd[g] * r[g]; xv[u] = x[g]; },
+        [&](int u, int64_t g) {
+          x[g] = xv[u] + alpha_prev * (double)pv[u];
+          p[g] = zv[u] + betaf * pv[u];
+        });
+  } else {
+    for_line_batches<LB>(
+        a, [&](int u, int64_t g) { pv[u] = p[g]; zv[u] = invd[g] * r[g]; },
+        [&](int u, int64_t g) { p[g] = zv[u] + betaf * pv[u]; });
   }
 }
 
 // Iteration part 1b: Ap = A p as a sum of face fluxes t (p_g - p_n) (exact
 // for equal neighbours, so a smooth p keeps its small A p instead of a
 // difference of two large sums), partial p.Ap; the last block forms alpha
-// and clears the pending x update (part 1a applied it).
+// and clears the pending x update (part 1a applied it).  One warp per
+// tissue line; all thirteen loads of a cell are issued before the sums
+// (32-bit neighbour offsets keep the addressing to one base per array).
+// The conductance table sits in shared memory (its reads diverge across a
+// warp at material boundaries).  A shared-memory 2.5-D blocked variant
+// (8 x 32 columns marching in i) measured slower on B200: it is
+// latency-bound at one plane in flight per block.
 __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
+  __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
+  __syncthreads();
   const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
-  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
+  const int sj = a.pk, si = a.pj * a.pk;   // the padded plane fits in 32 bits
+  const int64_t pin = a.pin;
+  const int lane = threadIdx.x & 31;
+  const int n_warps = gridDim.x * (TB / 32);
   double acc[1] = {0.0};
-#pragma unroll 2
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
-    const int l = lab[g];
-    if (l == 0 || g == pin) continue;
-    const float pg = p[g];
-    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    float ap = 0.0f;
+  for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
+    const int64_t g0 = a.line_g0[L];
+    const int len = a.line_len[L];
+    for (int k = lane; k < len; k += 32) {
+      const int64_t g = g0 + k;
+      const uint8_t* __restrict__ lc = lab + g;
+      const float* __restrict__ pc = p + g;
+      const int off[6] = {si, -si, sj, -sj, 1, -1};
+      const int l = lc[0];
+      const float pg = pc[0];
+      int ln[6];
+      float pn[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) ap += c_T32[l * HP_MAX_MATERIALS + lab[nb[f]]] * (pg - p[nb[f]]);
-    Ap[g] = ap;
-    acc[0] += (double)pg * (double)ap;
+      for (int f = 0; f < 6; ++f) {
+        ln[f] = lc[off[f]];
+        pn[f] = pc[off[f]];
+      }
+      float ap = 0.0f;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) ap += T[l * HP_MAX_MATERIALS + ln[f]] * (pg - pn[f]);
+      if (l == 0 || g == pin) ap = 0.0f;
+      Ap[g] = ap;
+      acc[0] += (double)pg * (double)ap;
+    }
   }
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
@@ -211,23 +270,23 @@ __global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float alphaf = (float)alpha;
-  const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ invd = a.invd;
   const float* __restrict__ Ap = a.Ap;
   float* __restrict__ rv = a.r;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
-    if (lab[g] == 0 || g == pin) continue;
-    const float r = rv[g] - alphaf * Ap[g];
-    rv[g] = r;
-    const float z = invd[g] * r;
-    acc[0] += (double)r * z;
-    acc[1] += (double)z * z;
-    acc[2] += (double)r * r;
-    acc[3] = fmax(acc[3], (double)fabsf(z));
-  }
+  constexpr int LB = 8;
+  float rb[LB], ib[LB];
+  for_line_batches<LB>(
+      a, [&](int u, int64_t g) { rb[u] = rv[g] - alphaf * Ap[g]; ib[u] = invd[g]; },
+      [&](int u, int64_t g) {
+        const float r = rb[u];
+        rv[g] = r;
+        const float z = ib[u] * r;
+        acc[0] += (double)r * z;
+        acc[1] += (double)z * z;
+        acc[2] += (double)r * r;
+        acc[3] = fmax(acc[3], (double)fabsf(z));
+      });
   double tot[4];
   if (block_reduce_last<4>(acc, true, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double rz_new = tot[0];
@@ -375,6 +434,7 @@ struct HpTorso {
   TorsoArgs a;
   SrcArgs s;
   int nblk;
+  int nblk_k[3];  // PCG iteration kernels: each one's resident grid
   int ni, nj, nk;
   int64_t n_rows;
   std::vector<void*> allocs;
@@ -520,6 +580,16 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   }
   h->nblk = nsm * 8;
+  {
+    // the line loops stride over the grid, so a grid larger than what is
+    // resident would leave a tail wave: each kernel gets its resident grid
+    int o = 0;
+    const void* fs[3] = {(const void*)pcg_p_update, (const void*)pcg_ap, (const void*)pcg_k2};
+    for (int q = 0; q < 3; ++q) {
+      HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fs[q], TB, 0));
+      h->nblk_k[q] = nsm * std::min(8, std::max(o, 1));
+    }
+  }
   TT_TRY(tal(h, &a.scal, N_SCAL));
   TT_TRY(tal(h, &a.iscal, N_ISCAL));
   TT_TRY(tal(h, &a.part, (size_t)h->nblk * NPART));
@@ -528,6 +598,30 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   HP_CUDA_TRY(cudaMemsetAsync(a.iscal, 0, N_ISCAL * 4, s));
   HP_CUDA_TRY(cudaMemsetAsync(a.ticket, 0, 4, s));
   TT_TRY(tup(h, &h->grid_of_row, grid_of_row.data(), n_rows, s));
+  {
+    // tissue lines of the padded grid: first .. last tissue cell in k
+    std::vector<int64_t> g0;
+    std::vector<int32_t> len;
+    for (int i = 1; i <= ni; ++i)
+      for (int j = 1; j <= nj; ++j) {
+        const int64_t base = ((int64_t)i * PJ + j) * PK;
+        int k0 = -1, k1 = -1;
+        for (int k = 1; k <= nk; ++k)
+          if (lab[base + k] != 0) {
+            if (k0 < 0) k0 = k;
+            k1 = k;
+          }
+        if (k0 >= 0) {
+          g0.push_back(base + k0);
+          len.push_back(k1 - k0 + 1);
+        }
+      }
+    a.n_lines = (int32_t)g0.size();
+
+    TT_TRY(tup(h, (int64_t**)&a.line_g0, g0.data(), g0.size(), s));
+    TT_TRY(tup(h, (int32_t**)&a.line_len, len.data(), len.size(), s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));  // g0 / len are stack temporaries
+  }
   // heart sources: segments of heart voxels per receiving row
   SrcArgs& sa = h->s;
   sa.n_heart = d->n_heart;
@@ -596,9 +690,9 @@ extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; 
 
 static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
   for (int q = 0; q < n; ++q) {
-    pcg_p_update<<<h->nblk, TB, 0, s>>>(h->a);
-    pcg_ap<<<h->nblk, TB, 0, s>>>(h->a);
-    pcg_k2<<<h->nblk, TB, 0, s>>>(h->a);
+    pcg_p_update<<<h->nblk_k[0], TB, 0, s>>>(h->a);
+    pcg_ap<<<h->nblk_k[1], TB, 0, s>>>(h->a);
+    pcg_k2<<<h->nblk_k[2], TB, 0, s>>>(h->a);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
