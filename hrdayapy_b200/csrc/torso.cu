@@ -67,7 +67,11 @@ struct TorsoArgs {
   int32_t n_lines;
   const int64_t* line_g0;
   const int32_t* line_len;
+  // label | LAB_UNIFORM when all six neighbours carry the cell's own label
+  const uint8_t* label_u;
 };
+
+constexpr int LAB_UNIFORM = 0x80;
 
 __constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
 __constant__ double c_T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
@@ -207,15 +211,17 @@ __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
 // tissue line; all thirteen loads of a cell are issued before the sums
 // (32-bit neighbour offsets keep the addressing to one base per array).
 // The conductance table sits in shared memory (its reads diverge across a
-// warp at material boundaries).  A shared-memory 2.5-D blocked variant
-// (8 x 32 columns marching in i) measured slower on B200: it is
-// latency-bound at one plane in flight per block.
+// warp at material boundaries).  Measured and dropped on B200 (full torso,
+// 5.8 M rows): a shared-memory 2.5-D blocked variant (8 x 32 columns
+// marching 16 planes in i, 53-56 us against 37 us here: latency-bound at one
+// plane in flight per block), two cells per thread (76 registers, 52 us) and
+// a summed-difference path for uniform cells (40 us).
 __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
   for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
   __syncthreads();
-  const uint8_t* __restrict__ lab = a.label;
+  const uint8_t* __restrict__ lab = a.label_u;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
   const int sj = a.pk, si = a.pj * a.pk;   // the padded plane fits in 32 bits
@@ -231,14 +237,18 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
       const uint8_t* __restrict__ lc = lab + g;
       const float* __restrict__ pc = p + g;
       const int off[6] = {si, -si, sj, -sj, 1, -1};
-      const int l = lc[0];
+      const int lf = lc[0];
+      const int l = lf & (LAB_UNIFORM - 1);
       const float pg = pc[0];
-      int ln[6];
       float pn[6];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        ln[f] = lc[off[f]];
-        pn[f] = pc[off[f]];
+      for (int f = 0; f < 6; ++f) pn[f] = pc[off[f]];
+      // inside a material region every face has the same conductance: the
+      // neighbours' labels are read only at material boundaries
+      int ln[6] = {l, l, l, l, l, l};
+      if (!(lf & LAB_UNIFORM)) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) ln[f] = lc[off[f]] & (LAB_UNIFORM - 1);
       }
       float ap = 0.0f;
 #pragma unroll
@@ -617,6 +627,15 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
         }
       }
     a.n_lines = (int32_t)g0.size();
+    std::vector<uint8_t> lab_u(lab);
+    for (int64_t r = 0; r < n_rows; ++r) {
+      const int64_t g = grid_of_row[r];
+      const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
+      bool uni = true;
+      for (int f = 0; f < 6; ++f) uni = uni && lab[nb[f]] == lab[g];
+      if (uni) lab_u[g] |= (uint8_t)LAB_UNIFORM;
+    }
+    TT_TRY(tup(h, (uint8_t**)&a.label_u, lab_u.data(), lab_u.size(), s));
 
     TT_TRY(tup(h, (int64_t**)&a.line_g0, g0.data(), g0.size(), s));
     TT_TRY(tup(h, (int32_t**)&a.line_len, len.data(), len.size(), s));
