@@ -321,19 +321,27 @@ def run_torso(args):
             pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=5)
             pc.train(fr[0:8].contiguous(), ks=tuple(range(0, 64, 8)), repeats=1, lr=1e-3)
         solver.reset()
-        its, ms = [], []
+        its, ms, rst = [], [], []
         for f in range(8, n_fr):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
             if name == "plain_pcg":
                 _, st = solver.solve_frame(fr[f], 1e-6, "rel", 50000)
             else:
-                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 300, use_net=(name == "learned_fcg"))
+                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 300,
+                                       use_net=args.net_every if name == "learned_fcg" else 0)
             torch.cuda.synchronize()
             if f >= 8 + 1 + args.warmup:
                 ms.append((time.perf_counter() - t1) * 1e3)
                 its.append(int(st.iterations))
+                rst.append(int(st.restarts))
         out[name] = {"ms_per_frame": float(np.mean(ms)), "iterations": its}
+        if name != "plain_pcg":
+            # +100: the network run fell back to the two-level method; +1000:
+            # plain PCG finished the frame; below 100: true-residual restarts
+            out[name]["restarts"] = rst
+        if name == "learned_fcg":
+            out[name]["network_every"] = args.net_every
     rows = solver.n_rows
     if pc is not None:
         pc.close()
@@ -452,7 +460,7 @@ def run_ours(args):
         if args.theta:
             line["theta_scheme"] = theta_leg(prob)
         if args.torso:
-            line["torso"] = torso_leg(prob)
+            line["torso"] = torso_leg(prob, net_every=args.net_every)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -495,7 +503,7 @@ def theta_leg(prob, n_steps=100, warm=20, theta=0.5, cg_tol=1e-5):
             "vm_finite": bool(np.isfinite(vm).all())}
 
 
-def torso_leg(prob, n_train=8, n_test=5):
+def torso_leg(prob, n_train=8, n_test=5, net_every=1):
     """Torso forward solve (192 x 160 x 256 voxels at 1.5 mm, lungs, blood
     pools, the biventricular shell embedded; 12-lead + 16 x 16 read-out) on
     Vm frames simulated here by the fused monodomain step (1 ms apart).  The
@@ -547,7 +555,7 @@ def torso_leg(prob, n_train=8, n_test=5):
     for name in ("plain_pcg", "two_level_fcg", "learned_fcg"):
         solver.reset()
         solver.solve_frame(frames[test0], 1e-6, "rel", 50000)
-        its, ms, rel = [], [], []
+        its, ms, rel, rst = [], [], [], []
         for f in range(test0 + 1, test0 + 1 + n_test):
             torch.cuda.synchronize()
             t1 = time.perf_counter()
@@ -555,13 +563,18 @@ def torso_leg(prob, n_train=8, n_test=5):
                 _, st = solver.solve_frame(frames[f], 1e-6, "rel", 50000)
             else:
                 _, st = pc.solve_frame(frames[f], 1e-6, 50000, 300,
-                                       use_net=(name == "learned_fcg"))
+                                       use_net=net_every if name == "learned_fcg" else 0)
             torch.cuda.synchronize()
             ms.append((time.perf_counter() - t1) * 1e3)
             its.append(int(st.iterations))
             rel.append(float(st.rel_residual))
+            rst.append(int(st.restarts))
         out[name] = {"ms_per_frame": float(np.mean(ms)), "iterations": its,
                      "max_rel_residual": max(rel)}
+        if name != "plain_pcg":
+            out[name]["restarts"] = rst     # +100 network fallback, +1000 plain PCG
+        if name == "learned_fcg":
+            out[name]["network_every"] = net_every
     n_rows = solver.n_rows
     ag, nc = pc.coarse_info()
     pc.close()
@@ -685,6 +698,8 @@ def main():
                     help="torso voxels for --workload torso (extent fixed at 288 x 240 x 384 mm)")
     ap.add_argument("--torso-solvers", default="plain_pcg,two_level_fcg,learned_fcg",
                     help="torso workload: solvers to time (the last one is the headline)")
+    ap.add_argument("--net-every", type=int, default=1, choices=[1, 2, 4],
+                    help="learned FCG: the network term on every k-th iteration")
     ap.add_argument("--no-theta", dest="theta", action="store_false",
                     help="skip the theta = 0.5 (Crank-Nicolson) leg")
     ap.add_argument("--no-torso", dest="torso", action="store_false",

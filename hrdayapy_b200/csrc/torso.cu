@@ -216,11 +216,11 @@ __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
 // marching 16 planes in i, 53-56 us against 37 us here: latency-bound at one
 // plane in flight per block), two cells per thread (76 registers, 52 us) and
 // a summed-difference path for uniform cells (40 us).
-__global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
-  __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
-  if (a.iscal[IS_DONE]) return;
-  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
-  __syncthreads();
+// Line SpMV core shared by the PCG and flexible-CG passes: Ap = A p over the
+// tissue lines (Ap = 0 on air and at the pin), calling cell(g, p_g, Ap_g)
+// for every cell; T is the conductance table in shared memory.
+template <class Cell>
+__device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, Cell&& cell) {
   const uint8_t* __restrict__ lab = a.label_u;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
@@ -228,7 +228,6 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
   const int64_t pin = a.pin;
   const int lane = threadIdx.x & 31;
   const int n_warps = gridDim.x * (TB / 32);
-  double acc[1] = {0.0};
   for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
     const int64_t g0 = a.line_g0[L];
     const int len = a.line_len[L];
@@ -255,9 +254,18 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
       for (int f = 0; f < 6; ++f) ap += T[l * HP_MAX_MATERIALS + ln[f]] * (pg - pn[f]);
       if (l == 0 || g == pin) ap = 0.0f;
       Ap[g] = ap;
-      acc[0] += (double)pg * (double)ap;
+      cell(g, pg, ap);
     }
   }
+}
+
+__global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
+  __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
+  if (a.iscal[IS_DONE]) return;
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
+  __syncthreads();
+  double acc[1] = {0.0};
+  spmv_lines(a, T, [&](int64_t, float pg, float ap) { acc[0] += (double)pg * (double)ap; });
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double pAp = tot[0];
@@ -436,15 +444,25 @@ __global__ void gather_rows_f(const float* b, const int64_t* grid_of_row, int64_
   if (q < n) out[q] = b[grid_of_row[q]];
 }
 
+// flexible-CG passes (defined with the FCG driver below)
+__global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a);
+__global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a);
+__global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a);
+__global__ void __launch_bounds__(TB) fcg_p(TorsoArgs a, int first);
+
 }  // namespace hp
 
 using namespace hp;
+
+// kernels that stride over the tissue lines, in the order of HpTorso::nblk_k
+enum LineKernel : int { K_P_UPDATE = 0, K_AP, K_K2, K_FCG_SPMV, K_FCG_UPDATE, K_FCG_BETA, K_FCG_P,
+                        N_LINE_KERNELS };
 
 struct HpTorso {
   TorsoArgs a;
   SrcArgs s;
   int nblk;
-  int nblk_k[3];  // PCG iteration kernels: each one's resident grid
+  int nblk_k[N_LINE_KERNELS];  // line kernels: each one's resident grid
   int ni, nj, nk;
   int64_t n_rows;
   std::vector<void*> allocs;
@@ -463,7 +481,7 @@ struct HpTorso {
   int parity;
   bool have_x;
   cudaGraphExec_t graph[2];
-  cudaGraphExec_t fcg_graph[2];   // FCG chunk without / with the network
+  cudaGraphExec_t fcg_graph[4];   // FCG chunk without the network / net every 1, 2, 4
   const void* fcg_graph_pc;       // preconditioner handle the FCG graphs hold
   cudaStream_t fcg_graph_stream;
   int graph_chunk;
@@ -558,7 +576,7 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   h->graph[0] = h->graph[1] = nullptr;
   h->graph_chunk = 0;
   h->graph_stream = nullptr;
-  h->fcg_graph[0] = h->fcg_graph[1] = nullptr;
+  for (int k = 0; k < 4; ++k) h->fcg_graph[k] = nullptr;
   h->fcg_graph_pc = nullptr;
   h->fcg_graph_stream = nullptr;
   h->ni = ni; h->nj = nj; h->nk = nk;
@@ -594,8 +612,11 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     // the line loops stride over the grid, so a grid larger than what is
     // resident would leave a tail wave: each kernel gets its resident grid
     int o = 0;
-    const void* fs[3] = {(const void*)pcg_p_update, (const void*)pcg_ap, (const void*)pcg_k2};
-    for (int q = 0; q < 3; ++q) {
+    const void* fs[N_LINE_KERNELS] = {(const void*)pcg_p_update, (const void*)pcg_ap,
+                                      (const void*)pcg_k2,       (const void*)fcg_spmv,
+                                      (const void*)fcg_update,   (const void*)fcg_beta,
+                                      (const void*)fcg_p};
+    for (int q = 0; q < N_LINE_KERNELS; ++q) {
       HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fs[q], TB, 0));
       h->nblk_k[q] = nsm * std::min(8, std::max(o, 1));
     }
@@ -709,9 +730,9 @@ extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; 
 
 static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
   for (int q = 0; q < n; ++q) {
-    pcg_p_update<<<h->nblk_k[0], TB, 0, s>>>(h->a);
-    pcg_ap<<<h->nblk_k[1], TB, 0, s>>>(h->a);
-    pcg_k2<<<h->nblk_k[2], TB, 0, s>>>(h->a);
+    pcg_p_update<<<h->nblk_k[K_P_UPDATE], TB, 0, s>>>(h->a);
+    pcg_ap<<<h->nblk_k[K_AP], TB, 0, s>>>(h->a);
+    pcg_k2<<<h->nblk_k[K_K2], TB, 0, s>>>(h->a);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -918,26 +939,20 @@ hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, c
                         float* z, int use_net, cudaStream_t s);
 }
 
-// q = A p (p in p0), partial p.q and p.r; last block: alpha = p.r / p.q
+// q = A p (p in p0), partial p.q and p.r; last block: alpha = p.r / p.q.
+// The flexible-CG passes walk the tissue lines like the PCG ones (the
+// preconditioner output z is zero on air and at the pin as well).
 __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
+  __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
-  const int64_t SJ = a.pk, SI = (int64_t)a.pj * a.pk;
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
+  __syncthreads();
+  const float* __restrict__ rv = a.r;
   double acc[2] = {0.0, 0.0};
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < a.ng; g += (int64_t)gridDim.x * TB) {
-    const int l = a.label[g];
-    if (l == 0 || g == a.pin) continue;
-    const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-    const float pv = a.p0[g];
-    float q = 0.0f;   // face-flux form, as in pcg_k1
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      const float t = c_T32[l * HP_MAX_MATERIALS + a.label[nb[f]]];
-      q += t * (pv - a.p0[nb[f]]);
-    }
-    a.Ap[g] = q;
+  spmv_lines(a, T, [&](int64_t g, float pv, float q) {
     acc[0] += (double)pv * q;
-    acc[1] += (double)pv * a.r[g];
-  }
+    acc[1] += (double)pv * rv[g];
+  });
   double tot[2];
   if (block_reduce_last<2>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_PAP] = tot[0];
@@ -957,21 +972,26 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float af = (float)alpha;
-  const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ p = a.p0;
   const float* __restrict__ Ap = a.Ap;
   float* __restrict__ rv = a.r;
   double* __restrict__ x = a.x;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[1] = {0.0};
-#pragma unroll 4
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride) {
-    if (lab[g] == 0 || g == pin) continue;
-    x[g] += alpha * (double)p[g];
-    const float r = rv[g] - af * Ap[g];
-    rv[g] = r;
-    acc[0] += (double)r * r;
-  }
+  constexpr int LB = 4;
+  float pb[LB], rb[LB];
+  double xb[LB];
+  for_line_batches<LB>(
+      a,
+      [&](int u, int64_t g) {
+        pb[u] = p[g];
+        xb[u] = x[g];
+        rb[u] = rv[g] - af * Ap[g];
+      },
+      [&](int u, int64_t g) {
+        x[g] = xb[u] + alpha * (double)pb[u];
+        rv[g] = rb[u];
+        acc[0] += (double)rb[u] * rb[u];
+      });
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_RR] = tot[0];
@@ -990,14 +1010,14 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
 
 // partial z.q (z in p1); last block: beta = -z.q / p.q
 __global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a) {
-  const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ z = a.p1;
   const float* __restrict__ Ap = a.Ap;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
   double acc[1] = {0.0};
-#pragma unroll 4
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride)
-    if (lab[g] != 0 && g != pin) acc[0] += (double)z[g] * Ap[g];
+  constexpr int LB = 8;
+  float zb[LB], qb[LB];
+  for_line_batches<LB>(
+      a, [&](int u, int64_t g) { zb[u] = z[g]; qb[u] = Ap[g]; },
+      [&](int u, int64_t) { acc[0] += (double)zb[u] * qb[u]; });
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0)
     a.scal[SC_BETA] = -tot[0] / a.scal[SC_PAP];
@@ -1006,13 +1026,13 @@ __global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a) {
 // p = z + beta p
 __global__ void __launch_bounds__(TB) fcg_p(TorsoArgs a, int first) {
   const float beta = first ? 0.0f : (float)a.scal[SC_BETA];
-  const uint8_t* __restrict__ lab = a.label;
   const float* __restrict__ z = a.p1;
   float* __restrict__ p = a.p0;
-  const int64_t pin = a.pin, ng = a.ng, stride = (int64_t)gridDim.x * TB;
-#pragma unroll 4
-  for (int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x; g < ng; g += stride)
-    if (lab[g] != 0 && g != pin) p[g] = z[g] + beta * p[g];
+  constexpr int LB = 8;
+  float zb[LB], pb[LB];
+  for_line_batches<LB>(
+      a, [&](int u, int64_t g) { zb[u] = z[g]; pb[u] = p[g]; },
+      [&](int u, int64_t g) { p[g] = zb[u] + beta * pb[u]; });
 }
 
 __global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, float* __restrict__ e) {
@@ -1024,14 +1044,17 @@ __global__ void error_kernel(TorsoArgs a, const double* __restrict__ xstar, floa
 constexpr int FCG_CHUNK = 4;
 
 // The FCG iteration body (A p, x / r update and stopping tests, z = M(r),
-// beta, p) for FCG_CHUNK iterations, captured once per network setting,
-// stream and preconditioner handle.
+// beta, p) for FCG_CHUNK iterations, captured once per network period,
+// stream and preconditioner handle.  use_net = k > 0 applies the network
+// term on every k-th iteration of the chunk (k divides FCG_CHUNK) and the
+// Jacobi + coarse terms alone on the others: flexible CG admits a
+// preconditioner that changes from one iteration to the next.
 static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s) {
-  const int q = use_net ? 1 : 0;
+  const int q = use_net == 0 ? 0 : (use_net == 1 ? 1 : (use_net == 2 ? 2 : 3));
   if (h->fcg_graph[q] && h->fcg_graph_stream == s && h->fcg_graph_pc == (const void*)p)
     return HP_OK;
   if (h->fcg_graph_stream != s || h->fcg_graph_pc != (const void*)p) {
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 4; ++k)
       if (h->fcg_graph[k]) { cudaGraphExecDestroy(h->fcg_graph[k]); h->fcg_graph[k] = nullptr; }
   }
   TorsoArgs& a = h->a;
@@ -1039,12 +1062,12 @@ static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s
   HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   hp_status st = HP_OK;
   for (int it = 0; it < FCG_CHUNK && st == HP_OK; ++it) {
-    fcg_spmv<<<h->nblk, TB, 0, s>>>(a);
-    fcg_update<<<h->nblk, TB, 0, s>>>(a);
-    st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
+    fcg_spmv<<<h->nblk_k[K_FCG_SPMV], TB, 0, s>>>(a);
+    fcg_update<<<h->nblk_k[K_FCG_UPDATE], TB, 0, s>>>(a);
+    st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net > 0 && it % use_net == 0, s);
     if (st != HP_OK) break;
-    fcg_beta<<<h->nblk, TB, 0, s>>>(a);
-    fcg_p<<<h->nblk, TB, 0, s>>>(a, 0);
+    fcg_beta<<<h->nblk_k[K_FCG_BETA], TB, 0, s>>>(a);
+    fcg_p<<<h->nblk_k[K_FCG_P], TB, 0, s>>>(a, 0);
   }
   cudaError_t ce = cudaStreamEndCapture(s, &g);
   if (st != HP_OK) return st;
@@ -1087,7 +1110,7 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
   // preconditioner initialises lazily, before the capture)
   st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
   if (st != HP_OK) return st;
-  fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
+  fcg_p<<<h->nblk_k[K_FCG_P], TB, 0, s>>>(a, 1);
   st = fcg_graph(h, p, use_net, s);
   if (st != HP_OK) return st;
   bool restart = false;
@@ -1095,10 +1118,10 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
     if (restart) {
       st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net, s);
       if (st != HP_OK) return st;
-      fcg_p<<<h->nblk, TB, 0, s>>>(a, 1);
+      fcg_p<<<h->nblk_k[K_FCG_P], TB, 0, s>>>(a, 1);
       restart = false;
     }
-    HP_CUDA_TRY(cudaGraphLaunch(h->fcg_graph[use_net ? 1 : 0], s));
+    HP_CUDA_TRY(cudaGraphLaunch(h->fcg_graph[use_net == 0 ? 0 : (use_net == 1 ? 1 : (use_net == 2 ? 2 : 3))], s));
     st = read_scalars(h, s);
     if (st != HP_OK) return st;
     it = h->h_iscal[IS_ITER];
@@ -1136,14 +1159,15 @@ static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, i
   double rel = 0.0;
   bool fallback = false;
   hp_status result = HP_OK;
-  for (int net = use_net ? 1 : 0; net >= 0; --net) {
+  // the run with the network (use_net = its period), then without it
+  for (int net = use_net; net >= 0; net = net > 0 ? 0 : -1) {
     int it = 0;
     const int budget = std::max(1, std::min(fallback_iter, max_iter - it_total));
     hp_status st = fcg_run(h, p, tol, budget, net, &it, &restarts, &rel, &fallback, s);
     if (st != HP_OK) return st;
     it_total += it;
     if (!fallback) break;
-    if (net == 1) restarts += 100;
+    if (net > 0) restarts += 100;
   }
   if (fallback) {
     HpSolveStats st2;
@@ -1175,6 +1199,8 @@ extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const fl
                                               HpSolveStats* stats, void* stream) {
   HP_REQUIRE(h && p, "hp_torso_solve_frame_fcg: null handle");
   HP_REQUIRE(max_iter >= 1 && fallback_iter >= 1, "hp_torso_solve_frame_fcg: bad iteration limits");
+  HP_REQUIRE(use_net == 0 || use_net == 1 || use_net == 2 || use_net == 4,
+             "hp_torso_solve_frame_fcg: use_net must be 0, 1, 2 or 4");
   HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame_fcg: tol must be positive");
   cudaStream_t s = (cudaStream_t)stream;
   hp_status st = build_rhs(h, vm, vm_on_device, s);
@@ -1274,10 +1300,10 @@ extern "C" hp_status hp_torso_reset(HpTorso* h) {
 
 extern "C" hp_status hp_torso_destroy(HpTorso* h) {
   if (!h) return HP_OK;
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < 2; ++q)
     if (h->graph[q]) cudaGraphExecDestroy(h->graph[q]);
+  for (int q = 0; q < 4; ++q)
     if (h->fcg_graph[q]) cudaGraphExecDestroy(h->fcg_graph[q]);
-  }
   for (void* p : h->allocs) cudaFree(p);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->h_iscal) cudaFreeHost(h->h_iscal);

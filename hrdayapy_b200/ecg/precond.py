@@ -132,7 +132,12 @@ class LearnedPreconditioner:
     def solve_frame(self, vm, tol=1e-6, max_iter=5000, fallback_iter=200, out=None,
                     use_net=True):
         """One frame by flexible CG with M (use_net=False: without the
-        network); plain Jacobi-PCG finishes it past fallback_iter."""
+        network; an integer k in {1, 2, 4}: the network term on every k-th
+        iteration, True = 1); plain Jacobi-PCG finishes it past
+        fallback_iter."""
+        use_net = int(use_net)
+        if use_net not in (0, 1, 2, 4):
+            raise ValueError("use_net must be False, True or a period in {1, 2, 4}")
         s = self.solver
         st = _lib.HpSolveStats()
         on_dev = 0

@@ -388,7 +388,9 @@ hp_status hp_torso_arrays(HpTorso *h, HpTorsoArrays *out);
 
 /* Flexible CG with the learned preconditioner for one frame, judged by the
  * same FP64 true relative residual <= tol.  use_net = 0 runs the same
- * solver without the network (Jacobi + coarse level).  If a run with the
+ * solver without the network (Jacobi + coarse level); use_net = k in
+ * {1, 2, 4} adds the network term on every k-th iteration (flexible CG
+ * admits a preconditioner that varies between iterations).  If a run with the
  * network has not converged after fallback_iter iterations, stagnates or
  * breaks down, FCG restarts from the current iterate without the network
  * (stats->restarts += 100); if that fails as well, plain Jacobi-PCG
