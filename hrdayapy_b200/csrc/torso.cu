@@ -42,7 +42,8 @@ enum Scal : int {
   SC_TRUE_RR, SC_SRC_MEAN, SC_STAT, SC_TOL, SC_HIST0, N_SCAL = SC_HIST0 + 8
 };
 enum IScal : int {
-  IS_DONE = 0, IS_ITER, IS_RULE, IS_MAXIT, IS_BREAKDOWN, IS_NONFINITE, IS_STAGNANT, IS_NH, N_ISCAL
+  IS_DONE = 0, IS_ITER, IS_RULE, IS_MAXIT, IS_BREAKDOWN, IS_NONFINITE, IS_STAGNANT, IS_NH,
+  IS_STAG_ON, N_ISCAL
 };
 
 struct TorsoArgs {
@@ -1001,7 +1002,8 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
     // stagnation: less than 3 % progress over the last 5 iterations
     const int nh = ++a.iscal[IS_NH];
     a.scal[SC_HIST0 + (nh - 1) % 8] = stat;
-    const bool stagnant = nh > 6 && stat > 0.97 * a.scal[SC_HIST0 + (nh - 6) % 8];
+    const bool stagnant =
+        a.iscal[IS_STAG_ON] && nh > 6 && stat > 0.97 * a.scal[SC_HIST0 + (nh - 6) % 8];
     if (!isfinite(tot[0])) { a.iscal[IS_NONFINITE] = 1; a.iscal[IS_DONE] = 1; }
     else if (stat < 0.5 * a.scal[SC_TOL] || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
     else if (stagnant) { a.iscal[IS_STAGNANT] = 1; a.iscal[IS_DONE] = 1; }
@@ -1088,7 +1090,10 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
   TorsoArgs& a = h->a;
   *fallback = false;
   HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &tol, 8, cudaMemcpyHostToDevice, s));
+  // the stagnation test guards the runs with the network; the method
+  // without it runs until convergence or the iteration budget
   int32_t is_init[N_ISCAL] = {0, 0, HP_STOP_REL, fallback_iter, 0, 0};
+  is_init[IS_STAG_ON] = use_net ? 1 : 0;
   HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_init, sizeof(is_init), cudaMemcpyHostToDevice, s));
   true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
   HP_CUDA_TRY(cudaGetLastError());
@@ -1139,6 +1144,7 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
       if (rel <= tol) break;
       ++*restarts_out;
       int32_t is_re[N_ISCAL] = {0, it, HP_STOP_REL, fallback_iter, 0, 0};
+      is_re[IS_STAG_ON] = use_net ? 1 : 0;
       HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_re, sizeof(is_re), cudaMemcpyHostToDevice, s));
       restart = true;
     }
@@ -1151,8 +1157,9 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
 // Flexible CG with the learned preconditioner.  Safeguards, in order: when
 // the run with the network fails (no convergence within fallback_iter,
 // stagnation or breakdown), FCG restarts from the current iterate without
-// the network (the two-level method, restarts += 100); when that fails too,
-// plain Jacobi-PCG finishes the frame (restarts += 1000).
+// the network (the two-level method, restarts += 100; no stagnation test);
+// when that fails too, plain Jacobi-PCG finishes the frame (restarts +=
+// 1000).
 static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
                            int use_net, HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
   int it_total = 0, restarts = 0;
