@@ -430,8 +430,11 @@ def run_ours(args):
     achieved = n_vox * bpv / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
 
-    # end to end through the C-ABI handle: host buffers in, Vm frames out
-    e2e = e2e_run(prob, args, fs)
+    # end to end through the C-ABI handle: host buffers in, Vm frames out;
+    # three repetitions, the median reported (the first one also pays
+    # first-use costs of the process: pinned buffers, module loads)
+    reps = sorted((e2e_run(prob, args, fs) for _ in range(3)), key=lambda r: r["value"])
+    e2e = dict(reps[1], repetitions=[r["value"] for r in reps])
     if rank == 0:
         line = {
             "metric": "monodomain voxel-steps/s", "value": value, "unit": "voxel-steps/s",
@@ -614,15 +617,18 @@ def e2e_run(prob, args, fs):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim = M.MonoHandle(p2)
+    t1 = time.perf_counter()
     for f in range(k):
         sim.run(fs, graph_chunk=fs)
         sim.vm_frames(f, 1, out=out[f].numpy())
     torch.cuda.synchronize()
-    dt_s = time.perf_counter() - t0
+    t2 = time.perf_counter()
+    dt_s = t2 - t0
     sim.close()
     return {"value": p2.n_myo * fs * k / dt_s, "unit": "voxel-steps/s",
             "h2d_bytes_per_step": int(h2d // k), "d2h_bytes_per_step": int(p2.n_myo * 4),
-            "steps": k, "includes": "hp_mono_create upload + run + per-frame Vm D2H"}
+            "steps": k, "includes": "hp_mono_create upload + run + per-frame Vm D2H",
+            "create_s": t1 - t0, "run_and_d2h_s": t2 - t1}
 
 
 def cpu_baseline(prob, info, args, budget_s=15.0):

@@ -78,3 +78,38 @@ def test_ensemble_matches_separate_runs(kernel):
     pb.variant_gkr = None
     vm_u, _, _ = run(pb)
     assert np.abs(ens.split(vm_e)[1] - vm_u).max() > 0.1
+
+
+@pytest.mark.gpu
+def test_theta_scheme_ensemble_matches_separate_runs():
+    """At theta = 0.5 the ensemble's CG solves all variants together (one
+    set of CG scalars), so variants are not bit-identical to separate runs,
+    but every variant stays within the parity tolerances of its own run."""
+    import dataclasses
+    from hrdayapy_b200 import monodomain as M
+    from hrdayapy_b200.ensemble import build_ensemble
+    pa = _variant(11, (28, 24, 18), 20.0)
+    pb = _variant(12, (24, 20, 16), 20.0)
+    cn = dict(theta=0.5, cn_tol=1e-6, cn_max_iter=100)
+    pa, pb = dataclasses.replace(pa, **cn), dataclasses.replace(pb, **cn)
+    ens = build_ensemble([pa, pb])
+
+    def run(p):
+        sim = M.MonoHandle(p)
+        sim.run(p.n_steps, graph_chunk=16)
+        vm = sim.vm_frames()
+        a, na, d, nd = sim.events()
+        _, _, unconv, brk = sim.cn_stats()
+        sim.close()
+        assert unconv == 0 and brk == 0
+        return vm, a[0]
+
+    vm_e, act_e = run(ens.problem)
+    for v, p in enumerate((pa, pb)):
+        vm_s, act_s = run(p)
+        ve = ens.split(vm_e)[v]
+        assert np.sqrt(np.mean((ve.astype(np.float64) - vm_s) ** 2)) <= 0.5
+        ae = ens.split(act_e)[v]
+        ok = np.isfinite(act_s)
+        assert (np.isfinite(ae) == ok).all()
+        assert np.max(np.abs(ae[ok] - act_s[ok])) <= 0.1
