@@ -50,7 +50,10 @@ def _run(D, H, W, cin, cout, epi, seed=0):
     return y, ref
 
 
-@pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (64, 64), (96, 32), (48, 16)])
+# (16, 16), (16, 32), (48, 16), (32, 32) run row-blocked CTAs, the others one
+# line per CTA; H = 5 leaves a partial block of output lines
+@pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32),
+                                      (48, 16)])
 def test_conv_forward(cin, cout):
     y, ref = _run(3, 5, 256, cin, cout, epi=1)
     scale = ref.abs().max().item()
