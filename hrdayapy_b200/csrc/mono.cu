@@ -93,6 +93,8 @@ struct MonoArgs {
   // at n_active_pad (n_active rounded up to a warp); slot >> bv_shift = brick
   int32_t n_active, n_active_pad, bv_shift;
   const int32_t* active_slot;
+  // theta-scheme: the CG solution x ([slots | Purkinje]) of the step
+  const float* cn_x;
 };
 
 // TTP06 phenotype table (ttp06_phenotype_constants.py:54-61), index = pheno-1.
@@ -978,16 +980,35 @@ constexpr int ION_THREADS = 128;
 // i of active_slot, not the slot), so the ionic half's state loads and
 // stores are fully coalesced; tag, V and W stay per slot for the stencil.
 // mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
-__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off,
-                                                                   int mode) {
+// mode 0: the ionic half of step i+1 on V_{i+1} = Vpost; mode 1: the
+// prologue, the ionic half of step 0 on V_0 into W_0; mode 2: the end of a
+// theta-scheme step, V_{i+1} = clamp(x) with the outputs of step i recorded
+// exactly as the explicit step records them, then the ionic half of step
+// i+1 on it.
+template <int mode>
+__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+  __shared__ int64_t s_vm_frame, s_anim_frame;
   const int64_t step = *a.d_step + step_off;
+  if constexpr (mode == 2) {
+    if (threadIdx.x == 0) {
+      s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
+      s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
+    }
+    __syncthreads();
+  }
   const bool odd = step & 1;
-  const int64_t istep = mode ? 0 : step + 1;
+  const int64_t istep = mode == 1 ? 0 : step + 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < a.n_active) {
     const int64_t slot = a.active_slot[i];
     const uint32_t tag = a.tag[slot];
-    const float Vn = a.Vpost[slot];
+    float Vn;
+    if constexpr (mode == 2) {
+      Vn = fminf(fmaxf(a.cn_x[slot], -150.0f), 80.0f);
+      voxel_outputs(a, slot, tag, Vn, a.Vpost[slot], step, s_vm_frame, s_anim_frame);
+    } else {
+      Vn = a.Vpost[slot];
+    }
     const int64_t na = a.n_active;
     CellState cs;
 #pragma unroll
@@ -998,12 +1019,21 @@ __global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, 
 #pragma unroll
     for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
     const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
-    float* __restrict__ Wout = mode ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
+    float* __restrict__ Wout = mode == 1 ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
     Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
   } else {
     const int p = i - a.n_active_pad;
-    if (p >= 0 && p < a.n_pk)
-      purkinje_ionic(a, p, a.pk_Vpost[p], istep, mode ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
+    if (p >= 0 && p < a.n_pk) {
+      float Vn;
+      if constexpr (mode == 2) {
+        Vn = fminf(fmaxf(a.cn_x[a.n_slots + p], -150.0f), 80.0f);
+        a.pk_Vpost[p] = Vn;
+        if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p] = Vn;
+      } else {
+        Vn = a.pk_Vpost[p];
+      }
+      purkinje_ionic(a, p, Vn, istep, mode == 1 ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
+    }
   }
 }
 
@@ -1148,32 +1178,6 @@ __global__ void __launch_bounds__(CN_TB) cn_dir_kernel(CnArgs c) {
   for (int64_t e = blockIdx.x * (int64_t)CN_TB + threadIdx.x; e < c.n;
        e += (int64_t)gridDim.x * CN_TB)
     c.p[e] = c.dinv[e] * c.r[e] + beta * c.p[e];
-}
-
-// End of the CN diffusion half: V_{i+1} = clamp(x), then the outputs of step
-// i exactly as the explicit step records them (threads as the ionic launch:
-// compact tissue list, then Purkinje nodes from n_active_pad).
-__global__ void __launch_bounds__(ION_THREADS) cn_finish_kernel(MonoArgs a, CnArgs c) {
-  __shared__ int64_t s_vm_frame, s_anim_frame;
-  const int64_t step = *a.d_step;
-  if (threadIdx.x == 0) {
-    s_vm_frame = (a.vm_every > 0 && step % a.vm_every == 0) ? step / a.vm_every : -1;
-    s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
-  }
-  __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < a.n_active) {
-    const int64_t slot = a.active_slot[i];
-    const float Vn = fminf(fmaxf(c.x[slot], -150.0f), 80.0f);
-    voxel_outputs(a, slot, a.tag[slot], Vn, a.Vpost[slot], step, s_vm_frame, s_anim_frame);
-  } else {
-    const int p = i - a.n_active_pad;
-    if (p >= 0 && p < a.n_pk) {
-      const float Vn = fminf(fmaxf(c.x[a.n_slots + p], -150.0f), 80.0f);
-      a.pk_Vpost[p] = Vn;
-      if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p] = Vn;
-    }
-  }
 }
 
 // Loop condition of a solve captured in a CUDA graph (a conditional WHILE
@@ -1365,9 +1369,9 @@ static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) 
   if (grid == 0) return HP_OK;
   if (mode == 0 && h->diff) {
     h->diff<<<h->diff_grid, h->bv, h->diff_smem, s>>>(h->a, step_off);
-    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off, 0);
+    if (h->ion_grid > 0) mono_ionic_kernel<0><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
   } else if (mode == 1 && h->diff) {
-    if (h->ion_grid > 0) mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off, 1);
+    if (h->ion_grid > 0) mono_ionic_kernel<1><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
   } else if (mode == 0 && h->pipe)
     h->pipe<<<h->pipe_grid, h->bv, h->pipe_smem, s>>>(h->a, step_off);
   else
@@ -1517,6 +1521,7 @@ static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, 
   // padding entries of the CG vectors stay zero (the passes skip them)
   for (float* v : {c.x, c.r, c.p, c.q}) HP_CUDA_TRY(cudaMemsetAsync(v, 0, n * sizeof(float), s));
   HP_CUDA_TRY(cudaMallocHost((void**)&h->cn_host, 2 * sizeof(int32_t)));
+  h->a.cn_x = c.x;
   HP_CUDA_TRY(cudaStreamCreateWithFlags(&h->cn_body_stream, cudaStreamNonBlocking));
   h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 2);
   HP_CUDA_TRY(cudaGetLastError());
@@ -1535,7 +1540,8 @@ static void cn_iteration(HpMono* h, cudaStream_t s) {
 
 // One theta-scheme step: the stencil pass that starts the solve, CG
 // iterations in chunks (sized by the previous step's count) until the done
-// flag, the outputs of V_{i+1} = clamp(x), the ionic half and the step count.
+// flag, the outputs of V_{i+1} = clamp(x) with the ionic half (one launch)
+// and the step count.
 static hp_status cn_step(HpMono* h, cudaStream_t s) {
   const CnArgs& c = h->cn_a;
   h->cn_start<<<h->cn_pgrid, h->bv, h->diff_smem, s>>>(h->a, c);
@@ -1553,10 +1559,7 @@ static hp_status cn_step(HpMono* h, cudaStream_t s) {
   }
   // next step: enqueue this step's count (+1) before the first test
   h->cn_chunk = std::max(1, std::min(h->cn_host[1] + 1, 64));
-  if (h->ion_grid > 0) {
-    cn_finish_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, c);
-    mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0, 0);
-  }
+  if (h->ion_grid > 0) mono_ionic_kernel<2><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0);
   advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, 1);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -1595,10 +1598,7 @@ static hp_status cn_capture_steps(HpMono* h, int n, cudaStream_t s) {
     cudaGraph_t bo = nullptr;
     HP_CUDA_TRY(cudaStreamEndCapture(sb, &bo));
     HP_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-    if (h->ion_grid > 0) {
-      cn_finish_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, c);
-      mono_ionic_kernel<<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0, 0);
-    }
+    if (h->ion_grid > 0) mono_ionic_kernel<2><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, 0);
     advance_kernel<<<1, 1, 0, s>>>((int64_t*)h->a.d_step, 1);
     HP_CUDA_TRY(cudaGetLastError());
   }
