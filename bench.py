@@ -430,6 +430,16 @@ def run_ours(args):
     achieved = n_vox * bpv / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
 
+    # DRAM bytes of one time step from the ncu capture of this workload's
+    # split step (both launches; the capture is of 4x4x8 bricks, 19-point)
+    traffic, traffic_note = None, "no ncu capture for this configuration"
+    if (kinfo[0] == 3 and tuple(prob.layout.brick) == (4, 4, 8) and prob.anisotropic
+            and args.workload == "biv_shell"):
+        traffic = 5.0e8
+        traffic_note = ("bytes per time step (dram__bytes_read.sum + dram__bytes_write.sum of "
+                        "mono_diffuse_kernel 132 MB + mono_ionic_kernel 368 MB, one ncu "
+                        "capture, profiles/mono_step_biv_shell.md) vs algorithmic "
+                        f"{bpv * n_vox / 1e6:.0f} MB")
     # end to end through the C-ABI handle: host buffers in, Vm frames out;
     # three repetitions, the median reported (the first one also pays
     # first-use costs of the process: pinned buffers, module loads)
@@ -448,7 +458,8 @@ def run_ours(args):
                        "autotuned": tune_table is not None,
                        "l2": "working set > L2 (no flush)", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_note": traffic_note,
                          "bytes_per_voxel_step": bpv, "peak_source": peak_kind},
             "e2e": e2e,
             "gpu_launches": int(args.steps * fs * (2 if kinfo[0] == 3 else 1) + args.steps),
