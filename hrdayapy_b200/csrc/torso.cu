@@ -220,8 +220,83 @@ __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
 // Line SpMV core shared by the PCG and flexible-CG passes: Ap = A p over the
 // tissue lines (Ap = 0 on air and at the pin), calling cell(g, p_g, Ap_g)
 // for every cell; T is the conductance table in shared memory.
+//
+// Each lane takes two neighbouring cells of its line: the run is widened to
+// start on an even cell (one air cell before the first tissue cell, and at
+// most one after the last), so p, Ap and the labels of the pair move as one
+// 8-byte / 2-byte access at the cell and at its four i / j neighbours (the
+// padded plane and row strides are even), and the +-k neighbours come from
+// the adjacent lanes by shuffles (lanes 0 and 31 load theirs).  Neighbour
+// labels are read only where a cell's six neighbours do not all share its
+// label.  Per-cell arithmetic is the same sum of face fluxes in the same
+// face order as before.
 template <class Cell>
 __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, Cell&& cell) {
+  const uint8_t* __restrict__ lab = a.label_u;
+  const float* __restrict__ p = a.p0;
+  float* __restrict__ Ap = a.Ap;
+  const int sj = a.pk, si = a.pj * a.pk;   // even; the padded plane fits in 32 bits
+  const int64_t pin = a.pin;
+  const int lane = threadIdx.x & 31;
+  const int n_warps = gridDim.x * (TB / 32);
+  constexpr int M = LAB_UNIFORM - 1;
+  for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
+    const int64_t g0 = a.line_g0[L];
+    const int64_t ga = g0 & ~(int64_t)1;                  // even start
+    const int npairs = (int)((g0 + a.line_len[L] - ga + 1) >> 1);
+    for (int q0 = 0; q0 < npairs; q0 += 32) {
+      const int q = q0 + lane;
+      const bool on = q < npairs;
+      const int64_t c = ga + 2 * (int64_t)q;            // first cell of the pair
+      float2 pc = make_float2(0.0f, 0.0f), pip = pc, pim = pc, pjp = pc, pjm = pc;
+      uchar2 lc = make_uchar2(0, 0);
+      if (on) {
+        pc = *(const float2*)(p + c);
+        pip = *(const float2*)(p + c + si);
+        pim = *(const float2*)(p + c - si);
+        pjp = *(const float2*)(p + c + sj);
+        pjm = *(const float2*)(p + c - sj);
+        lc = *(const uchar2*)(lab + c);
+      }
+      // -k of the first cell = second cell of the lane below; +k of the
+      // second cell = first cell of the lane above
+      float km = __shfl_up_sync(0xffffffffu, pc.y, 1);
+      float kp = __shfl_down_sync(0xffffffffu, pc.x, 1);
+      if (on && lane == 0) km = p[c - 1];
+      if (on && lane == 31) kp = p[c + 2];
+      if (!on) continue;
+      const float pv[2] = {pc.x, pc.y};
+      const float pn0[2][6] = {{pip.x, pim.x, pjp.x, pjm.x, pc.y, km},
+                               {pip.y, pim.y, pjp.y, pjm.y, kp, pc.x}};
+      const int lf[2] = {lc.x, lc.y};
+      float ap2[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int l = lf[e] & M;
+        int ln[6] = {l, l, l, l, l, l};
+        if (!(lf[e] & LAB_UNIFORM)) {
+          const uint8_t* __restrict__ le = lab + c + e;
+          const int off[6] = {si, -si, sj, -sj, 1, -1};
+#pragma unroll
+          for (int f = 0; f < 6; ++f) ln[f] = le[off[f]] & M;
+        }
+        float ap = 0.0f;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) ap += T[l * HP_MAX_MATERIALS + ln[f]] * (pv[e] - pn0[e][f]);
+        if (l == 0 || c + e == pin) ap = 0.0f;
+        ap2[e] = ap;
+      }
+      *(float2*)(Ap + c) = make_float2(ap2[0], ap2[1]);
+      cell(c, pv[0], ap2[0]);
+      cell(c + 1, pv[1], ap2[1]);
+    }
+  }
+}
+
+// The same with one cell per lane, for a padded row of odd length (the
+// pair accesses need even strides).
+template <class Cell>
+__device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const float* T, Cell&& cell) {
   const uint8_t* __restrict__ lab = a.label_u;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
@@ -260,13 +335,16 @@ __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, C
   }
 }
 
+template <bool PAIRS>
 __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
   for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
   __syncthreads();
   double acc[1] = {0.0};
-  spmv_lines(a, T, [&](int64_t, float pg, float ap) { acc[0] += (double)pg * (double)ap; });
+  auto cell = [&](int64_t, float pg, float ap) { acc[0] += (double)pg * (double)ap; };
+  if constexpr (PAIRS) spmv_lines(a, T, cell);
+  else spmv_lines_single(a, T, cell);
   double tot[1];
   if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double pAp = tot[0];
@@ -446,6 +524,7 @@ __global__ void gather_rows_f(const float* b, const int64_t* grid_of_row, int64_
 }
 
 // flexible-CG passes (defined with the FCG driver below)
+template <bool PAIRS>
 __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a);
 __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a);
 __global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a);
@@ -464,6 +543,9 @@ struct HpTorso {
   SrcArgs s;
   int nblk;
   int nblk_k[N_LINE_KERNELS];  // line kernels: each one's resident grid
+  bool pairs;                  // stencil on cell pairs (even padded row)
+  void (*ap_fn)(TorsoArgs);
+  void (*fspmv_fn)(TorsoArgs);
   int ni, nj, nk;
   int64_t n_rows;
   std::vector<void*> allocs;
@@ -613,8 +695,12 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     // the line loops stride over the grid, so a grid larger than what is
     // resident would leave a tail wave: each kernel gets its resident grid
     int o = 0;
-    const void* fs[N_LINE_KERNELS] = {(const void*)pcg_p_update, (const void*)pcg_ap,
-                                      (const void*)pcg_k2,       (const void*)fcg_spmv,
+    // cell pairs need even padded strides (an even padded row)
+    h->pairs = (PK % 2) == 0;
+    h->ap_fn = h->pairs ? pcg_ap<true> : pcg_ap<false>;
+    h->fspmv_fn = h->pairs ? fcg_spmv<true> : fcg_spmv<false>;
+    const void* fs[N_LINE_KERNELS] = {(const void*)pcg_p_update, (const void*)h->ap_fn,
+                                      (const void*)pcg_k2,       (const void*)h->fspmv_fn,
                                       (const void*)fcg_update,   (const void*)fcg_beta,
                                       (const void*)fcg_p};
     for (int q = 0; q < N_LINE_KERNELS; ++q) {
@@ -732,7 +818,7 @@ extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; 
 static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
   for (int q = 0; q < n; ++q) {
     pcg_p_update<<<h->nblk_k[K_P_UPDATE], TB, 0, s>>>(h->a);
-    pcg_ap<<<h->nblk_k[K_AP], TB, 0, s>>>(h->a);
+    h->ap_fn<<<h->nblk_k[K_AP], TB, 0, s>>>(h->a);
     pcg_k2<<<h->nblk_k[K_K2], TB, 0, s>>>(h->a);
   }
   HP_CUDA_TRY(cudaGetLastError());
@@ -943,6 +1029,7 @@ hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, c
 // q = A p (p in p0), partial p.q and p.r; last block: alpha = p.r / p.q.
 // The flexible-CG passes walk the tissue lines like the PCG ones (the
 // preconditioner output z is zero on air and at the pin as well).
+template <bool PAIRS>
 __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
@@ -950,10 +1037,12 @@ __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
   __syncthreads();
   const float* __restrict__ rv = a.r;
   double acc[2] = {0.0, 0.0};
-  spmv_lines(a, T, [&](int64_t g, float pv, float q) {
+  auto cell = [&](int64_t g, float pv, float q) {
     acc[0] += (double)pv * q;
     acc[1] += (double)pv * rv[g];
-  });
+  };
+  if constexpr (PAIRS) spmv_lines(a, T, cell);
+  else spmv_lines_single(a, T, cell);
   double tot[2];
   if (block_reduce_last<2>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_PAP] = tot[0];
@@ -1064,7 +1153,7 @@ static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s
   HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   hp_status st = HP_OK;
   for (int it = 0; it < FCG_CHUNK && st == HP_OK; ++it) {
-    fcg_spmv<<<h->nblk_k[K_FCG_SPMV], TB, 0, s>>>(a);
+    h->fspmv_fn<<<h->nblk_k[K_FCG_SPMV], TB, 0, s>>>(a);
     fcg_update<<<h->nblk_k[K_FCG_UPDATE], TB, 0, s>>>(a);
     st = pc::precond_apply(p, a.label, a.invd, a.r, a.p1, use_net > 0 && it % use_net == 0, s);
     if (st != HP_OK) break;
