@@ -159,15 +159,17 @@ conv3_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat16* __
 // -------------------------------------------------------------------------
 // Row-blocked variant: one CTA computes R output lines (h0 .. h0+R-1 at the
 // same (d, w0..w0+127)), one TMEM accumulator of COUT FP32 columns per line.
+// One thread issues the copies up to NS stages ahead, another the products
+// (copy latency no longer serialises with the products' completion).
 // The K loop runs over dz and the R+2 input lines h0-1 .. h0+R of that
 // depth slice: each input line is loaded once and feeds every output line
 // within one row of it (up to three), and the 9 (dy, dx) taps of a depth
 // slice arrive in one bulk copy per slice -- against one line tile per CTA,
 // which loads every input line three times per depth slice and the weights
-// nine times.  Two line stages and two weight buffers (slice zi uses
-// buffer zi & 1; a buffer is rewritten only after the MMAs of every stage
-// that read it have completed, which the line-stage "empty" wait already
-// guarantees because stages complete in order).
+// nine times.  Two weight buffers (slice zi uses buffer zi & 1; a buffer is
+// rewritten only after the MMAs of every stage that read it have completed,
+// which the line-stage "empty" wait already guarantees because stages
+// complete in order).
 template <int CIN, int COUT, int R>
 struct RowsCfg {
   static constexpr int G = CIN / 8;
@@ -176,7 +178,10 @@ struct RowsCfg {
   static constexpr int B_BYTES = 9 * CIN * COUT * 2;
   static constexpr int ACC = (COUT + 31) / 32 * 32;   // TMEM columns per output line
   static constexpr uint32_t COLS = R * ACC <= 32 ? 32 : (R * ACC <= 64 ? 64 : (R * ACC <= 128 ? 128 : (R * ACC <= 256 ? 256 : 512)));
-  static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 128;
+  // line stages in flight: four where that keeps the CTA's shared memory
+  // small (48 KB), else two (more CTAs per SM measured faster there)
+  static constexpr int NS = 4 * A_BYTES + 2 * B_BYTES + 128 <= 48 * 1024 ? 4 : 2;
+  static constexpr int SMEM = NS * A_BYTES + 2 * B_BYTES + 128;
   static constexpr int NSTG = 3 * (R + 2);
   static constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
   static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
@@ -193,23 +198,27 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
                      const __nv_bfloat16* __restrict__ mask, int D, int H, int W, int epi,
                      int* err) {
   using C = RowsCfg<CIN, COUT, R>;
+  constexpr int NS = C::NS;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-  __shared__ __align__(8) uint64_t full[2];
-  __shared__ __align__(8) uint64_t empty[2];
+  __shared__ __align__(8) uint64_t full[NS];
+  __shared__ __align__(8) uint64_t empty[NS];
   __shared__ __align__(8) uint64_t done;
   __shared__ uint32_t tmem_base;
-  __shared__ int failed;
+  __shared__ volatile int failed;
+  __shared__ int issued_s, consumed_s;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int w0 = blockIdx.x * TILE_M, h0 = blockIdx.y * R, d = blockIdx.z;
 
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+    for (int b = 0; b < NS; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
     mbar_init(&done, 1);
     failed = 0;
+    issued_s = 0;
+    consumed_s = 0;
     fence_barrier_init();
   }
   if (warp == 0) tmem_alloc(&tmem_base, C::COLS);
@@ -217,10 +226,23 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base;
+  uint8_t* const Bbase = smem + NS * C::A_BYTES;
 
-  if (tid == 0) {
-    uint8_t* const Bbase = smem + 2 * C::A_BYTES;
-    auto issue = [&](int s, int buf) {
+  // Producer (thread 32): line stage s goes to buffer s % NS; it is
+  // refilled once the products of the stage that last used it completed
+  // (its "empty" barrier), so the copies run up to NS stages ahead of the
+  // products.  A weight buffer is rewritten (first stage of slice 2) only
+  // after the products of every stage of slice 0 completed: stages complete
+  // in order and slice 0 ends at least NS stages earlier.
+  if (tid == 32) {
+    int s = 0;
+    for (; s < C::NSTG && !failed; ++s) {
+      const int buf = s % NS;
+      if (s >= NS && !mbar_wait(&empty[buf], ((s / NS) - 1) & 1)) {
+        atomicOr(err, 2);
+        failed = 1;
+        break;
+      }
       const int zi = s / (R + 2), ri = s % (R + 2);
       uint8_t* A = smem + buf * C::A_BYTES;
       const bool new_slice = ri == 0;
@@ -231,16 +253,15 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
       if (new_slice)
         bulk_load(Bbase + (zi & 1) * C::B_BYTES, Wp + (size_t)9 * zi * CIN * COUT, C::B_BYTES,
                   &full[buf]);
-    };
-    int issued = 0;
-    issue(0, 0);
-    issue(1, 1);
-    issued = 2;
-    int consumed = 0;
-    for (int s = 0; s < C::NSTG; ++s) {
-      const int buf = s & 1;
-      const uint32_t par = (s >> 1) & 1;
-      if (!mbar_wait(&full[buf], par)) {
+    }
+    issued_s = s;
+  }
+  // MMA issuer (thread 0)
+  if (tid == 0) {
+    int s = 0;
+    for (; s < C::NSTG; ++s) {
+      const int buf = s % NS;
+      if (failed || !mbar_wait(&full[buf], (s / NS) & 1)) {
         atomicOr(err, 1);
         failed = 1;
         break;
@@ -268,22 +289,14 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
         }
       }
       mma_commit(&empty[buf]);
-      consumed = s + 1;
-      if (s + 2 < C::NSTG) {
-        if (!mbar_wait(&empty[buf], par)) {
-          atomicOr(err, 2);
-          failed = 1;
-          break;
-        }
-        issue(s + 2, buf);
-        ++issued;
-      }
     }
-    if (failed) {
-      // let the copies already issued land before the CTA releases smem
-      for (int s = consumed; s < issued; ++s) (void)mbar_wait(&full[s & 1], (s >> 1) & 1);
-    }
+    consumed_s = s;
     mma_commit(&done);
+  }
+  __syncthreads();
+  if (tid == 32 && failed) {
+    // let the copies already issued land before the CTA releases smem
+    for (int s = consumed_s; s < issued_s; ++s) (void)mbar_wait(&full[s % NS], (s / NS) & 1);
   }
   __syncthreads();
   const bool ok = mbar_wait(&done, 0) && !failed;
