@@ -1037,63 +1037,33 @@ __global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, 
   }
 }
 
-// Stencil pass of the CN solve with plain halo loads, persistent CTAs over
-// bricks then chunks of BV Purkinje nodes (the set-up pass, and the whole
-// solve where the persistent diffusion kernel is not used).
-//   mode 0 (start of a step): x = W, r = Lh W, p = Dinv r; sums
-//          ||W + (1 - theta) Lh W||^2, ||r||^2, <r, Dinv r>_w;
-//   mode 1 (iteration): q = p - theta Lh p; sum <p, q>_w, alpha = rz / pq;
-//   mode 2 (set-up): dinv = 1 / (1 - theta diag Lh).
+// Set-up of the theta-scheme solve: the Jacobi inverse dinv = 1 / (1 - theta
+// diag Lh) of every tissue slot and Purkinje node (0 on padding slots), from
+// the same stencil code with every difference read as -1.  Persistent CTAs
+// over bricks, then chunks of BV Purkinje nodes; plain halo loads (it runs
+// once per handle).
 template <int BI, int BJ, int BK, bool ANISO>
-__global__ void __launch_bounds__(BI * BJ * BK)
-cn_stencil_kernel(MonoArgs a, CnArgs c, int mode) {
+__global__ void __launch_bounds__(BI * BJ * BK) cn_diag_kernel(MonoArgs a, CnArgs c) {
   using G = TileGeom<BI, BJ, BK>;
   constexpr int BV = G::BV, SI = G::SI, SJ = G::SJ;
-  if (mode == 1 && c.iscal[CI_DONE]) return;
-  const int64_t step = *a.d_step;
-  const bool odd = step & 1;
   const int64_t ns = a.n_slots;
-  const float* __restrict__ Smyo = mode == 0 ? (odd ? a.Vs1 : a.Vs0) : c.p;
-  const float* __restrict__ Spk = mode == 0 ? (odd ? a.pk_Vs1 : a.pk_Vs0) : c.p + ns;
   __shared__ int nb27[27];
-  __shared__ float tV[G::N];
   __shared__ float tW[ANISO ? 3 * G::N : 1];
   __shared__ float tD[ANISO ? 3 * G::N : 1];
   const int tid = threadIdx.x;
   const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
   const int cc = (li + 1) * SI + (lj + 1) * SJ + (lk + 1);
   const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
-  double v[3] = {0.0, 0.0, 0.0};
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     if (it >= a.n_bricks) {
       const int pn = (it - a.n_bricks) * BV + tid;
-      if (pn >= a.n_pk) continue;
-      const int64_t e = ns + pn;
-      const float w = c.pk_weight;
-      if (mode == 2) {
-        c.dinv[e] = 1.0f / (1.0f - c.theta * purkinje_acc<true>(a, pn, Spk, Smyo));
-        continue;
-      }
-      const float acc = purkinje_acc(a, pn, Spk, Smyo);
-      if (mode == 0) {
-        const float Wi = Spk[pn], z = c.dinv[e] * acc, b = Wi + c.omt * acc;
-        c.x[e] = Wi;
-        c.r[e] = acc;
-        c.p[e] = z;
-        v[0] += (double)b * b;
-        v[1] += (double)acc * acc;
-        v[2] += (double)w * acc * z;
-      } else {
-        const float pi = Spk[pn], qi = pi - c.theta * acc;
-        c.q[e] = qi;
-        v[0] += (double)w * pi * qi;
-      }
+      if (pn < a.n_pk)
+        c.dinv[ns + pn] = 1.0f / (1.0f - c.theta * purkinje_acc<true>(a, pn, nullptr, nullptr));
       continue;
     }
     __syncthreads();  // the previous brick's tiles are no longer read
     if (tid < 27) nb27[tid] = a.nbr[(int64_t)it * 27 + tid];
     __syncthreads();
-    if (mode != 2) load_region<BI, BJ, BK, -1, BI + 1, -1, BJ + 1, -1, BK + 1>(tV, Smyo, nb27, tid);
     if constexpr (ANISO) {
       load_region<BI, BJ, BK, -1, BI, 0, BJ, 0, BK>(tW, a.wface, nb27, tid);
       load_region<BI, BJ, BK, 0, BI, -1, BJ, 0, BK>(tW + G::N, a.wface + ns, nb27, tid);
@@ -1105,36 +1075,11 @@ cn_stencil_kernel(MonoArgs a, CnArgs c, int mode) {
     __syncthreads();
     const int64_t slot = (int64_t)it * BV + tid;
     const uint32_t tag = a.tag[slot];
-    if (!(tag & HP_TAG_PHENO_MASK)) {  // padding: keeps every vector at 0
-      if (mode == 2) c.dinv[slot] = 0.0f;
-      else if (mode == 0) c.x[slot] = c.r[slot] = c.p[slot] = 0.0f;
-      else c.q[slot] = 0.0f;
-      continue;
-    }
-    if (mode == 2) {
-      c.dinv[slot] = 1.0f / (1.0f - c.theta * stencil_acc<SI, SJ, G::N, ANISO, true>(
-                                                 a, tV, tW, tD, cc, tag, slot, Spk));
-      continue;
-    }
-    const float acc = stencil_acc<SI, SJ, G::N, ANISO>(a, tV, tW, tD, cc, tag, slot, Spk);
-    if (mode == 0) {
-      const float Wi = tV[cc], z = c.dinv[slot] * acc, b = Wi + c.omt * acc;
-      c.x[slot] = Wi;
-      c.r[slot] = acc;
-      c.p[slot] = z;
-      v[0] += (double)b * b;
-      v[1] += (double)acc * acc;
-      v[2] += (double)acc * z;
-    } else {
-      const float pi = tV[cc], qi = pi - c.theta * acc;
-      c.q[slot] = qi;
-      v[0] += (double)pi * qi;
-    }
+    c.dinv[slot] = (tag & HP_TAG_PHENO_MASK)
+                       ? 1.0f / (1.0f - c.theta * stencil_acc<SI, SJ, G::N, ANISO, true>(
+                                                  a, nullptr, tW, tD, cc, tag, slot, nullptr))
+                       : 0.0f;
   }
-  if (mode == 2) return;
-  double tot[3];
-  if (cn_reduce_last<BV, 3>(v, c, tot) && threadIdx.x == 0)
-    cn_pass_scalars(c, mode == 0 ? OP_CN_START : OP_CN_APPLY, tot);
 }
 
 // x += alpha p, r -= alpha q; sums ||r||^2 and <r, Dinv r>_w; the last block
@@ -1266,7 +1211,7 @@ __global__ void fill_kernel(float* p, int64_t n, float v) {
 __global__ void advance_kernel(int64_t* d_step, int64_t n) { *d_step += n; }
 
 typedef void (*StepFn)(MonoArgs, int, int);
-typedef void (*CnFn)(MonoArgs, CnArgs, int);
+typedef void (*CnFn)(MonoArgs, CnArgs);
 typedef void (*CnPassFn)(MonoArgs, CnArgs);
 typedef void (*PipeFn)(MonoArgs, int);  // also the diffusion half of the split step
 typedef std::vector<uint32_t> (*HaloFn)(bool);
@@ -1291,7 +1236,7 @@ struct ShapeEntry {
    PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS,                      \
    DiffHalo<I, J, K, false>::PER_THREAD * I * J * K, DiffHalo<I, J, K, true>::PER_THREAD * I * J * K, \
    DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS,                      \
-   cn_stencil_kernel<I, J, K, false>, cn_stencil_kernel<I, J, K, true>,                      \
+   cn_diag_kernel<I, J, K, false>, cn_diag_kernel<I, J, K, true>,                            \
    cn_pass_kernel<I, J, K, false, OP_CN_START>, cn_pass_kernel<I, J, K, true, OP_CN_START>,  \
    cn_pass_kernel<I, J, K, false, OP_CN_APPLY>, cn_pass_kernel<I, J, K, true, OP_CN_APPLY>}
 static const ShapeEntry kShapes[] = {HP_SHAPE(4, 4, 8), HP_SHAPE(4, 8, 8), HP_SHAPE(2, 4, 16),
@@ -1312,7 +1257,7 @@ struct HpMono {
   int diff_grid;     // its persistent grid
   int ion_grid;      // grid of the ionic half
   size_t diff_smem;  // and dynamic shared memory per CTA
-  CnFn cn;           // theta > 0: set-up stencil pass (Jacobi diagonal), or null
+  CnFn cn;           // theta > 0: set-up pass (Jacobi diagonal), or null
   CnPassFn cn_start, cn_apply;  // tiled passes: start of a solve, A p
   CnArgs cn_a;
   int cn_grid;       // persistent grid of the set-up pass
@@ -1470,8 +1415,8 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   return HP_OK;
 }
 
-// Theta-scheme diffusion half: CG vectors, the persistent grid of the
-// stencil pass and the Jacobi diagonal (one stencil pass in mode 2).
+// Theta-scheme diffusion half: CG vectors, the grids of the tiled passes and
+// the vector kernels, and the Jacobi diagonal (cn_diag_kernel, once).
 static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, cudaStream_t s) {
   CnArgs& c = h->cn_a;
   memset(&c, 0, sizeof(c));
@@ -1523,7 +1468,7 @@ static hp_status setup_cn(HpMono* h, const ShapeEntry* se, const HpMonoDesc* d, 
   HP_CUDA_TRY(cudaMallocHost((void**)&h->cn_host, 2 * sizeof(int32_t)));
   h->a.cn_x = c.x;
   HP_CUDA_TRY(cudaStreamCreateWithFlags(&h->cn_body_stream, cudaStreamNonBlocking));
-  h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c, 2);
+  h->cn<<<h->cn_grid, h->bv, 0, s>>>(h->a, c);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
