@@ -328,7 +328,8 @@ def run_torso(args):
             if name == "plain_pcg":
                 _, st = solver.solve_frame(fr[f], 1e-6, "rel", 50000)
             else:
-                _, st = pc.solve_frame(fr[f], 1e-6, 50000, 300,
+                _, st = pc.solve_frame(fr[f], 1e-6, 50000,
+                                       args.net_iters if name == "learned_fcg" else 300,
                                        use_net=args.net_every if name == "learned_fcg" else 0)
             torch.cuda.synchronize()
             if f >= 8 + 1 + args.warmup:
@@ -342,6 +343,7 @@ def run_torso(args):
             out[name]["restarts"] = rst
         if name == "learned_fcg":
             out[name]["network_every"] = args.net_every
+            out[name]["network_iterations"] = args.net_iters
     rows = solver.n_rows
     if pc is not None:
         pc.close()
@@ -474,7 +476,7 @@ def run_ours(args):
         if args.theta:
             line["theta_scheme"] = theta_leg(prob)
         if args.torso:
-            line["torso"] = torso_leg(prob, net_every=args.net_every)
+            line["torso"] = torso_leg(prob, net_every=args.net_every, net_iters=args.net_iters)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -517,7 +519,7 @@ def theta_leg(prob, n_steps=100, warm=20, theta=0.5, cg_tol=1e-5):
             "vm_finite": bool(np.isfinite(vm).all())}
 
 
-def torso_leg(prob, n_train=8, n_test=5, net_every=1):
+def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
     """Torso forward solve (192 x 160 x 256 voxels at 1.5 mm, lungs, blood
     pools, the biventricular shell embedded; 12-lead + 16 x 16 read-out) on
     Vm frames simulated here by the fused monodomain step (1 ms apart).  The
@@ -576,7 +578,8 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1):
             if name == "plain_pcg":
                 _, st = solver.solve_frame(frames[f], 1e-6, "rel", 50000)
             else:
-                _, st = pc.solve_frame(frames[f], 1e-6, 50000, 300,
+                _, st = pc.solve_frame(frames[f], 1e-6, 50000,
+                                       net_iters if name == "learned_fcg" else 300,
                                        use_net=net_every if name == "learned_fcg" else 0)
             torch.cuda.synchronize()
             ms.append((time.perf_counter() - t1) * 1e3)
@@ -589,6 +592,7 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1):
             out[name]["restarts"] = rst     # +100 network fallback, +1000 plain PCG
         if name == "learned_fcg":
             out[name]["network_every"] = net_every
+            out[name]["network_iterations"] = net_iters   # then the two-level method
     n_rows = solver.n_rows
     ag, nc = pc.coarse_info()
     pc.close()
@@ -717,6 +721,9 @@ def main():
                     help="torso workload: solvers to time (the last one is the headline)")
     ap.add_argument("--net-every", type=int, default=1, choices=[1, 2, 4],
                     help="learned FCG: the network term on every k-th iteration")
+    ap.add_argument("--net-iters", type=int, default=25,
+                    help="learned FCG: iterations with the network before the two-level "
+                         "method takes over the frame")
     ap.add_argument("--no-theta", dest="theta", action="store_false",
                     help="skip the theta = 0.5 (Crank-Nicolson) leg")
     ap.add_argument("--no-torso", dest="torso", action="store_false",

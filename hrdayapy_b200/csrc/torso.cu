@@ -1246,19 +1246,22 @@ static hp_status fcg_run(HpTorso* h, HpPrecond* p, double tol, int fallback_iter
 // Flexible CG with the learned preconditioner.  Safeguards, in order: when
 // the run with the network fails (no convergence within fallback_iter,
 // stagnation or breakdown), FCG restarts from the current iterate without
-// the network (the two-level method, restarts += 100; no stagnation test);
-// when that fails too, plain Jacobi-PCG finishes the frame (restarts +=
-// 1000).
+// the network (the two-level method, restarts += 100; no stagnation test,
+// up to max(fallback_iter, 1000) iterations); when that fails too, plain
+// Jacobi-PCG finishes the frame (restarts += 1000).
 static hp_status fcg_solve(HpTorso* h, HpPrecond* p, double tol, int max_iter, int fallback_iter,
                            int use_net, HpSolveStats* stats, hp_status* result_out, cudaStream_t s) {
   int it_total = 0, restarts = 0;
   double rel = 0.0;
   bool fallback = false;
   hp_status result = HP_OK;
-  // the run with the network (use_net = its period), then without it
+  // the run with the network (use_net = its period) for at most
+  // fallback_iter iterations, then without it (the two-level method, which
+  // converges on its own: up to 1000 iterations, or fallback_iter if more)
   for (int net = use_net; net >= 0; net = net > 0 ? 0 : -1) {
     int it = 0;
-    const int budget = std::max(1, std::min(fallback_iter, max_iter - it_total));
+    const int cap = net > 0 ? fallback_iter : std::max(fallback_iter, 1000);
+    const int budget = std::max(1, std::min(cap, max_iter - it_total));
     hp_status st = fcg_run(h, p, tol, budget, net, &it, &restarts, &rel, &fallback, s);
     if (st != HP_OK) return st;
     it_total += it;

@@ -393,8 +393,10 @@ hp_status hp_torso_arrays(HpTorso *h, HpTorsoArrays *out);
  * admits a preconditioner that varies between iterations).  If a run with the
  * network has not converged after fallback_iter iterations, stagnates or
  * breaks down, FCG restarts from the current iterate without the network
- * (stats->restarts += 100); if that fails as well, plain Jacobi-PCG
- * finishes the frame (stats->restarts += 1000). */
+ * (stats->restarts += 100; up to max(fallback_iter, 1000) iterations); if
+ * that fails as well, plain Jacobi-PCG finishes the frame
+ * (stats->restarts += 1000).  A small fallback_iter thus limits the network
+ * to the first iterations of every frame. */
 hp_status hp_torso_solve_frame_fcg(HpTorso *h, HpPrecond *p, const float *vm,
                                    int32_t vm_on_device, float *out, int32_t out_on_device,
                                    double tol, int32_t max_iter, int32_t fallback_iter,
