@@ -384,6 +384,10 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+        # the CPU baseline (N = 1 only) and the theta-scheme and torso legs
+        # belong to the single-GPU line: replicas time the step alone, so no
+        # rank waits at the final barrier while rank 0 runs extra work
+        args.cpu_baseline = args.theta = args.torso = False
     prob, info = build_workload(args.workload)
     fs = prob.frame_steps
     tune_table = None
