@@ -625,8 +625,11 @@ def e2e_run(prob, args, fs):
     import torch
     from hrdayapy_b200 import monodomain as M
     import dataclasses
-    k = max(1, min(args.steps, 10))
-    p2 = dataclasses.replace(prob, n_steps=k * fs, site_on=prob.site_on[: k * fs + 1].copy(),
+    # 40 frames (40 ms of simulated time) at the default 20 bench steps: the
+    # handle's creation (problem upload) is paid once per run, as in a user's
+    # run of hundreds of frames
+    k = max(1, min(2 * args.steps, 40))
+    p2 = dataclasses.replace(prob, n_steps=k * fs, site_on=np.resize(prob.site_on, k * fs + 1),
                              vm_every=fs)
     h2d = (p2.tag.nbytes + (p2.wface.nbytes + p2.doff.nbytes if p2.anisotropic else 0) +
            p2.layout.brick_nbr.nbytes + p2.pk_ptr.nbytes + p2.pk_idx.nbytes +
@@ -646,7 +649,8 @@ def e2e_run(prob, args, fs):
     sim.close()
     return {"value": p2.n_myo * fs * k / dt_s, "unit": "voxel-steps/s",
             "h2d_bytes_per_step": int(h2d // k), "d2h_bytes_per_step": int(p2.n_myo * 4),
-            "steps": k, "includes": "hp_mono_create upload + run + per-frame Vm D2H",
+            "steps": k, "includes": "hp_mono_create upload + run + per-frame Vm D2H "
+                                    "(frames of 1 ms, one per bench step)",
             "create_s": t1 - t0, "run_and_d2h_s": t2 - t1}
 
 
