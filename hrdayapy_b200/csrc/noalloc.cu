@@ -6,22 +6,28 @@
 // callers bound by a fixed memory budget.  hp_torso_residual_noalloc gives
 // them the solver's convergence judge -- ||b - A x|| and ||b|| in FP64 over
 // the torso operator -- without any cudaMalloc: the only scratch it needs
-// (the per-block partial sums of a deterministic reduction and a ticket
-// counter) lives in the file-scope array g_noalloc_scratch below.
+// (the per-block partial sums of a deterministic reduction, a ticket
+// counter and two error counters) lives in the file-scope array
+// g_noalloc_scratch below.
 //
 // Limits and sharing:
 //   * at most HP_NOALLOC_MAX_CELLS padded grid cells per call (one thread
 //     per cell, one partial per 256-cell block);
 //   * the array exists once per GPU that loads the library and stays
-//     allocated (1.5 MB) until the process exits;
+//     allocated until the process exits: (4 + 2 * HP_NOALLOC_MAX_BLOCKS)
+//     doubles = 1,048,608 bytes (about 1.0 MiB);
 //   * every call on a device uses the same array, which keeps the last
-//     call's contents: the ticket is cleared at the start of each call, so
-//     sequential calls are independent, but calls that overlap on the GPU
-//     (concurrent streams, or host threads calling at once) race and must
-//     not be issued;
+//     call's contents: the ticket and the error counters are cleared at the
+//     start of each call, so sequential calls are independent, but calls
+//     that overlap on the GPU (concurrent streams, or host threads calling
+//     at once) race and must not be issued;
+//   * the call is synchronous: it copies its two sums back to the host and
+//     waits for the stream before it returns;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current, so make that first
-//     call before any stream capture begins.
+//     (cudaGetSymbolAddress) with that device current and keeps it for the
+//     life of the process, so make that first call before any stream
+//     capture begins, and do not use the entry point across a
+//     cudaDeviceReset (the kept address belongs to the old context).
 #include "hp_common.cuh"
 
 #include <math.h>
@@ -34,8 +40,9 @@ constexpr int TB = 256;
 constexpr int64_t MAX_CELLS = (int64_t)HP_NOALLOC_MAX_BLOCKS * TB;
 constexpr int MAX_DEVICES = 64;
 
-// [0] ticket (uint32) + error count (uint32), [1] ||r||^2, [2] ||b||^2,
-// [3] spare, [4 + 2 q], [5 + 2 q]: partials of block q.
+// [0] ticket (uint32) + count of interior voxels with a label >= n_materials
+// (uint32), [1] ||r||^2, [2] ||b||^2, [3] count of border cells that are not
+// air (uint32), [4 + 2 q], [5 + 2 q]: partials of block q.
 static __device__ __align__(256) double g_noalloc_scratch[4 + 2 * HP_NOALLOC_MAX_BLOCKS];
 
 struct Params {
@@ -59,6 +66,7 @@ residual_kernel(Params p, const uint8_t* __restrict__ label, const double* __res
                 const float* __restrict__ b, double* scratch) {
   unsigned int* ticket = (unsigned int*)scratch;
   unsigned int* bad = ticket + 1;
+  unsigned int* bad_border = (unsigned int*)(scratch + 3);
   const int64_t g = blockIdx.x * (int64_t)TB + threadIdx.x;
   double rr = 0.0, bb = 0.0;
   if (g < p.ng) {
@@ -66,6 +74,7 @@ residual_kernel(Params p, const uint8_t* __restrict__ label, const double* __res
     const int i = (int)(g / SI), j = (int)((g / SJ) % p.pj), k = (int)(g % SJ);
     const bool interior = i > 0 && i < p.pi - 1 && j > 0 && j < p.pj - 1 && k > 0 && k < p.pk - 1;
     const int l = label[g];
+    if (!interior && l != 0) atomicAdd(bad_border, 1u);
     if (interior && l != 0 && g != p.pin) {
       if (l >= p.n_materials) {
         atomicAdd(bad, 1u);
@@ -171,7 +180,7 @@ extern "C" hp_status hp_torso_residual_noalloc(int32_t ni, int32_t nj, int32_t n
   HP_REQUIRE(n_materials >= 1 && n_materials <= HP_MAX_MATERIALS,
              "hp_torso_residual_noalloc: n_materials must be 1..%d", HP_MAX_MATERIALS);
   HP_REQUIRE(h_m > 0.0, "hp_torso_residual_noalloc: h_m must be positive");
-  const int64_t ng = (int64_t)(ni + 2) * (nj + 2) * (nk + 2);
+  const int64_t ng = ((int64_t)ni + 2) * ((int64_t)nj + 2) * ((int64_t)nk + 2);
   HP_REQUIRE(ng <= MAX_CELLS,
              "hp_torso_residual_noalloc: padded grid of %lld cells exceeds the maximum of %lld "
              "cells (its scratch array is fixed at build time)",
@@ -190,15 +199,21 @@ extern "C" hp_status hp_torso_residual_noalloc(int32_t ni, int32_t nj, int32_t n
   for (int q = 0; q < HP_MAX_MATERIALS; ++q) p.sigma[q] = q < n_materials ? sigma[q] : 0.0;
   p.inv_h2 = 1.0 / (h_m * h_m);
   cudaStream_t s = (cudaStream_t)stream;
-  // the ticket and the error count must start at zero
-  HP_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(double), s));
+  // the ticket and both error counters must start at zero (words 0-3)
+  HP_CUDA_TRY(cudaMemsetAsync(scratch, 0, 4 * sizeof(double), s));
   const unsigned int nblk = (unsigned int)((ng + TB - 1) / TB);
   residual_kernel<<<nblk, TB, 0, s>>>(p, label, x, b, scratch);
   HP_CUDA_TRY(cudaGetLastError());
-  double res[3];
-  HP_CUDA_TRY(cudaMemcpyAsync(res, scratch, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  double res[4];
+  HP_CUDA_TRY(cudaMemcpyAsync(res, scratch, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
   unsigned int bad = ((unsigned int*)&res[0])[1];
+  unsigned int bad_border = ((unsigned int*)&res[3])[0];
+  if (bad_border) {
+    hp::set_error("hp_torso_residual_noalloc: %u cells of the one-voxel border carry a nonzero "
+                  "label; the border of the padded grid must be air (label 0)", bad_border);
+    return HP_ERR_INVALID;
+  }
   if (bad) {
     hp::set_error("hp_torso_residual_noalloc: %u voxels carry a label >= n_materials", bad);
     return HP_ERR_INVALID;

@@ -280,15 +280,19 @@ hp_status hp_torso_destroy(HpTorso *h);
  * owns every allocation, a real-time loop, a fixed memory budget): computes
  * out[0] = ||b - A x|| and out[1] = ||b|| (host doubles) for the torso
  * operator of hp_torso_create, with no cudaMalloc -- its only scratch is a
- * fixed array inside the library (HP_NOALLOC_MAX_BLOCKS partials, 1.5 MB per
- * GPU, held until exit).  label (uint8), x (fp64) and b (fp32) are device
- * arrays over the PADDED grid (ni+2) x (nj+2) x (nk+2), k fastest, whose
- * one-voxel border is air; pin_cell is the padded flat index of the pinned
- * voxel (-1: none); sigma (host) holds n_materials conductivities in S/m
- * (label 0 = air).  Padded grids above HP_NOALLOC_MAX_CELLS are rejected
- * with HP_ERR_INVALID.  Every call shares the scratch array: calls that
- * overlap on the GPU race.  The first call on a device resolves the array's
- * address on that device, so make it before any stream capture.
+ * fixed array inside the library of (4 + 2 * HP_NOALLOC_MAX_BLOCKS) doubles
+ * (1,048,608 bytes, about 1.0 MiB, per GPU, held until exit).  label
+ * (uint8), x (fp64) and b (fp32) are device arrays over the PADDED grid
+ * (ni+2) x (nj+2) x (nk+2), k fastest, whose one-voxel border must be air
+ * (a nonzero border label is rejected with HP_ERR_INVALID); pin_cell is the
+ * padded flat index of the pinned voxel (-1: none); sigma (host) holds
+ * n_materials conductivities in S/m (label 0 = air).  Padded grids above
+ * HP_NOALLOC_MAX_CELLS are rejected with HP_ERR_INVALID.  The call is
+ * synchronous (it waits for its stream before returning).  Every call
+ * shares the scratch array: calls that overlap on the GPU race.  The first
+ * call on a device resolves the array's address on that device and keeps
+ * it, so make it before any stream capture, and do not use the entry point
+ * across a cudaDeviceReset.
  */
 #define HP_NOALLOC_MAX_BLOCKS 65536
 #define HP_NOALLOC_MAX_CELLS (HP_NOALLOC_MAX_BLOCKS * 256LL)

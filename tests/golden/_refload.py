@@ -8,13 +8,15 @@ animation-only) is replaced by a stub because skimage is absent.
 from __future__ import annotations
 
 import importlib.util
+import os
 import sys
 import types
 from pathlib import Path
 
 import numpy as np
 
-REF_ROOT = Path("/root/reference")
+# root of the upstream HrdayaPy checkout (the directory holding hrdayapy/)
+REF_ROOT = Path(os.environ.get("HRDAYAPY_REF_ROOT", "/root/reference"))
 
 
 def _pkg(name: str, path: Path) -> None:

@@ -84,3 +84,26 @@ def test_noalloc_rejects_oversized_grid():
                                      -1, C.c_void_p(16), C.c_void_p(16), _lib.ptr(out), None)
     assert st == 1
     assert b"exceeds the maximum" in L.hp_last_error()
+
+
+def test_noalloc_rejects_tissue_on_the_border():
+    """The padded grid's one-voxel border must be air: a conductive border
+    cell would act as a neighbour the solver's operator does not have."""
+    import torch
+    from hrdayapy_b200 import _lib
+    L = _lib.lib()
+    ni, nj, nk = 6, 5, 4
+    lab = np.zeros((ni + 2, nj + 2, nk + 2), np.uint8)
+    lab[1:-1, 1:-1, 1:-1] = 1
+    lab[0, 3, 2] = 1                       # tissue on the border
+    dev = torch.device("cuda")
+    lab_d = torch.from_numpy(lab.ravel()).to(dev)
+    x_d = torch.zeros(lab.size, dtype=torch.float64, device=dev)
+    b_d = torch.ones(lab.size, dtype=torch.float32, device=dev)
+    sig = np.array([0.0, 0.2])
+    out = np.zeros(2)
+    st = L.hp_torso_residual_noalloc(ni, nj, nk, C.c_void_p(lab_d.data_ptr()), _lib.ptr(sig), 2,
+                                     1e-3, -1, C.c_void_p(x_d.data_ptr()),
+                                     C.c_void_p(b_d.data_ptr()), _lib.ptr(out), None)
+    assert st == 1
+    assert b"border" in L.hp_last_error()
