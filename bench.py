@@ -362,6 +362,16 @@ def run_torso(args):
                                        "peak_source": kind}}), flush=True)
 
 
+# (kernel id, brick, anisotropic) -> (DRAM bytes per myocardial voxel-step,
+# the capture it comes from): ncu --metrics dram__bytes_read.sum,
+# dram__bytes_write.sum over both launches of one time step
+DRAM_BYTES_PER_VOXEL_STEP = {
+    (3, (4, 4, 8), True): (5.0e8 / 2544045,
+                           "split step: mono_diffuse_kernel 132 MB + mono_ionic_kernel 368 MB "
+                           "on the 2,544,045-voxel shell"),
+}
+
+
 def bytes_per_voxel_step(prob):
     """Algorithmic HBM bytes per myocardial voxel-step of the fused kernel:
     18 TTP06 state variables + membrane potential read and written (FP32,
@@ -371,6 +381,7 @@ def bytes_per_voxel_step(prob):
 
 
 def run_ours(args):
+    import dataclasses
     import torch
     from hrdayapy_b200 import monodomain as M
 
@@ -401,6 +412,7 @@ def run_ours(args):
         prob.frame_steps = fs
     total_steps = (args.warmup + args.steps) * fs
     prob.n_steps = total_steps
+    site_on_full = np.array(prob.site_on)       # the whole run's schedule, for the parity leg
     prob.site_on = np.resize(prob.site_on, total_steps + 1)
     n_vox = prob.n_myo
     stream = torch.cuda.Stream()
@@ -436,16 +448,15 @@ def run_ours(args):
     achieved = n_vox * bpv / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
 
-    # DRAM bytes of one time step from the ncu capture of this workload's
-    # split step (both launches; the capture is of 4x4x8 bricks, 19-point)
-    traffic, traffic_note = None, "no ncu capture for this configuration"
-    if (kinfo[0] == 3 and tuple(prob.layout.brick) == (4, 4, 8) and prob.anisotropic
-            and args.workload == "biv_shell"):
-        traffic = 5.0e8
-        traffic_note = ("bytes per time step (dram__bytes_read.sum + dram__bytes_write.sum of "
-                        "mono_diffuse_kernel 132 MB + mono_ionic_kernel 368 MB, one ncu "
-                        "capture, profiles/mono_step_biv_shell.md) vs algorithmic "
-                        f"{bpv * n_vox / 1e6:.0f} MB")
+    # DRAM bytes per time step: dram__bytes_read.sum + dram__bytes_write.sum
+    # of one step's launches from an ncu capture of the same kernel and brick
+    # shape, per myocardial voxel, scaled by this workload's voxel count
+    traffic, traffic_note = None, "no ncu capture for this kernel / brick shape"
+    cap = DRAM_BYTES_PER_VOXEL_STEP.get((kinfo[0], tuple(prob.layout.brick), bool(prob.anisotropic)))
+    if cap is not None:
+        traffic = cap[0] * n_vox
+        traffic_note = (f"{cap[0]:.1f} B per voxel-step x {n_vox} voxels ({cap[1]}) vs "
+                        f"algorithmic {bpv * n_vox / 1e6:.0f} MB")
     # end to end through the C-ABI handle: host buffers in, Vm frames out;
     # three repetitions, the median reported (the first one also pays
     # first-use costs of the process: pinned buffers, module loads)
@@ -474,13 +485,15 @@ def run_ours(args):
                       "vm_range_mV": [float(vm_last.min()), float(vm_last.max())]},
         }
         if args.cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(prob, info, args)
+            line["cpu_baseline"], line["check"]["parity"] = shell_parity_and_cpu_baseline(
+                dataclasses.replace(prob, site_on=site_on_full), args, parity_ms=args.parity_ms)
         if tune_table is not None:
             line["autotune"] = [{k: v for k, v in t.items()} for t in tune_table[:8]]
         if args.theta:
             line["theta_scheme"] = theta_leg(prob)
         if args.torso:
-            line["torso"] = torso_leg(prob, net_every=args.net_every, net_iters=args.net_iters)
+            line["torso"] = torso_leg(prob, net_every=args.net_every, net_iters=args.net_iters,
+                                      parity=args.cpu_baseline)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -523,7 +536,7 @@ def theta_leg(prob, n_steps=96, warm=496, theta=0.5, cg_tol=1e-5):
             "vm_finite": bool(np.isfinite(vm).all())}
 
 
-def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
+def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25, parity=True, n_parity=2):
     """Torso forward solve (192 x 160 x 256 voxels at 1.5 mm, lungs, blood
     pools, the biventricular shell embedded; 12-lead + 16 x 16 read-out) on
     Vm frames simulated here by the fused monodomain step (1 ms apart).  The
@@ -572,6 +585,7 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
     t_train = time.perf_counter() - t0
     test0 = 4 * n_train      # frame index (into `frames`) the held-out chain starts from
     out = {}
+    xs = {}                  # solutions of the first n_parity held-out frames, per method
     for name in ("plain_pcg", "two_level_fcg", "learned_fcg"):
         solver.reset()
         solver.solve_frame(frames[test0], 1e-6, "rel", 50000)
@@ -590,6 +604,8 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
             its.append(int(st.iterations))
             rel.append(float(st.rel_residual))
             rst.append(int(st.restarts))
+            if parity and f <= test0 + n_parity:
+                xs.setdefault(name, []).append(solver.solution())
         out[name] = {"ms_per_frame": float(np.mean(ms)), "iterations": its,
                      "max_rel_residual": max(rel)}
         if name != "plain_pcg":
@@ -601,6 +617,11 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
     ag, nc = pc.coarse_info()
     pc.close()
     solver.close()
+    extra = {}
+    if parity:
+        vm_par = frames[test0 + 1:test0 + 1 + n_parity].cpu().numpy()
+        extra["cpu_baseline"], extra["check"] = torso_parity_and_cpu_baseline(
+            grid, vox, coords, reg, geo["h"], vm_par, xs, rows)
     peak, peak_kind = peaks()
     p = out["plain_pcg"]
     t_it = p["ms_per_frame"] * 1e-3 / max(np.mean(p["iterations"]), 1)
@@ -617,7 +638,8 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25):
             "pcg_roofline": {"bound": "hbm", "bytes_per_unknown_per_iteration": 40,
                              "achieved": 40.0 * n_rows / t_it / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": 40.0 * n_rows / t_it / 1e9 / peak, "peak_source": peak_kind,
-                             "note": "plain PCG time per iteration incl. its per-frame set-up"}}
+                             "note": "plain PCG time per iteration incl. its per-frame set-up"},
+            **extra}
 
 
 def e2e_run(prob, args, fs):
@@ -654,26 +676,126 @@ def e2e_run(prob, args, fs):
             "create_s": t1 - t0, "run_and_d2h_s": t2 - t1}
 
 
-def cpu_baseline(prob, info, args, budget_s=15.0):
-    """FP64 CPU restatement of the reference method (oracle), all host
-    threads, on a bounded number of time steps of the same workload."""
+def shell_parity_and_cpu_baseline(prob, args, parity_ms=16.0, chunk=25):
+    """The FP64 CPU restatement of the reference method (oracle: the C time
+    loop on all host threads) runs the workload from rest for parity_ms of
+    simulated time (16 ms: the tree's first junction band fires at 12.7 ms
+    and the wavefront has entered the myocardium), recording every
+    myocardial node's first -20 mV crossing in the loop.  The wall time of
+    its time loop is the CPU baseline (voxel-steps/s); its final state and
+    activation times are the FP64 run that the GPU's FP32 run of the same
+    steps (same kernel and bricks as the timed run) is checked against:
+    Vm RMS over all myocardial nodes and over the Purkinje nodes after the
+    last step, max activation-time error over the voxels both runs
+    activated, and how many voxels only one run activated."""
+    import dataclasses
+    from hrdayapy_b200 import monodomain as M, synthetic
     from oracle import mono as orc
-    from hrdayapy_b200 import synthetic
+    n = int(round(parity_ms / prob.dt))
+    if len(prob.site_on) < n + 1:
+        raise SystemExit("parity leg: stimulus table shorter than the parity window")
+    p = dataclasses.replace(prob, n_steps=n, site_on=np.array(prob.site_on[:n + 1]), vm_every=0,
+                            frame_every=0, act_threshold=-20.0, deact_threshold=-20.0)
+    sim = M.MonoHandle(p)
+    sim.run(n, graph_chunk=prob.frame_steps)
+    a, na, _, _ = sim.events()
+    vm, vp = sim.voltage()
+    sim.close()
     g = synthetic.last_inputs()
-    nthreads = orc.lib().orc_num_threads()
     ctx = orc.setup(*g["args"], vm_save_dt=None, **g["kw"])
-    t0 = time.perf_counter()
-    orc.advance(ctx, 2, snapshots=False)
-    per_step = (time.perf_counter() - t0) / 2
-    n = int(max(2, min(500, budget_s / max(per_step, 1e-6))))
-    t0 = time.perf_counter()
-    orc.advance(ctx, n, snapshots=False)
-    elapsed = time.perf_counter() - t0
-    N = ctx["N"]
-    return {"value": N * n / elapsed, "unit": "voxel-steps/s", "cores": int(nthreads),
+    first, _, _ = orc.advance_events(ctx, n, -20.0, chunk=chunk)
+    secs = ctx["_adv_seconds"]
+    N, Np = ctx["N"], ctx["Np"]
+    Vo = ctx["V"]
+    rms = float(np.sqrt(np.mean((vm.astype(np.float64) - Vo[Np:]) ** 2)))
+    rms_p = float(np.sqrt(np.mean((vp.astype(np.float64) - Vo[:Np]) ** 2))) if Np else 0.0
+    act_g = na >= 1
+    act_o = np.isfinite(first)
+    both = act_g & act_o
+    err = float(np.max(np.abs(a[0][both].astype(np.float64) - first[both]))) if both.any() else None
+    check = {"reference": f"FP64 oracle of the reference method, same {n} steps from rest",
+             "steps": n, "simulated_ms": n * prob.dt,
+             "vm_rms_mV": rms, "purkinje_vm_rms_mV": rms_p,
+             "max_act_err_ms": err, "act_threshold_mV": -20.0,
+             "activated_both": int(both.sum()), "activated_gpu_only": int((act_g & ~act_o).sum()),
+             "activated_oracle_only": int((act_o & ~act_g).sum()),
+             "tolerances": {"vm_rms_mV": 0.5, "max_act_err_ms": 0.1}}
+    base = {"value": N * n / secs, "unit": "voxel-steps/s", "cores": int(orc.lib().orc_num_threads()),
             "kind": "port",
-            "sample": f"{n} time steps of the full workload ({N} nodes incl. Purkinje), "
-                      f"FP64, set-up excluded"}
+            "sample": f"{n} time steps (0-{n * prob.dt:g} ms) from rest of the full workload "
+                      f"({N} nodes incl. Purkinje), FP64; set-up and crossing bookkeeping excluded"}
+    return base, check
+
+
+def torso_parity_and_cpu_baseline(grid, vox, coords, reg, h_fine_mm, vm_frames, xs, rows,
+                                  sigma_i=0.2625):
+    """FP64 check of the GPU's torso potentials on held-out frames, and the
+    reference method timed on the host cores.  The oracle assembles the
+    reference's stiffness (harmonic-mean faces, build_torso_grid.py:276-397),
+    pins it, builds each frame's FP64 source (compute_bspm.py:381-419) and
+    solves it by FP64 Jacobi-CG (orc_csr_pcg) to a 1e-10 relative true
+    residual.  Frame 0 starts from the GPU's plain-PCG solution (any start
+    reaches the same 1e-10 solution).  Frame 1 is first solved as the
+    reference solves a frame -- Jacobi-PCG warm-started from the previous
+    frame's solution, here to the 1e-6 relative residual of the
+    configuration -- and that solve is timed (the CPU baseline, ms/frame),
+    then continued to 1e-10.  Per GPU method: the true relative residual of
+    its solution re-evaluated on the host with the FP64 operator, the
+    relative L2 of each of the 12 leads over the frames against the FP64
+    solution, and of the 16 x 16 body-surface grid (as is, and with each
+    frame's mean removed: an FP32 right-hand side carries a rounding-size
+    net source that the pinned system turns into a near-uniform offset,
+    which leads cancel)."""
+    from oracle import mono as orc, torso as O
+    from hrdayapy_b200.ecg import torso as T
+    dx = float(grid["dx_mm"])
+    A, _, _ = O.assemble_stiffness(grid["sigma_vol"], dx * 1e-3, grid["active_mask"])
+    pin = int(grid["pin_row"])
+    Ap = O.pinned_csr(A, pin)
+    del A
+    K = O.heart_laplacian(np.asarray(vox, np.int64), len(vox))
+    proj, valid = O.projection_map(np.asarray(coords, np.float64), np.asarray(reg["R"], np.float64),
+                                   np.asarray(reg["t"], np.float64), 1.0,
+                                   np.asarray(grid["origin_mm"], np.float64), dx,
+                                   np.asarray(grid["active_id_map"]), grid["shape"])
+    nrow = Ap.shape[0]
+    bs = [O.frame_rhs(K, v, proj, valid, nrow, pin, sigma_i, h_fine_mm * 1e-3, dx) for v in vm_frames]
+    x0, it0, rel0, _ = O.pcg_fp64(Ap, bs[0], xs["plain_pcg"][0], tol=1e-10)
+    t = time.perf_counter()
+    x1, it1, rel1, _ = O.pcg_fp64(Ap, bs[1], x0, tol=1e-6)
+    t_cpu = time.perf_counter() - t
+    x1, it1b, rel1b, _ = O.pcg_fp64(Ap, bs[1], x1, tol=1e-10)
+    xo = [x0, x1]
+    rows = np.asarray(rows, np.int64)
+
+    def leads(xl):
+        e = np.stack([x[rows[:10]] for x in xl], 1) * 1e3          # (10, frames) mV
+        return T.twelve_lead(e), np.stack([x[rows[10:]] for x in xl], 1) * 1e3
+
+    Lo, Go = leads(xo)
+    out = {}
+    for name, xl in xs.items():
+        Lg, Gg = leads(xl[:len(xo)])
+        rel_lead = np.linalg.norm(Lg - Lo, axis=1) / np.linalg.norm(Lo, axis=1)
+        Gd = (Gg - Gg.mean(0)) - (Go - Go.mean(0))
+        out[name] = {
+            "host_true_rel_residual": [float(np.linalg.norm(b - Ap @ x) / np.linalg.norm(b))
+                                       for b, x in zip(bs, xl)],
+            "ecg_rel_l2_per_lead": [float(v) for v in rel_lead],
+            "ecg_rel_l2_max": float(rel_lead.max()),
+            "grid_rel_l2": float(np.linalg.norm(Gg - Go) / np.linalg.norm(Go)),
+            "grid_rel_l2_offset_free": float(np.linalg.norm(Gd) /
+                                             np.linalg.norm(Go - Go.mean(0)))}
+    check = {"reference": "FP64 Jacobi-CG on the reference's assembled stiffness and FP64 "
+                          "source, to a 1e-10 relative true residual",
+             "frames": len(xo), "oracle_rel_residual": [rel0, rel1b],
+             "oracle_iterations": [it0, it1 + it1b], "tolerance_ecg_rel_l2": 1e-3, **out}
+    base = {"value": t_cpu * 1e3, "unit": "ms/frame", "iterations": it1,
+            "cores": int(orc.lib().orc_num_threads()), "kind": "port",
+            "sample": "one held-out frame: FP64 Jacobi-PCG on the assembled reference operator, "
+                      "warm-started from the previous frame's solution, to the 1e-6 relative "
+                      "true residual"}
+    return base, check
 
 
 def run_reference(args):
@@ -722,7 +844,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="biv_shell")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false",
+                    help="skip the FP64 oracle legs (CPU baselines and the parity checks)")
+    ap.add_argument("--parity-ms", type=float, default=16.0,
+                    help="simulated ms of the FP64 oracle run the shell is checked against")
     ap.add_argument("--torso-shape", default="192,160,256",
                     help="torso voxels for --workload torso (extent fixed at 288 x 240 x 384 mm)")
     ap.add_argument("--torso-solvers", default="plain_pcg,two_level_fcg,learned_fcg",

@@ -397,6 +397,69 @@ def advance(ctx, n_steps, snapshots=True):
     return snaps[:n_snap], psnaps[:n_snap], times
 
 
+def advance_events(ctx, n_steps, act_threshold=-20.0, frame_every=0, chunk=250):
+    """Runs n_steps more time steps and records, in the loop, the first
+    upward crossing of ``act_threshold`` of every myocardial node between
+    consecutive post-step states, interpolated as activation_maps.py:63-89
+    does (float32, den == 0 -> 1e-9, frac clipped to [0, 1]); the same as
+    compute_activation_maps on snapshots saved every step
+    (activation_maps.py:295-350), without holding them all: the steps run in
+    chunks of ``chunk`` with every-step snapshots.  Returns (first
+    activation time per myocardial node, NaN where none; Vm frames at the
+    global steps that are multiples of ``frame_every`` (None if 0); their
+    times).  The crossing state carries over between calls through ctx;
+    ctx["_adv_seconds"] accumulates the wall time of the time loop alone
+    (the C calls, without the crossing bookkeeping)."""
+    import time
+    N_myo = ctx["N"] - ctx["Np"]
+    first = ctx.setdefault("_act_first", np.full(N_myo, np.nan, np.float32))
+    thr = np.float32(act_threshold)
+    se0 = ctx["snap_every"]
+    ctx["snap_every"] = 1
+    frames, ftimes = [], []
+    try:
+        done = 0
+        while done < n_steps:
+            n = min(chunk, n_steps - done)
+            t0 = time.perf_counter()
+            Vm, _, t = advance(ctx, n, snapshots=True)
+            ctx["_adv_seconds"] = ctx.get("_adv_seconds", 0.0) + time.perf_counter() - t0
+            prev = ctx.get("_act_prev")
+            if prev is not None:
+                Vm2 = np.concatenate([prev[0][None], Vm])
+                t2 = np.concatenate([np.array([prev[1]], np.float32), t])
+            else:
+                Vm2, t2 = Vm, t
+            above = Vm2 >= thr
+            rising = np.diff(above.astype(np.int8), axis=0) == 1
+            fi, ni = np.nonzero(rising)
+            if fi.size:
+                Vi, Vj = Vm2[fi, ni], Vm2[fi + 1, ni]
+                den = Vj - Vi
+                den = np.where(den == 0, np.float32(1e-9), den)
+                frac = np.clip((thr - Vi) / den, 0.0, 1.0)
+                tc = (t2[fi] + frac * (t2[fi + 1] - t2[fi])).astype(np.float32)
+                # first crossing per node: fi ascends within the chunk
+                order = np.lexsort((fi, ni))
+                ni_o, tc_o = ni[order], tc[order]
+                uniq, pos = np.unique(ni_o, return_index=True)
+                new = np.isnan(first[uniq])
+                first[uniq[new]] = tc_o[pos][new]
+            ctx["_act_prev"] = (Vm[-1].copy(), np.float32(t[-1]))
+            if frame_every:
+                k0 = ctx["step"] - n
+                sel = [r for r in range(n) if (k0 + r) % frame_every == 0]
+                if sel:
+                    frames.append(Vm[sel])
+                    ftimes.append(t[sel])
+            done += n
+    finally:
+        ctx["snap_every"] = se0
+    fr = np.concatenate(frames) if frames else None
+    ft = np.concatenate(ftimes) if ftimes else None
+    return first.copy(), fr, ft
+
+
 def run(nodes, elements, act_times, S, phi, **kw):
     """Full FP64 run of the reference method from rest.  Returns
     ``Vm`` (n_snap, N_myo) float32, ``time_vm``, ``Vp`` Purkinje snapshots,

@@ -16,6 +16,11 @@ FP64 CPU restatement of HrdayaPy's torso forward solve, used only by tests/,
   judged against
 * :func:`pcg_reference`      -- _pcg_gpu (compute_bspm.py:164-263) in FP64
   numpy, with its rms / linf stopping statistics
+* :func:`pinned_csr`, :func:`pcg_fp64` -- the pinned system in CSR form
+  without a LIL round trip, and _pcg_gpu's Jacobi-CG run in FP64 in C
+  (torso_oracle.c, pthreads) to a relative true residual: the FP64
+  solution the GPU's potentials are judged against at full torso size, and
+  the reference method timed on the host cores
 
 Pinned by tests/test_oracle_golden.py against tests/golden/torso.npz.
 """
@@ -164,3 +169,48 @@ def pcg_reference(A_pinned, b, x0=None, tol_mV=0.01, max_iter=500, metric="rms")
         p = z + (rz_new / rz) * p
         rz = rz_new
     return x, max_iter, stat(Minv * r) * 1e3
+
+
+def pinned_csr(A, pin):
+    """The pinned system of make_gpu_solver (compute_bspm.py:327-336): row
+    and column ``pin`` zeroed, 1 on its diagonal; CSR, without a LIL round
+    trip (fast at millions of rows)."""
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    keep = np.ones(n)
+    keep[pin] = 0.0
+    D = sp.diags(keep, format="csr")
+    Ap = (D @ A @ D).tocsr()
+    Ap = Ap + sp.csr_matrix(([1.0], ([pin], [pin])), shape=(n, n))
+    Ap.sort_indices()
+    return Ap.tocsr()
+
+
+def pcg_fp64(A_pinned, b, x0=None, tol=1e-10, max_iter=20000):
+    """Jacobi-PCG in FP64 (orc_csr_pcg) from x0 to ||b - A x|| <= tol ||b||
+    (true residual).  Returns (x, iterations, true relative residual,
+    restarts)."""
+    import ctypes
+    from .mono import lib
+    L = lib()
+    if not hasattr(L, "_pcg_typed"):
+        P = ctypes.c_void_p
+        L.orc_csr_pcg.argtypes = [ctypes.c_int64, P, P, P, P, P, P, ctypes.c_double,
+                                  ctypes.c_int64, P]
+        L.orc_csr_pcg.restype = ctypes.c_int
+        L._pcg_typed = True
+    A = sp.csr_matrix(A_pinned)
+    ptr = np.ascontiguousarray(A.indptr, np.int64)
+    idx = np.ascontiguousarray(A.indices, np.int32)
+    val = np.ascontiguousarray(A.data, np.float64)
+    d = A.diagonal()
+    minv = np.where(np.abs(d) > 1e-30, 1.0 / np.where(d == 0, 1.0, d), 0.0)
+    bb = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.shape[0]) if x0 is None else np.array(x0, np.float64)
+    out = np.zeros(3)
+    c = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.orc_csr_pcg(A.shape[0], c(ptr), c(idx), c(val), c(minv), c(bb), c(x), float(tol),
+                       int(max_iter), c(out))
+    if rc != 0:
+        raise MemoryError("orc_csr_pcg: out of host memory")
+    return x, int(out[0]), float(out[1]), int(out[2])

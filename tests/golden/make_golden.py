@@ -29,6 +29,11 @@ Fixtures (all seeded, small enough to commit):
 * torso.npz         -- _assemble_stiffness / _find_surface_ids on a small
                        synthetic torso, build_heart_laplacian /
                        build_projection_map, and solve_frame on one Vm frame.
+* bspm_loop.npz     -- the upstream chain end to end: run_coupled (theta 0,
+                       FP64) writes vm_snapshots.npz of a 24x24x8 slab at
+                       0.5 mm (1 ms frames), run_bspm_loop solves every frame
+                       on the small torso of torso.npz and writes bspm.npz;
+                       both files' arrays (vm_*, out_*) and their dtypes.
 """
 from __future__ import annotations
 
@@ -271,6 +276,72 @@ def torso():
         phi_full_ref=phi_full, ref_iters=n_it)
 
 
+def bspm_case():
+    """Slab, stimulus and registration of bspm_loop (restated in the tests)."""
+    nx, ny, nz = 24, 24, 8
+    S = np.ones((nx, ny, nz), np.uint8)
+    phi = np.ones(S.shape, np.float32)
+    ect = np.zeros(S.shape, bool)
+    ect[:4, :4, :] = True
+    nodes, el, act = _stub(nx, ny, nz)
+    kw = dict(voxel_size=0.5, dx_p=0.25, sigma_P=0.0, sigma_M=0.13, Cm=0.01, A_P=133.33,
+              A_M=140.0, R_P=0.015, dt=0.02, T=12.0, theta=0.0,
+              stim_protocol=[dict(name="corner", target="ectopic", amp=0.52, dur=1.0,
+                                  onset=0.0)],
+              ectopic_region=ect, stim_len_mm=1.0, c_pmj=0.0, n_pmj=1)
+    reg = dict(R=np.eye(3), t=np.array([9.75, 7.5, 16.0]), scale=1.0, dice=0.9)
+    return (nodes, el, act, S, phi), kw, reg
+
+
+def bspm_loop():
+    btg = ref.build_torso_grid
+    cb = ref.compute_bspm
+    (nodes, el, act, S, phi), kw, reg = bspm_case()
+    lab = torso_case()
+    dx = 1.5
+    sig_map = {1: 0.2, 2: 0.05, 3: 0.7}
+    sigma = np.zeros(lab.shape)
+    for k, v in sig_map.items():
+        sigma[lab == k] = v
+    active = lab != 0
+    active_flat = np.where(active.ravel())[0].astype(np.int32)
+    id_map = np.full(lab.size, -1, np.int32)
+    id_map[active_flat] = np.arange(len(active_flat), dtype=np.int32)
+    A = btg._assemble_stiffness(sigma, dx * 1e-3, active, active_flat, id_map)
+    surf_flat, surf_rows = btg._find_surface_ids(lab, active, id_map)
+    interior = np.where(active.ravel())[0]
+    pin_row = int(id_map[int(interior[len(interior) // 2])])
+    origin = np.zeros(3)
+    grid = dict(shape=lab.shape, dx_mm=dx, origin_mm=origin, sigma_vol=sigma,
+                active_mask=active, tissue_mask=active, active_ids=active_flat,
+                active_id_map=id_map, surface_flat=surf_flat, surface_rows=surf_rows,
+                surface_xyz=btg.voxel_ids_to_xyz(surf_flat, lab.shape, dx, origin),
+                pin_row=pin_row, A_scipy=A, use_sbm=False)
+    out = {}
+    sync = torch.cuda.synchronize
+    torch.cuda.synchronize = lambda *a, **k: None     # the loop syncs CUDA after its warm-up
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            vm_path = Path(td) / "vm_snapshots.npz"
+            out_path = Path(td) / "bspm.npz"
+            quiet(ref.pipeline.run_coupled, nodes, el, act, S, S.copy(), phi, cg_tol=1e-12,
+                  cg_max_iter=200, n_frames=10, device="cpu", dtype=torch.float64,
+                  vm_save_dt=1.0, out_vm_npz=vm_path, **kw)
+            quiet(cb.run_bspm_loop, vm_path, grid, reg, 0.2625, 0.5, out_path, cg_tol_mV=1e-6,
+                  cg_max_iter=5000, cg_metric="rms", verbose=False)
+            for tag, path in (("vm", vm_path), ("out", out_path)):
+                z = np.load(path)
+                out[f"{tag}_keys"] = np.array(sorted(z.files))
+                out[f"{tag}_dtypes"] = np.array([str(z[k].dtype) for k in sorted(z.files)])
+                for k in z.files:
+                    out[f"{tag}_{k}"] = z[k]
+    finally:
+        torch.cuda.synchronize = sync
+    np.savez_compressed(HERE / "bspm_loop.npz", labels=lab, dx=dx,
+                        sigma_keys=np.array(list(sig_map)),
+                        sigma_vals=np.array(list(sig_map.values())), **out)
+
+
 def act_maps():
     """The upstream activation-map writer on upstream snapshots; keys are
     prefixed "slab_" (340 ms isotropic run, thresholds -20 / -60 mV) and
@@ -365,8 +436,9 @@ def pmj_exp4():
 
 if __name__ == "__main__":
     torch.set_num_threads(8)
-    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso"]
+    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso", "bspm"]
     for w in which:
         print("generating", w, flush=True)
         {"cells": ttp06_cells, "pacing": ttp06_pacing, "iso": mono_iso,
-         "aniso": mono_aniso, "maps": act_maps, "pmj": pmj_exp4, "torso": torso}[w]()
+         "aniso": mono_aniso, "maps": act_maps, "pmj": pmj_exp4, "torso": torso,
+         "bspm": bspm_loop}[w]()

@@ -135,3 +135,21 @@ def test_torso_operator_and_solution(golden):
     # the FP64 restatement of _pcg_gpu reproduces the solution and its stop
     xp, it, st = T.pcg_reference(T.pinned(A, pin), b, None, tol_mV=1e-7, max_iter=5000, metric="linf")
     assert st < 1e-7 and np.linalg.norm(xp - x) / np.linalg.norm(x) < 1e-6
+
+
+def test_in_loop_events_equal_snapshot_maps(golden):
+    """advance_events (chunked, every-step crossings) gives the same first
+    activation times as compute_activation_maps on every-step snapshots, and
+    the upstream fixture's; its frames are the snapshots at its cadence."""
+    g = golden("mono_iso.npz")
+    (nodes, el, act, S, phi), kw = cases.iso_case()
+    r = mono.run(nodes, el, act, S, phi, vm_save_dt=0.02, **kw)
+    a = mono.activation_maps(r["Vm"], r["time_vm"], -20.0, -20.0)["activation_times"][:, 0]
+    ctx = mono.setup(nodes, el, act, S, phi, vm_save_dt=None, **kw)
+    n = ctx["n_steps"]
+    first, fr, ft = mono.advance_events(ctx, n // 3, -20.0, frame_every=25, chunk=70)
+    first, fr2, ft2 = mono.advance_events(ctx, n - n // 3, -20.0, frame_every=25, chunk=130)
+    np.testing.assert_array_equal(first, a)
+    np.testing.assert_allclose(first, g["act"][:, 0], atol=1e-5)
+    np.testing.assert_array_equal(np.concatenate([fr, fr2]), r["Vm"][::25])
+    np.testing.assert_array_equal(np.concatenate([ft, ft2]), r["time_vm"][::25])

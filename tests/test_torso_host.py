@@ -52,3 +52,27 @@ def test_twelve_lead_definitions():
     assert np.allclose(L[0] + L[2], L[1])                      # Einthoven
     assert np.allclose(L[3] + L[4] + L[5], 0.0)                # augmented leads sum to zero
     assert np.allclose(L[6], 4.0 - (RA + LA + LL) / 3)
+
+
+def test_fp64_pcg_oracle_matches_direct_solve():
+    """The threaded FP64 Jacobi-CG of the oracle (the reference's _pcg_gpu
+    in FP64 with a relative true-residual stop) reaches the direct solve of
+    the pinned system, from zero and from a perturbed warm start; the CSR
+    pinning equals the reference's LIL pinning."""
+    lab, sigma_map, dx, vox, coords, reg, h, frames = torso_cases.random_case(shape=(24, 20, 28))
+    grid = torso_grid_from_labels(lab, sigma_map, dx)
+    A, _, _ = O.assemble_stiffness(grid["sigma_vol"], dx * 1e-3, grid["active_mask"])
+    pin = grid["pin_row"]
+    Ap = O.pinned_csr(A, pin)
+    assert abs(Ap - O.pinned(A, pin).tocsr()).max() == 0.0
+    proj, valid = T.projection_map(coords, reg["R"], reg["t"], 1.0, grid["origin_mm"], dx,
+                                   grid["active_id_map"], grid["shape"])
+    K = O.heart_laplacian(vox, len(vox))
+    b = O.frame_rhs(K, frames[1], proj.astype(np.int64), valid, A.shape[0], pin, 0.2625,
+                    h * 1e-3, dx)
+    xd = O.Solver(A, pin).solve(b)
+    for x0 in (None, xd * (1.0 + 1e-3 * np.sin(np.arange(len(xd))))):
+        x, it, rel, rst = O.pcg_fp64(Ap, b, x0, tol=1e-11)
+        assert rel <= 1e-11 and it > 0
+        assert np.linalg.norm(Ap @ x - b) <= 1e-11 * np.linalg.norm(b) * 1.0001
+        assert np.linalg.norm(x - xd) <= 1e-7 * np.linalg.norm(xd)
