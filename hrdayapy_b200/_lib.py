@@ -135,6 +135,10 @@ def _declare_optional(L):
                                          C.c_float, C.c_double, P, P]
     L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, P, P]
+    L.hp_conv3_wgrad_workspace.argtypes = [C.c_int32] * 5
+    L.hp_conv3_wgrad_workspace.restype = C.c_int64
+    L.hp_conv3_wgrad.argtypes = [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P,
+                                 P, P, C.c_int64, P, P]
 
 
 def check(status: int, what: str = ""):

@@ -5,6 +5,7 @@
 
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 namespace hp {
@@ -370,8 +371,9 @@ static hp_status get_encode() {
   return HP_OK;
 }
 
-// Tensor map over X[D][H][W][C] (bf16) with box (8 ch, 130 voxels, 1, 1).
-hp_status make_line_map(CUtensorMap* map, const void* X, int D, int H, int W, int Cch) {
+// Tensor map over X[D][H][W][C] (bf16) with box (8 ch, box_w voxels, 1, 1).
+hp_status make_line_map(CUtensorMap* map, const void* X, int D, int H, int W, int Cch,
+                        int box_w = LINE) {
   hp_status s = get_encode();
   if (s != HP_OK) return s;
   if (((uintptr_t)X & 15) != 0) {
@@ -381,7 +383,7 @@ hp_status make_line_map(CUtensorMap* map, const void* X, int D, int H, int W, in
   cuuint64_t dims[4] = {(cuuint64_t)Cch, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D};
   cuuint64_t strides[3] = {(cuuint64_t)Cch * 2, (cuuint64_t)W * Cch * 2,
                            (cuuint64_t)H * W * Cch * 2};
-  cuuint32_t box[4] = {8, (cuuint32_t)LINE, 1, 1};
+  cuuint32_t box[4] = {8, (cuuint32_t)box_w, 1, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)X, dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -460,6 +462,311 @@ hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y
   return HP_OK;
 }
 
+
+// -------------------------------------------------------------------------
+// Weight gradient of a 3x3x3 layer on the tensor cores:
+//   gw[co][ci][t] = sum_v G[v][co] X[v + off(t)][ci],  gb[co] = sum_v G[v][co]
+// as GEMMs with K = voxels.  The [voxel][8-channel] line tiles that TMA
+// brings in for the forward pass are, read transposed, MN-major UMMA
+// operands: a core matrix is 8 voxel rows (K) of 16 bytes (8 channels), K
+// groups 128 bytes apart, channel groups one tile chunk apart.  A CTA owns
+// one dz and a range of output lines (d, h, 128 voxels along W); per line
+// it loads the three input lines (d+dz, h-1..h+1) of X (130 voxels with the
+// halo, zero-filled outside the grid) as 3 CIN/8 chunk slots and the G line
+// as N/8 chunks.  The slots form M tiles of 128 rows (16 slots; rows past
+// the last slot read zeroed slots), and the three dx taps are the same tile
+// with the descriptor start moved by one voxel row (16 bytes), as in the
+// forward kernel.  Each (M tile, dx) accumulates over the CTA's lines in
+// its own TMEM columns (M = 128 rows, N = padded COUT, FP32).  The CTAs'
+// partial sums go to a workspace and a second kernel adds them in a fixed
+// order: the result does not depend on scheduling (no atomics).
+template <int CIN, int N>
+struct WgCfg {
+  static constexpr int G = CIN / 8;              // chunks per input line
+  static constexpr int S = 3 * G;                // loaded slots per line (dy = -1, 0, 1)
+  static constexpr int T = (S + 15) / 16;        // M tiles of 128 rows
+  static constexpr int A_BYTES = 16 * T * CHUNK;
+  static constexpr int A_TX = S * LINE * 16;
+  static constexpr int B_BYTES = (N / 8) * TILE_M * 16;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int SMEM = 2 * STAGE + 128;
+  static constexpr int ACC = 3 * T * N;          // TMEM columns of the accumulators
+  static constexpr uint32_t COLS =
+      ACC <= 32 ? 32 : (ACC <= 64 ? 64 : (ACC <= 128 ? 128 : (ACC <= 256 ? 256 : 512)));
+  // BF16 x BF16 -> FP32, M = 128, both operands MN-major (bits 15 and 16)
+  static constexpr uint32_t IDESC = idesc_bf16(TILE_M, N) | (1u << 15) | (1u << 16);
+  static_assert(CIN % 8 == 0 && N % 16 == 0 && N <= 256, "channel counts");
+  static_assert(ACC <= 512, "TMEM columns");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+  static_assert(A_BYTES % 128 == 0 && B_BYTES % 128 == 0, "stage alignment");
+};
+
+template <int CIN, int N>
+__global__ void __launch_bounds__(128)
+wgrad3_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmG,
+                 int D, int H, int WT, int lines_per_cta, float* __restrict__ part, int* err) {
+  using C = WgCfg<CIN, N>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ __align__(8) uint64_t empty[2];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int failed;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int dz = (int)blockIdx.y - 1;
+  const int nl = D * H * WT;
+  const int l0 = blockIdx.x * lines_per_cta;
+  const int l1 = min(nl, l0 + lines_per_cta);
+
+  // the slots past the loaded ones are read by the last M tile: zero them
+  // in both stages (the TMA never writes them)
+  for (int buf = 0; buf < 2; ++buf) {
+    uint4* z = (uint4*)(smem + buf * C::STAGE + C::S * CHUNK);
+    const int n16 = (16 * C::T - C::S) * CHUNK / 16;
+    for (int q = tid; q < n16; q += 128) z[q] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  fence_proxy_async();
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(&done, 1);
+    failed = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(&tmem_base, C::COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  const int nmine = max(0, l1 - l0);
+
+  if (tid == 0 && nmine > 0) {
+    auto issue = [&](int li, int buf) {
+      const int wt = li % WT, h = (li / WT) % H, d = li / (WT * H);
+      uint8_t* A = smem + buf * C::STAGE;
+      uint8_t* B = A + C::A_BYTES;
+      mbar_expect_tx(&full[buf], C::A_TX + C::B_BYTES);
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int g = 0; g < C::G; ++g)
+          tma_load_4d(A + (dy * C::G + g) * CHUNK, &tmX, g * 8, wt * TILE_M - 1, h + dy - 1,
+                      d + dz, &full[buf]);
+#pragma unroll
+      for (int g = 0; g < N / 8; ++g)
+        tma_load_4d(B + g * TILE_M * 16, &tmG, g * 8, wt * TILE_M, h, d, &full[buf]);
+    };
+    int issued = 0, consumed = 0;
+    issue(l0, 0);
+    issued = 1;
+    if (nmine > 1) {
+      issue(l0 + 1, 1);
+      issued = 2;
+    }
+    for (int s = 0; s < nmine; ++s) {
+      const int buf = s & 1;
+      const uint32_t par = (s >> 1) & 1;
+      if (!mbar_wait(&full[buf], par)) {
+        atomicOr(err, 8);
+        failed = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(smem + buf * C::STAGE);
+      const uint32_t b0 = a0 + C::A_BYTES;
+#pragma unroll
+      for (int t = 0; t < C::T; ++t) {
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+          for (int k = 0; k < TILE_M / 16; ++k) {
+            const uint64_t ad = smem_desc(a0 + 16 * t * CHUNK + dx * 16 + k * 256, 128, CHUNK);
+            const uint64_t bd = smem_desc(b0 + k * 256, 128, TILE_M * 16);
+            mma_bf16(tmem + (uint32_t)((t * 3 + dx) * N), ad, bd, C::IDESC, (s | k) != 0);
+          }
+        }
+      }
+      mma_commit(&empty[buf]);
+      consumed = s + 1;
+      if (s + 2 < nmine) {
+        if (!mbar_wait(&empty[buf], par)) {
+          atomicOr(err, 16);
+          failed = 1;
+          break;
+        }
+        issue(l0 + s + 2, buf);
+        ++issued;
+      }
+    }
+    if (failed) {
+      for (int s = consumed; s < issued; ++s) (void)mbar_wait(&full[s & 1], (s >> 1) & 1);
+    }
+  }
+  if (tid == 0) mma_commit(&done);
+  __syncthreads();
+  const bool ok = mbar_wait(&done, 0) && !failed;
+  if (!ok && tid == 0) atomicOr(err, 32);
+  tc_fence_after();
+  // epilogue: TMEM lane tid = GEMM row tid of every (M tile, dx)
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  const int64_t base = ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * (C::T * 3);
+#pragma unroll 1
+  for (int q = 0; q < C::T * 3; ++q) {
+    float* dst = part + ((base + q) * TILE_M + tid) * N;
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      float v[16];
+      if (ok && nmine > 0) {
+        tmem_ld16(trow + (uint32_t)(q * N + c0), v);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) v[u] = 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 16; u += 4) *(float4*)(dst + c0 + u) = make_float4(v[u], v[u + 1], v[u + 2], v[u + 3]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, C::COLS);
+}
+
+// Per-block partial sums of G over voxels (bias gradient), fixed order:
+// thread (r, co) sums voxels r, r + R, ... of the block's range, then the
+// block adds its R rows in order.
+constexpr int GS_BLOCKS = 256;
+__global__ void __launch_bounds__(256)
+gsum_partial_kernel(const __nv_bfloat16* __restrict__ G, int64_t n, int coP, float* __restrict__ part) {
+  __shared__ float sh[256];
+  const int R = 256 / coP;
+  const int r = threadIdx.x / coP, co = threadIdx.x % coP;
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t v0 = blockIdx.x * chunk, v1 = min(n, v0 + chunk);
+  float acc = 0.0f;
+  if (r < R)
+    for (int64_t v = v0 + r; v < v1; v += R) acc += __bfloat162float(G[v * coP + co]);
+  sh[threadIdx.x] = r < R ? acc : 0.0f;
+  __syncthreads();
+  if (threadIdx.x < coP) {
+    float s = 0.0f;
+    for (int q = 0; q < R; ++q) s += sh[q * coP + threadIdx.x];
+    part[(int64_t)blockIdx.x * coP + threadIdx.x] = s;
+  }
+}
+
+// gw[co][ci][t] and gb[co] from the partials, each summed in CTA order.
+template <int CIN, int N>
+__global__ void __launch_bounds__(256)
+wgrad_reduce_kernel(const float* __restrict__ part, int nchunk, const float* __restrict__ gpart,
+                    int cout, float* __restrict__ gw, float* __restrict__ gb) {
+  using C = WgCfg<CIN, N>;
+  const int64_t nw = (int64_t)cout * CIN * 27;
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e < nw) {
+    const int t = (int)(e % 27), ci = (int)((e / 27) % CIN), co = (int)(e / (27 * CIN));
+    const int dzi = t / 9, dy = (t / 3) % 3, dx = t % 3;
+    const int slot = dy * C::G + ci / 8;
+    const int mt = slot / 16, row = (slot % 16) * 8 + ci % 8;
+    float s = 0.0f;
+    for (int c = 0; c < nchunk; ++c) {
+      const int64_t q = ((int64_t)dzi * nchunk + c) * (C::T * 3) + mt * 3 + dx;
+      s += part[(q * TILE_M + row) * N + co];
+    }
+    gw[e] = s;
+  } else if (e < nw + cout) {
+    const int co = (int)(e - nw);
+    float s = 0.0f;
+    for (int b = 0; b < GS_BLOCKS; ++b) s += gpart[(int64_t)b * N + co];
+    gb[co] = s;
+  }
+}
+
+static int wg_chunks(int nl) {
+  // about two CTAs per SM over the three dz slices, at least one line each
+  const int target = 100;
+  const int per = std::max(1, (nl + target - 1) / target);
+  return (nl + per - 1) / per;
+}
+
+int64_t wgrad3_workspace(int D, int H, int W, int cin, int cout) {
+  const int N = cout < 16 ? 16 : cout;
+  const int T = (3 * (cin / 8) + 15) / 16;
+  const int nl = D * H * std::max(1, W / TILE_M);
+  return (int64_t)3 * wg_chunks(nl) * T * 3 * TILE_M * N * 4 + (int64_t)GS_BLOCKS * N * 4;
+}
+
+typedef void (*WgFn)(CUtensorMap, CUtensorMap, int, int, int, int, float*, int*);
+typedef void (*WgRedFn)(const float*, int, const float*, int, float*, float*);
+struct WgEntry {
+  int cin, n, smem;
+  WgFn fn;
+  WgRedFn red;
+};
+#define HP_WG(ci, n) {ci, n, WgCfg<ci, n>::SMEM, wgrad3_tc_kernel<ci, n>, wgrad_reduce_kernel<ci, n>}
+static const WgEntry kWg[] = {
+    HP_WG(16, 16), HP_WG(16, 32), HP_WG(32, 32), HP_WG(32, 64), HP_WG(64, 64), HP_WG(96, 32),
+    HP_WG(48, 16), HP_WG(32, 16), HP_WG(64, 32),
+};
+#undef HP_WG
+
+hp_status wgrad3_launch(const void* X, const void* G, int D, int H, int W, int cin, int cout,
+                        float* gw, float* gb, void* work, int64_t work_bytes, int* err,
+                        cudaStream_t s) {
+  const int N = cout < 16 ? 16 : cout;
+  const WgEntry* e = nullptr;
+  for (const auto& c : kWg)
+    if (c.cin == cin && c.n == N) e = &c;
+  if (!e) {
+    hp::set_error("weight gradient %d->%d is not compiled", cin, cout);
+    return HP_ERR_UNSUPPORTED;
+  }
+  if (W % TILE_M != 0 || D < 1 || H < 1) {
+    hp::set_error("weight gradient grid W=%d must be a multiple of %d", W, TILE_M);
+    return HP_ERR_INVALID;
+  }
+  if (((uintptr_t)G & 15) || ((uintptr_t)work & 15)) {
+    hp::set_error("weight gradient buffers must be 16-byte aligned");
+    return HP_ERR_INVALID;
+  }
+  const int64_t need = wgrad3_workspace(D, H, W, cin, cout);
+  if (work_bytes < need) {
+    hp::set_error("weight gradient workspace of %lld bytes is below the %lld needed",
+                  (long long)work_bytes, (long long)need);
+    return HP_ERR_INVALID;
+  }
+  CUtensorMap mx, mg;
+  hp_status st = make_line_map(&mx, X, D, H, W, cin, LINE);
+  if (st != HP_OK) return st;
+  st = make_line_map(&mg, G, D, H, W, N, TILE_M);
+  if (st != HP_OK) return st;
+  static bool attr_set[sizeof(kWg) / sizeof(kWg[0])] = {false};
+  const int idx = (int)(e - kWg);
+  if (!attr_set[idx]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute((const void*)e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     e->smem));
+    attr_set[idx] = true;
+  }
+  const int WT = W / TILE_M;
+  const int nl = D * H * WT;
+  const int nchunk = wg_chunks(nl);
+  const int per = (nl + nchunk - 1) / nchunk;
+  float* part = (float*)work;
+  const int T = (3 * (cin / 8) + 15) / 16;
+  float* gpart = part + (int64_t)3 * nchunk * T * 3 * TILE_M * N;
+  e->fn<<<dim3(nchunk, 3), 128, e->smem, s>>>(mx, mg, D, H, WT, per, part, err);
+  HP_CUDA_TRY(cudaGetLastError());
+  gsum_partial_kernel<<<GS_BLOCKS, 256, 0, s>>>((const __nv_bfloat16*)G, (int64_t)D * H * W, N,
+                                                gpart);
+  HP_CUDA_TRY(cudaGetLastError());
+  const int64_t nout = (int64_t)cout * cin * 27 + cout;
+  e->red<<<(unsigned)((nout + 255) / 256), 256, 0, s>>>(part, nchunk, gpart, cout, gw, gb);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 }  // namespace tc
 }  // namespace hp
 
@@ -474,4 +781,18 @@ extern "C" hp_status hp_conv3_forward(const void* X, const void* Wp, const float
   HP_REQUIRE(epi != hp::tc::EPI_MASK || mask, "hp_conv3_forward: mask epilogue needs mask");
   return hp::tc::conv3_launch(X, Wp, bias, Y, mask, D, H, W, cin, cout, epi, err,
                               (cudaStream_t)stream);
+}
+
+extern "C" int64_t hp_conv3_wgrad_workspace(int32_t D, int32_t H, int32_t W, int32_t cin,
+                                            int32_t cout) {
+  if (D < 1 || H < 1 || W < 1 || cin < 8 || cout < 1) return -1;
+  return hp::tc::wgrad3_workspace(D, H, W, cin, cout);
+}
+
+extern "C" hp_status hp_conv3_wgrad(const void* X, const void* G, int32_t D, int32_t H, int32_t W,
+                                    int32_t cin, int32_t cout, float* gw, float* gb, void* work,
+                                    int64_t work_bytes, int32_t* err, void* stream) {
+  HP_REQUIRE(X && G && gw && gb && work && err, "hp_conv3_wgrad: null argument");
+  return hp::tc::wgrad3_launch(X, G, D, H, W, cin, cout, gw, gb, work, work_bytes, err,
+                               (cudaStream_t)stream);
 }

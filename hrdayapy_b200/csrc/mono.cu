@@ -976,17 +976,25 @@ __global__ void __launch_bounds__(BI * BJ * BK) cn_pass_kernel(MonoArgs a, CnArg
 
 constexpr int ION_THREADS = 128;
 
+// 8-byte access to two adjacent floats as one packed pair
+__device__ __forceinline__ F2 ld_pair(const float* p) {
+  return F2{*(const unsigned long long*)p};
+}
+__device__ __forceinline__ void st_pair(float* p, F2 v) { *(unsigned long long*)p = v.x; }
+
 // The split step keeps the 18 TTP06 states in compact tissue order (index
-// i of active_slot, not the slot), so the ionic half's state loads and
-// stores are fully coalesced; tag, V and W stay per slot for the stencil.
-// mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
+// i of active_slot, not the slot; row stride n_active_pad, a multiple of 32),
+// so the ionic half's state loads and stores are fully coalesced; tag, V and
+// W stay per slot for the stencil.  Each thread advances two cells (compact
+// indices 2t, 2t + 1, or two Purkinje nodes) with the packed-FP32 TTP06: its
+// state moves as 8-byte pairs.
 // mode 0: the ionic half of step i+1 on V_{i+1} = Vpost; mode 1: the
 // prologue, the ionic half of step 0 on V_0 into W_0; mode 2: the end of a
 // theta-scheme step, V_{i+1} = clamp(x) with the outputs of step i recorded
 // exactly as the explicit step records them, then the ionic half of step
 // i+1 on it.
 template <int mode>
-__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+__global__ void __launch_bounds__(ION_THREADS, 4) mono_ionic_kernel(MonoArgs a, int step_off) {
   __shared__ int64_t s_vm_frame, s_anim_frame;
   const int64_t step = *a.d_step + step_off;
   if constexpr (mode == 2) {
@@ -998,41 +1006,85 @@ __global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, 
   }
   const bool odd = step & 1;
   const int64_t istep = mode == 1 ? 0 : step + 1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < a.n_active) {
-    const int64_t slot = a.active_slot[i];
-    const uint32_t tag = a.tag[slot];
-    float Vn;
-    if constexpr (mode == 2) {
-      Vn = fminf(fmaxf(a.cn_x[slot], -150.0f), 80.0f);
-      voxel_outputs(a, slot, tag, Vn, a.Vpost[slot], step, s_vm_frame, s_anim_frame);
-    } else {
-      Vn = a.Vpost[slot];
-    }
-    const int64_t na = a.n_active;
-    CellState cs;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = 2 * t;
+  if (i0 < a.n_active) {
+    const int nl = i0 + 1 < a.n_active ? 2 : 1;  // valid lanes
+    int64_t slot[2];
+    uint32_t tag[2];
+    float Vn[2];
+    int var[2];
+    CellParams cp[2];
 #pragma unroll
-    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + i];
-    const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
-    const CellParams cp = pheno_params(tag & HP_TAG_PHENO_MASK, a.var_gks[var], a.var_gkr[var]);
-    const float Iion = ttp06_step(Vn, cs, a.dt, cp);
-#pragma unroll
-    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
-    const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
-    float* __restrict__ Wout = mode == 1 ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
-    Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
-  } else {
-    const int p = i - a.n_active_pad;
-    if (p >= 0 && p < a.n_pk) {
-      float Vn;
+    for (int l = 0; l < 2; ++l) {
+      slot[l] = a.active_slot[l < nl ? i0 + l : i0];
+      tag[l] = a.tag[slot[l]];
       if constexpr (mode == 2) {
-        Vn = fminf(fmaxf(a.cn_x[a.n_slots + p], -150.0f), 80.0f);
-        a.pk_Vpost[p] = Vn;
-        if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p] = Vn;
+        Vn[l] = fminf(fmaxf(a.cn_x[slot[l]], -150.0f), 80.0f);
+        if (l < nl)
+          voxel_outputs(a, slot[l], tag[l], Vn[l], a.Vpost[slot[l]], step, s_vm_frame,
+                        s_anim_frame);
       } else {
-        Vn = a.pk_Vpost[p];
+        Vn[l] = a.Vpost[slot[l]];
       }
-      purkinje_ionic(a, p, Vn, istep, mode == 1 ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
+      var[l] = a.brick_variant ? a.brick_variant[slot[l] >> a.bv_shift] : 0;
+      cp[l] = pheno_params(tag[l] & HP_TAG_PHENO_MASK, a.var_gks[var[l]], a.var_gkr[var[l]]);
+    }
+    // a lone last cell fills lane 1 with itself; its state pair stays in the
+    // row's padding (i0 + 1 < n_active_pad)
+    const int64_t na = a.n_active_pad;
+    CellStateT<F2> cs;
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) cs.v[v] = ld_pair(a.state + (int64_t)v * na + i0);
+    const F2 I = ttp06_step2(pack2(Vn[0], Vn[1]), cs, a.dt, cp[0], cp[1]);
+#pragma unroll
+    for (int v = 0; v < N_STATE; ++v) st_pair(a.state + (int64_t)v * na + i0, cs.v[v]);
+    float* __restrict__ Wout = mode == 1 ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      if (l < nl) {
+        const float Iion = lane(I, l);
+        const float Is = stim_current(a, tag[l] >> HP_TAG_STIM_SHIFT, istep, var[l]);
+        Wout[slot[l]] = Vn[l] + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
+      }
+    }
+  } else {
+    const int p0 = 2 * (t - a.n_active_pad / 2);
+    if (p0 >= 0 && p0 < a.n_pk) {
+      const int nl = p0 + 1 < a.n_pk ? 2 : 1;
+      int p[2] = {p0, nl == 2 ? p0 + 1 : p0};
+      float Vn[2];
+      int var[2];
+      CellParams cp[2];
+      CellStateT<F2> cs;
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        if constexpr (mode == 2) {
+          Vn[l] = fminf(fmaxf(a.cn_x[a.n_slots + p[l]], -150.0f), 80.0f);
+          if (l < nl) {
+            a.pk_Vpost[p[l]] = Vn[l];
+            if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p[l]] = Vn[l];
+          }
+        } else {
+          Vn[l] = a.pk_Vpost[p[l]];
+        }
+        var[l] = a.pk_variant ? a.pk_variant[p[l]] : 0;
+        cp[l] = pheno_params(1, a.var_gks[var[l]], a.var_gkr[var[l]]);  // Purkinje -> endo
+      }
+#pragma unroll
+      for (int v = 0; v < N_STATE; ++v)
+        cs.v[v] = pack2(a.pk_state[(int64_t)v * a.n_pk + p[0]], a.pk_state[(int64_t)v * a.n_pk + p[1]]);
+      const F2 I = ttp06_step2(pack2(Vn[0], Vn[1]), cs, a.dt, cp[0], cp[1]);
+      float* __restrict__ Wout = mode == 1 ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1);
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        if (l < nl) {
+#pragma unroll
+          for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p[l]] = lane(cs.v[v], l);
+          const float Is = stim_current(a, a.pk_stim[p[l]], istep, var[l]);
+          Wout[p[l]] = Vn[l] + a.dt_over_Cm * (-(lane(I, l) * a.Cm) + Is);
+        }
+      }
     }
   }
 }
@@ -1386,7 +1438,8 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   h->diff = d->anisotropic ? se->diff_aniso : se->diff_iso;
   // states in compact tissue order (resting state, as for the slot order)
   if (!act.empty())
-    init_cells_kernel<<<1024, 256, 0, s>>>(h->a.state, h->a.Vpost, (int64_t)act.size(), d->v0);
+    init_cells_kernel<<<1024, 256, 0, s>>>(h->a.state, h->a.Vpost, (int64_t)h->a.n_active_pad,
+                                           d->v0);
   HP_CUDA_TRY(cudaGetLastError());
   // diffusion half: persistent CTAs over bricks, halo copy table per shape
   const std::vector<uint32_t> tab = se->halo(d->anisotropic != 0);
@@ -1411,7 +1464,9 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   h->diff_smem = smem;
   const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   h->diff_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
-  h->ion_grid = (h->a.n_active_pad + h->a.n_pk + ION_THREADS - 1) / ION_THREADS;
+  // two cells per thread: n_active_pad / 2 threads for the tissue, then the
+  // Purkinje pairs
+  h->ion_grid = (h->a.n_active_pad / 2 + (h->a.n_pk + 1) / 2 + ION_THREADS - 1) / ION_THREADS;
   return HP_OK;
 }
 
@@ -1953,12 +2008,13 @@ extern "C" hp_status hp_mono_copy_state(HpMono* h, float* st_slots, float* st_pk
     if (h->diff) {
       // the split step stores states in compact tissue order: scatter to slots
       HP_CUDA_TRY(cudaStreamSynchronize(s));
-      const int64_t ns = h->a.n_slots, na = h->a.n_active;
+      // (rows of stride n_active_pad)
+      const int64_t ns = h->a.n_slots, na = h->a.n_active, nr = h->a.n_active_pad;
       std::vector<int32_t> act(na);
       if (na) HP_CUDA_TRY(cudaMemcpy(act.data(), h->a.active_slot, na * 4, cudaMemcpyDeviceToHost));
       std::vector<float> tmp((size_t)N_STATE * na);
       for (int v = 0; v < N_STATE; ++v)
-        std::copy(st_slots + (size_t)v * na, st_slots + (size_t)(v + 1) * na, tmp.begin() + (size_t)v * na);
+        std::copy(st_slots + (size_t)v * nr, st_slots + (size_t)v * nr + na, tmp.begin() + (size_t)v * na);
       for (int v = 0; v < N_STATE; ++v) {
         float* dst = st_slots + (size_t)v * ns;
         std::fill(dst, dst + ns, 0.0f);

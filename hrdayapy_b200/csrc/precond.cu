@@ -23,8 +23,10 @@
 // keeps the 128-voxel W lines the convolution tiles on, and skip
 // concatenation.  It is trained on the GPU by its own kernels: forward,
 // data gradients through the same tensor-core convolution with flipped and
-// transposed weights (ReLU masks fused in its epilogue), weight gradients on
-// the CUDA cores, and Adam on FP32 master weights.  Loss: the fraction of
+// transposed weights (ReLU masks fused in its epilogue), weight gradients
+// on the tensor cores too (implicit GEMM over voxels, csrc/conv.cu, partial
+// sums added in a fixed order, so training is bit-reproducible), and Adam
+// on FP32 master weights.  Loss: the fraction of
 // the error's energy that one optimal step along M(r) leaves, for the
 // residual / error pairs (r, e) the plain solver's iterates give.
 #include "hp_common.cuh"
@@ -466,89 +468,6 @@ __global__ void __launch_bounds__(TB) energy_grad_kernel(EnergyArgs a, Dims cd, 
   if (blockIdx.x == 0 && threadIdx.x == 0) loss[0] = 1.0 - rz * rz / (zaz * re);
 }
 
-// Weight gradient of one 3x3x3 layer on the CUDA cores (FP32 accumulation):
-//   gw[co][ci][t] += sum_v X[v + off(t)][ci] * G[v][co],  gb[co] += sum_v G[v][co] (t = 13)
-// grid.x = 27 taps, grid.y = voxel chunks; each thread owns a 4 x 4 block of
-// (ci, co) pairs; voxel tiles of 32 are staged in shared memory as FP32.
-constexpr int WG_T = 32;
-__global__ void __launch_bounds__(TB)
-wgrad_kernel(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ G, Dims dm,
-             int cin, int cout, int coP, float* __restrict__ gw, float* __restrict__ gb) {
-  extern __shared__ float wsm[];
-  float* xs = wsm;                       // [WG_T][cin]
-  float* gs = wsm + WG_T * cin;          // [WG_T][cout]
-  const int t = blockIdx.x;
-  const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-  const int64_t n = dm.n();
-  const int64_t chunk = (n + gridDim.y - 1) / gridDim.y;
-  const int64_t v0 = blockIdx.y * chunk, v1 = min(n, v0 + chunk);
-  const int nci = cin / 4, nco = (cout + 3) / 4;
-  const int npair = nci * nco;
-  float acc[2][16];
-  float bacc[2] = {0.0f, 0.0f};
-#pragma unroll
-  for (int p = 0; p < 2; ++p)
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc[p][q] = 0.0f;
-  for (int64_t vt = v0; vt < v1; vt += WG_T) {
-    __syncthreads();
-    for (int q = threadIdx.x; q < WG_T * cin; q += TB) {
-      const int vv = q / cin, ci = q % cin;
-      const int64_t v = vt + vv;
-      float xv = 0.0f;
-      if (v < v1) {
-        const int w = v % dm.W, h = (v / dm.W) % dm.H, d = (int)(v / ((int64_t)dm.W * dm.H));
-        const int dd = d + dz, hh = h + dy, ww = w + dx;
-        if (dd >= 0 && dd < dm.D && hh >= 0 && hh < dm.H && ww >= 0 && ww < dm.W)
-          xv = __bfloat162float(X[(((int64_t)dd * dm.H + hh) * dm.W + ww) * cin + ci]);
-      }
-      xs[q] = xv;
-    }
-    for (int q = threadIdx.x; q < WG_T * cout; q += TB) {
-      const int vv = q / cout, co = q % cout;
-      const int64_t v = vt + vv;
-      gs[q] = v < v1 ? __bfloat162float(G[v * coP + co]) : 0.0f;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      const int pair = threadIdx.x + p * TB;
-      if (pair < npair) {
-        const int cb = (pair / nco) * 4, ob = (pair % nco) * 4;
-        for (int vv = 0; vv < WG_T; ++vv) {
-          float xv[4], gv[4];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) xv[a] = xs[vv * cin + cb + a];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) gv[b] = ob + b < cout ? gs[vv * cout + ob + b] : 0.0f;
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[p][a * 4 + b] += xv[a] * gv[b];
-        }
-      }
-    }
-    if (t == 13) {
-      for (int co = threadIdx.x; co < cout; co += TB)
-        for (int vv = 0; vv < WG_T; ++vv) bacc[co / TB] += gs[vv * cout + co];
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    const int pair = threadIdx.x + p * TB;
-    if (pair < npair) {
-      const int cb = (pair / nco) * 4, ob = (pair % nco) * 4;
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (ob + b < cout) atomicAdd(&gw[((int64_t)(ob + b) * cin + cb + a) * 27 + t], acc[p][a * 4 + b]);
-    }
-  }
-  if (t == 13)
-    for (int co = threadIdx.x; co < cout; co += TB) atomicAdd(&gb[co], bacc[co / TB]);
-}
-
 // Adam on the flat parameter vector
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps,
@@ -588,6 +507,8 @@ struct HpPrecond {
   __nv_bfloat16* wp[NL];
   __nv_bfloat16* wpt[NL];
   float* zero_bias;          // 96 zeros
+  float* wg_work;            // weight-gradient partial sums (largest layer)
+  int64_t wg_bytes;
   // activations
   __nv_bfloat16 *geo, *feat, *e1a, *e1b, *p1, *e2a, *e2b, *p2, *e3a, *e3b, *u2, *d2a, *d2b, *u1,
       *d1a, *d1b;
@@ -842,6 +763,12 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
   }
   PC_TRY(pal(h, &h->zero_bias, 96));
   HP_CUDA_TRY(cudaMemsetAsync(h->zero_bias, 0, 96 * 4, s));
+  h->wg_bytes = 0;
+  for (int l = 0; l < NL; ++l) {
+    const Dims dm = h->L[LLEV[l]];
+    h->wg_bytes = std::max(h->wg_bytes, tc::wgrad3_workspace(dm.D, dm.H, dm.W, LCIN[l], LCOUT[l]));
+  }
+  PC_TRY(pal(h, &h->wg_work, (h->wg_bytes + 3) / 4));
   const int64_t n1 = h->L[1].n(), n2 = h->L[2].n(), n3 = h->L[3].n();
   PC_TRY(pal(h, &h->geo, n1 * 16));
   PC_TRY(pal(h, &h->feat, n1 * 16));
@@ -947,14 +874,13 @@ static hp_status dgrad(HpPrecond* h, int l, const __nv_bfloat16* gpre, __nv_bflo
                           padc(LCOUT[l]), LCIN[l], mask ? tc::EPI_MASK : tc::EPI_LINEAR, h->err, s);
 }
 
-static void wgrad(HpPrecond* h, int l, const __nv_bfloat16* X, const __nv_bfloat16* G,
-                  cudaStream_t s) {
+// weight and bias gradients of layer l on the tensor cores (tc::wgrad3_launch:
+// implicit GEMM over voxels, partial sums added in a fixed order)
+static hp_status wgrad(HpPrecond* h, int l, const __nv_bfloat16* X, const __nv_bfloat16* G,
+                       cudaStream_t s) {
   const Dims dm = h->L[LLEV[l]];
-  const int cin = LCIN[l], cout = LCOUT[l];
-  const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(64, dm.n() / 4096));
-  const size_t smem = (size_t)WG_T * (cin + cout) * 4;
-  wgrad_kernel<<<dim3(27, chunks), TB, smem, s>>>(X, G, dm, cin, cout, padc(cout),
-                                                  h->grad + h->off_w[l], h->grad + h->off_b[l]);
+  return tc::wgrad3_launch(X, G, dm.D, dm.H, dm.W, LCIN[l], LCOUT[l], h->grad + h->off_w[l],
+                           h->grad + h->off_b[l], h->wg_work, h->wg_bytes, h->err, s);
 }
 
 static int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(4096, (n + 255) / 256)); }
@@ -1061,35 +987,35 @@ extern "C" hp_status hp_precond_train_step(HpPrecond* h, const uint8_t* label, c
   HP_CUDA_TRY(cudaMemsetAsync(h->grad, 0, h->n_par * 4, s));
 #define BW(x) do { st = (x); if (st != HP_OK) return st; } while (0)
   // OUT (linear, 16 -> 1 padded to 16)
-  wgrad(h, OUT, h->d1b, h->gout, s);
+  BW(wgrad(h, OUT, h->d1b, h->gout, s));
   BW(dgrad(h, OUT, h->gout, h->g_d1b, h->d1b, s));          // -> dpre of D1B
-  wgrad(h, D1B, h->d1a, h->g_d1b, s);
+  BW(wgrad(h, D1B, h->d1a, h->g_d1b, s));
   BW(dgrad(h, D1B, h->g_d1b, h->g_d1a, h->d1a, s));         // -> dpre of D1A
-  wgrad(h, D1A, h->u1, h->g_d1a, s);
+  BW(wgrad(h, D1A, h->u1, h->g_d1a, s));
   BW(dgrad(h, D1A, h->g_d1a, h->g_u1, nullptr, s));         // d u1 (48)
   upcat_back_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_u1, h->g_d2b, h->g_e1b, L1, 32, 16);
   relu_mask_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_d2b, h->d2b, n2 * 32);
-  wgrad(h, D2B, h->d2a, h->g_d2b, s);
+  BW(wgrad(h, D2B, h->d2a, h->g_d2b, s));
   BW(dgrad(h, D2B, h->g_d2b, h->g_d2a, h->d2a, s));
-  wgrad(h, D2A, h->u2, h->g_d2a, s);
+  BW(wgrad(h, D2A, h->u2, h->g_d2a, s));
   BW(dgrad(h, D2A, h->g_d2a, h->g_u2, nullptr, s));         // d u2 (96)
   upcat_back_kernel<<<grid_for(n2 * 64), 256, 0, s>>>(h->g_u2, h->g_e3b, h->g_e2b, L2, 64, 32);
   relu_mask_kernel<<<grid_for(n3 * 64), 256, 0, s>>>(h->g_e3b, h->e3b, n3 * 64);
-  wgrad(h, E3B, h->e3a, h->g_e3b, s);
+  BW(wgrad(h, E3B, h->e3a, h->g_e3b, s));
   BW(dgrad(h, E3B, h->g_e3b, h->g_e3a, h->e3a, s));
-  wgrad(h, E3A, h->p2, h->g_e3a, s);
+  BW(wgrad(h, E3A, h->p2, h->g_e3a, s));
   BW(dgrad(h, E3A, h->g_e3a, h->g_p2, nullptr, s));
   pool_back_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_p2, h->g_e2b, L2, 32);
   relu_mask_kernel<<<grid_for(n2 * 32), 256, 0, s>>>(h->g_e2b, h->e2b, n2 * 32);
-  wgrad(h, E2B, h->e2a, h->g_e2b, s);
+  BW(wgrad(h, E2B, h->e2a, h->g_e2b, s));
   BW(dgrad(h, E2B, h->g_e2b, h->g_e2a, h->e2a, s));
-  wgrad(h, E2A, h->p1, h->g_e2a, s);
+  BW(wgrad(h, E2A, h->p1, h->g_e2a, s));
   BW(dgrad(h, E2A, h->g_e2a, h->g_p1, nullptr, s));
   pool_back_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_p1, h->g_e1b, L1, 16);
   relu_mask_kernel<<<grid_for(n1 * 16), 256, 0, s>>>(h->g_e1b, h->e1b, n1 * 16);
-  wgrad(h, E1B, h->e1a, h->g_e1b, s);
+  BW(wgrad(h, E1B, h->e1a, h->g_e1b, s));
   BW(dgrad(h, E1B, h->g_e1b, h->g_e1a, h->e1a, s));
-  wgrad(h, E1A, h->feat, h->g_e1a, s);
+  BW(wgrad(h, E1A, h->feat, h->g_e1a, s));
 #undef BW
   HP_CUDA_TRY(cudaGetLastError());
   if (lr > 0.0f) {

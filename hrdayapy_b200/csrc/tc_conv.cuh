@@ -186,6 +186,14 @@ hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y
                        const void* mask, int D, int H, int W, int cin, int cout, int epi,
                        int* err, cudaStream_t s);
 
+// Weight gradient of one layer (conv.cu): gw [cout][cin][27] and gb [cout]
+// (FP32, overwritten) from X [D][H][W][cin] and G [D][H][W][max(cout, 16)]
+// (bf16), partial sums in `work` (wgrad3_workspace bytes).
+int64_t wgrad3_workspace(int D, int H, int W, int cin, int cout);
+hp_status wgrad3_launch(const void* X, const void* G, int D, int H, int W, int cin, int cout,
+                        float* gw, float* gb, void* work, int64_t work_bytes, int* err,
+                        cudaStream_t s);
+
 template <int N>
 struct TmemCols {
   static constexpr uint32_t value = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));

@@ -320,6 +320,24 @@ hp_status hp_conv3_forward(const void *X, const void *Wp, const float *bias, voi
                            const void *mask, int32_t D, int32_t H, int32_t W, int32_t cin,
                            int32_t cout, int32_t epi, int32_t *err, void *stream);
 
+/*
+ * Weight and bias gradients of one 3x3x3 convolution (zero padding 1) on the
+ * tensor cores (no counterpart in the reference, which has no learned
+ * part): gw[co][ci][t] = sum_v G[v][co] X[v + off(t)][ci] (t = 9 kz + 3 ky
+ * + kx) and gb[co] = sum_v G[v][co], written (not accumulated) as FP32.
+ * X: device bf16 [D][H][W][cin]; G: device bf16 [D][H][W][max(cout, 16)]
+ * (the layer's output-gradient layout).  work: device scratch of at least
+ * hp_conv3_wgrad_workspace() bytes, 16-byte aligned, for the per-CTA
+ * partial sums, which a second kernel adds in a fixed order: the result is
+ * the same bit for bit on every run.  W must be a multiple of 128 and
+ * (cin, cout) among the compiled pairs.  *err (device int) receives nonzero
+ * if a bounded device wait expired.
+ */
+int64_t hp_conv3_wgrad_workspace(int32_t D, int32_t H, int32_t W, int32_t cin, int32_t cout);
+hp_status hp_conv3_wgrad(const void *X, const void *G, int32_t D, int32_t H, int32_t W,
+                         int32_t cin, int32_t cout, float *gw, float *gb, void *work,
+                         int64_t work_bytes, int32_t *err, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Learned torso preconditioner and flexible CG (no counterpart in the  */
 /* reference, whose torso solver is Jacobi-PCG only)                    */
