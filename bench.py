@@ -485,8 +485,10 @@ def run_ours(args):
                       "vm_range_mV": [float(vm_last.min()), float(vm_last.max())]},
         }
         if args.cpu_baseline:
+            pp = dataclasses.replace(prob, site_on=site_on_full)
+            pp.frame_steps = fs
             line["cpu_baseline"], line["check"]["parity"] = shell_parity_and_cpu_baseline(
-                dataclasses.replace(prob, site_on=site_on_full), args, parity_ms=args.parity_ms)
+                pp, args, parity_ms=args.parity_ms)
         if tune_table is not None:
             line["autotune"] = [{k: v for k, v in t.items()} for t in tune_table[:8]]
         if args.theta:
@@ -692,12 +694,13 @@ def shell_parity_and_cpu_baseline(prob, args, parity_ms=16.0, chunk=25):
     from hrdayapy_b200 import monodomain as M, synthetic
     from oracle import mono as orc
     n = int(round(parity_ms / prob.dt))
+    fs = int(getattr(prob, "frame_steps", 50))
     if len(prob.site_on) < n + 1:
         raise SystemExit("parity leg: stimulus table shorter than the parity window")
     p = dataclasses.replace(prob, n_steps=n, site_on=np.array(prob.site_on[:n + 1]), vm_every=0,
                             frame_every=0, act_threshold=-20.0, deact_threshold=-20.0)
     sim = M.MonoHandle(p)
-    sim.run(n, graph_chunk=prob.frame_steps)
+    sim.run(n, graph_chunk=fs)
     a, na, _, _ = sim.events()
     vm, vp = sim.voltage()
     sim.close()

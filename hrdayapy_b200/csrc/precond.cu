@@ -36,6 +36,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 namespace hp {
@@ -490,6 +491,7 @@ using namespace hp;
 using namespace hp::pc;
 
 struct HpPrecond {
+  uint64_t serial;           // unique for the process (handles may reuse an address)
   int ni, nj, nk;            // fine (unpadded) torso dims
   int pj, pk;
   int64_t ng, pin;
@@ -706,6 +708,8 @@ extern "C" hp_status hp_precond_create(const HpPrecondDesc* d, HpPrecond** out, 
   HP_REQUIRE(d->sigma && d->h_m > 0.0, "hp_precond_create: sigma and h_m are required");
   cudaStream_t s = (cudaStream_t)stream;
   HpPrecond* h = new HpPrecond();
+  static std::atomic<uint64_t> next_serial{0};
+  h->serial = ++next_serial;
   h->ni = d->ni; h->nj = d->nj; h->nk = d->nk;
   h->pj = d->nj + 2; h->pk = d->nk + 2;
   h->ng = (int64_t)(d->ni + 2) * h->pj * h->pk;
@@ -941,6 +945,8 @@ hp_status precond_forward(HpPrecond* h, const uint8_t* label, const float* invd,
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
+
+uint64_t precond_serial(const HpPrecond* h) { return h->serial; }
 
 hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
                         float* z, int use_net, cudaStream_t s) {

@@ -88,28 +88,29 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
-// Block-reduces NV sums (and optionally one max stored as v[NV-1] when
-// last_is_max) into part[blockIdx], then returns true in the one block that
-// arrived last, after which `tot` holds the grid totals in every thread of
-// that block.
+// Block-reduces NV values into part[blockIdx] -- slot q is a sum, or a max
+// where bit q of max_mask is set (identity -inf) -- then returns true in the
+// one block that arrived last, after which `tot` holds the grid totals in
+// every thread of that block.
 template <int NV>
-__device__ bool block_reduce_last(double (&v)[NV], bool last_is_max, double* part,
+__device__ bool block_reduce_last(double (&v)[NV], uint32_t max_mask, double* part,
                                   unsigned int* ticket, double (&tot)[NV]) {
   __shared__ double sh[TB / 32][NV];
   __shared__ bool am_last;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
-    double w = (last_is_max && q == NV - 1) ? (double)warp_max((float)v[q]) : warp_sum(v[q]);
+    const bool mx = (max_mask >> q) & 1u;
+    double w = mx ? (double)warp_max((float)v[q]) : warp_sum(v[q]);
     if (lane == 0) sh[wid][q] = w;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
+      const bool mx = (max_mask >> q) & 1u;
       double s = sh[0][q];
-      for (int w = 1; w < TB / 32; ++w)
-        s = (last_is_max && q == NV - 1) ? fmax(s, sh[w][q]) : s + sh[w][q];
+      for (int w = 1; w < TB / 32; ++w) s = mx ? fmax(s, sh[w][q]) : s + sh[w][q];
       part[(int64_t)blockIdx.x * NPART + q] = s;
     }
     __threadfence();
@@ -121,12 +122,12 @@ __device__ bool block_reduce_last(double (&v)[NV], bool last_is_max, double* par
   __threadfence();
   // the last block sums all partials in block order (deterministic)
 #pragma unroll
-  for (int q = 0; q < NV; ++q) v[q] = (last_is_max && q == NV - 1) ? 0.0 : 0.0;
+  for (int q = 0; q < NV; ++q) v[q] = ((max_mask >> q) & 1u) ? -INFINITY : 0.0;
   for (int blk = threadIdx.x; blk < (int)gridDim.x; blk += TB) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       const double pv = ((volatile double*)part)[(int64_t)blk * NPART + q];
-      v[q] = (last_is_max && q == NV - 1) ? fmax(v[q], pv) : v[q] + pv;
+      v[q] = ((max_mask >> q) & 1u) ? fmax(v[q], pv) : v[q] + pv;
     }
   }
   // fixed-order tree over the block
@@ -138,7 +139,7 @@ __device__ bool block_reduce_last(double (&v)[NV], bool last_is_max, double* par
     if ((int)threadIdx.x < s) {
 #pragma unroll
       for (int q = 0; q < NV; ++q)
-        sh2[threadIdx.x][q] = (last_is_max && q == NV - 1)
+        sh2[threadIdx.x][q] = ((max_mask >> q) & 1u)
                                   ? fmax(sh2[threadIdx.x][q], sh2[threadIdx.x + s][q])
                                   : sh2[threadIdx.x][q] + sh2[threadIdx.x + s][q];
     }
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
   if constexpr (PAIRS) spmv_lines(a, T, cell);
   else spmv_lines_single(a, T, cell);
   double tot[1];
-  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+  if (block_reduce_last<1>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double pAp = tot[0];
     a.scal[SC_PAP] = pAp;
     a.scal[SC_ALPHA_PREV] = 0.0;   // every block of part 1a applied the pending x update
@@ -363,14 +364,29 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
 
 // Iteration part 2: r -= alpha Ap, z = M^-1 r, partial r.z, z.z, r.r, max|z|;
 // the last block forms beta and tests the stopping rule.
+// P99 (the reference's 'p99' metric, compute_bspm.py:195-219): stop when the
+// 0.99 quantile of |z| over the rows, linearly interpolated between order
+// statistics as torch.quantile does, is below tol.  With N rows, position
+// pos = 0.99 (N - 1), lo = floor(pos), and c rows at or above tol (their
+// order statistics start at N - c), the quantile is below tol when lo + 1 <
+// N - c, not below when lo >= N - c, and otherwise (lo = N - c - 1) equals
+// m_lt + (pos - lo) (m_ge - m_lt) with m_lt the largest |z| below tol and
+// m_ge the smallest at or above it: three reductions decide it exactly.
+// The reported statistic is that value in the last case and otherwise
+// m_lt (an upper bound of the quantile, below tol) or m_ge (a lower bound,
+// not below tol).
+template <bool P99>
 __global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float alphaf = (float)alpha;
+  const float tolf = (float)a.scal[SC_TOL];
   const float* __restrict__ invd = a.invd;
   const float* __restrict__ Ap = a.Ap;
   float* __restrict__ rv = a.r;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  // sums r.z, z.z, r.r and max |z|; P99: r.z, count |z| >= tol, max of |z|
+  // below tol, max of -|z| at or above tol
+  double acc[4] = {0.0, 0.0, P99 ? 0.0 : 0.0, P99 ? -INFINITY : 0.0};
   constexpr int LB = 8;
   float rb[LB], ib[LB];
   for_line_batches<LB>(
@@ -380,30 +396,58 @@ __global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
         rv[g] = r;
         const float z = ib[u] * r;
         acc[0] += (double)r * z;
-        acc[1] += (double)z * z;
-        acc[2] += (double)r * r;
-        acc[3] = fmax(acc[3], (double)fabsf(z));
+        if constexpr (P99) {
+          const float az = fabsf(z);
+          if (az >= tolf) {
+            acc[1] += 1.0;
+            acc[3] = fmax(acc[3], -(double)az);
+          } else {
+            acc[2] = fmax(acc[2], (double)az);
+          }
+        } else {
+          acc[1] += (double)z * z;
+          acc[2] += (double)r * r;
+          acc[3] = fmax(acc[3], (double)fabsf(z));
+        }
       });
   double tot[4];
-  if (block_reduce_last<4>(acc, true, a.part, a.ticket, tot) && threadIdx.x == 0) {
+  if (block_reduce_last<4>(acc, P99 ? 12u : 8u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double rz_new = tot[0];
     a.scal[SC_BETA] = rz_new / a.scal[SC_RZ];
     a.scal[SC_RZ] = rz_new;
     a.scal[SC_ALPHA_PREV] = alpha;
-    a.scal[SC_ZZ] = tot[1];
-    a.scal[SC_RR] = tot[2];
-    a.scal[SC_ZMAX] = tot[3];
     const int it = ++a.iscal[IS_ITER];
     const int rule = a.iscal[IS_RULE];
     double stat;
-    if (rule == HP_STOP_RMS) stat = sqrt(tot[1] / (double)a.n_rows);
-    else if (rule == HP_STOP_LINF) stat = tot[3];
-    else stat = sqrt(tot[2] / fmax(a.scal[SC_BB], 1e-300));  // recursive estimate
+    bool below;
+    if constexpr (P99) {
+      const double N = (double)a.n_rows, c = tot[1], m_lt = tot[2], m_ge = -tot[3];
+      const double pos = 0.99 * (N - 1.0), lo = floor(pos);
+      const double first_ge = N - c;
+      if (lo + 1.0 < first_ge) {
+        stat = m_lt;
+        below = true;
+      } else if (lo >= first_ge) {
+        stat = m_ge;
+        below = false;
+      } else {
+        stat = m_lt + (pos - lo) * (m_ge - m_lt);
+        below = stat < a.scal[SC_TOL];
+      }
+    } else {
+      a.scal[SC_ZZ] = tot[1];
+      a.scal[SC_RR] = tot[2];
+      a.scal[SC_ZMAX] = tot[3];
+      if (rule == HP_STOP_RMS) stat = sqrt(tot[1] / (double)a.n_rows);
+      else if (rule == HP_STOP_LINF) stat = tot[3];
+      else stat = sqrt(tot[2] / fmax(a.scal[SC_BB], 1e-300));  // recursive estimate
+      // REL: stop the recursion a little below tol; the true residual decides
+      const double lim = rule == HP_STOP_REL ? 0.5 * a.scal[SC_TOL] : a.scal[SC_TOL];
+      below = stat < lim;
+    }
     a.scal[SC_STAT] = stat;
-    // REL: stop the recursion a little below tol; the true residual decides
-    const double lim = rule == HP_STOP_REL ? 0.5 * a.scal[SC_TOL] : a.scal[SC_TOL];
     if (!isfinite(rz_new)) { a.iscal[IS_NONFINITE] = 1; a.iscal[IS_DONE] = 1; }
-    else if (stat < lim || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
+    else if (below || it >= a.iscal[IS_MAXIT]) a.iscal[IS_DONE] = 1;
   }
 }
 
@@ -442,7 +486,7 @@ __global__ void __launch_bounds__(TB) true_residual(TorsoArgs a, int reset) {
     acc[2] += (double)rf * ((double)a.invd[g] * rf);
   }
   double tot[3];
-  if (block_reduce_last<3>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+  if (block_reduce_last<3>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_TRUE_RR] = tot[0];
     a.scal[SC_BB] = tot[1];
     if (reset) {
@@ -489,7 +533,7 @@ __global__ void __launch_bounds__(TB) src_laplacian(SrcArgs s) {
     acc[0] += (double)iv;
   }
   double tot[1];
-  if (block_reduce_last<1>(acc, false, s.part, s.ticket, tot) && threadIdx.x == 0)
+  if (block_reduce_last<1>(acc, 0u, s.part, s.ticket, tot) && threadIdx.x == 0)
     s.scal[SC_SRC_MEAN] = tot[0] / (double)fmax(1.0, (double)*s.mean_count);
 }
 
@@ -565,7 +609,10 @@ struct HpTorso {
   bool have_x;
   cudaGraphExec_t graph[2];
   cudaGraphExec_t fcg_graph[4];   // FCG chunk without the network / net every 1, 2, 4
-  const void* fcg_graph_pc;       // preconditioner handle the FCG graphs hold
+  // serial number of the preconditioner handle the FCG graphs hold (not its
+  // address: a destroyed handle's address can come back for a new one, whose
+  // buffers the old graphs do not point to)
+  uint64_t fcg_graph_pc;
   cudaStream_t fcg_graph_stream;
   int graph_chunk;
   cudaStream_t graph_stream;
@@ -660,7 +707,7 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   h->graph_chunk = 0;
   h->graph_stream = nullptr;
   for (int k = 0; k < 4; ++k) h->fcg_graph[k] = nullptr;
-  h->fcg_graph_pc = nullptr;
+  h->fcg_graph_pc = 0;
   h->fcg_graph_stream = nullptr;
   h->ni = ni; h->nj = nj; h->nk = nk;
   h->n_rows = n_rows;
@@ -700,7 +747,7 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     h->ap_fn = h->pairs ? pcg_ap<true> : pcg_ap<false>;
     h->fspmv_fn = h->pairs ? fcg_spmv<true> : fcg_spmv<false>;
     const void* fs[N_LINE_KERNELS] = {(const void*)pcg_p_update, (const void*)h->ap_fn,
-                                      (const void*)pcg_k2,       (const void*)h->fspmv_fn,
+                                      (const void*)pcg_k2<false>, (const void*)h->fspmv_fn,
                                       (const void*)fcg_update,   (const void*)fcg_beta,
                                       (const void*)fcg_p};
     for (int q = 0; q < N_LINE_KERNELS; ++q) {
@@ -815,24 +862,27 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
 
 extern "C" int64_t hp_torso_rows(const HpTorso* h) { return h ? h->n_rows : -1; }
 
-static hp_status iter_launch(HpTorso* h, int n, cudaStream_t s) {
+static hp_status iter_launch(HpTorso* h, int n, bool p99, cudaStream_t s) {
   for (int q = 0; q < n; ++q) {
     pcg_p_update<<<h->nblk_k[K_P_UPDATE], TB, 0, s>>>(h->a);
     h->ap_fn<<<h->nblk_k[K_AP], TB, 0, s>>>(h->a);
-    pcg_k2<<<h->nblk_k[K_K2], TB, 0, s>>>(h->a);
+    if (p99) pcg_k2<true><<<h->nblk_k[K_K2], TB, 0, s>>>(h->a);
+    else pcg_k2<false><<<h->nblk_k[K_K2], TB, 0, s>>>(h->a);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
 
-// CG iterations in chunks of `chunk` (one CUDA graph), with the
-// host reading the done flag once per chunk.  Kernels after convergence
-// inside a chunk return immediately.
-static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
+// CG iterations in chunks of `chunk` (one CUDA graph per stopping-rule
+// kernel: graph[1] for the p99 rule), with the host reading the done flag
+// once per chunk.  Kernels after convergence inside a chunk return
+// immediately.
+static hp_status run_iterations(HpTorso* h, int max_iter, bool p99, cudaStream_t s) {
   const int chunk = 8;
+  const int gi = p99 ? 1 : 0;
   if (s == nullptr) {    // the legacy default stream cannot be captured
     for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
-      hp_status st = iter_launch(h, chunk, s);
+      hp_status st = iter_launch(h, chunk, p99, s);
       if (st != HP_OK) return st;
       HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
       HP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -840,22 +890,26 @@ static hp_status run_iterations(HpTorso* h, int max_iter, cudaStream_t s) {
     }
     return HP_OK;
   }
-  if (!h->graph[0] || h->graph_stream != s) {
-    if (h->graph[0]) cudaGraphExecDestroy(h->graph[0]);
-    h->graph[0] = nullptr;
+  if (h->graph_stream != s) {
+    for (int k = 0; k < 2; ++k) {
+      if (h->graph[k]) cudaGraphExecDestroy(h->graph[k]);
+      h->graph[k] = nullptr;
+    }
+    h->graph_stream = s;
+  }
+  if (!h->graph[gi]) {
     cudaGraph_t g;
     HP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    hp_status st = iter_launch(h, chunk, s);
+    hp_status st = iter_launch(h, chunk, p99, s);
     cudaError_t ce = cudaStreamEndCapture(s, &g);
     if (st != HP_OK) return st;
     HP_CUDA_TRY(ce);
-    HP_CUDA_TRY(cudaGraphInstantiate(&h->graph[0], g, 0));
+    HP_CUDA_TRY(cudaGraphInstantiate(&h->graph[gi], g, 0));
     cudaGraphDestroy(g);
     h->graph_chunk = chunk;
-    h->graph_stream = s;
   }
   for (int done_it = 0; done_it < max_iter + chunk; done_it += chunk) {
-    HP_CUDA_TRY(cudaGraphLaunch(h->graph[0], s));
+    HP_CUDA_TRY(cudaGraphLaunch(h->graph[gi], s));
     HP_CUDA_TRY(cudaMemcpyAsync(h->h_iscal, h->a.iscal, N_ISCAL * 4, cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
     if (h->h_iscal[IS_DONE]) break;
@@ -923,7 +977,7 @@ static hp_status pcg_solve(HpTorso* h, double tol, int rule, int max_iter, HpSol
     if (total_it >= max_iter) { result = HP_ERR_NOT_CONVERGED; break; }
     int32_t is_run[N_ISCAL] = {0, 0, rule, max_iter - total_it, 0, 0};
     HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_run, sizeof(is_run), cudaMemcpyHostToDevice, s));
-    hp_status st = run_iterations(h, max_iter - total_it, s);
+    hp_status st = run_iterations(h, max_iter - total_it, rule == HP_STOP_P99, s);
     if (st != HP_OK) return st;
     st = read_scalars(h, s);
     if (st != HP_OK) return st;
@@ -990,7 +1044,7 @@ extern "C" hp_status hp_torso_solve_frame(HpTorso* h, const float* vm, int32_t v
                                           int32_t rule, int32_t max_iter, HpSolveStats* stats,
                                           void* stream) {
   HP_REQUIRE(h, "hp_torso_solve_frame: null handle");
-  HP_REQUIRE(rule >= 0 && rule <= 2, "hp_torso_solve_frame: unknown rule %d", rule);
+  HP_REQUIRE(rule >= 0 && rule <= 3, "hp_torso_solve_frame: unknown rule %d", rule);
   HP_REQUIRE(max_iter >= 1, "hp_torso_solve_frame: max_iter must be >= 1");
   HP_REQUIRE(tol > 0.0, "hp_torso_solve_frame: tol must be positive");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1024,6 +1078,7 @@ namespace hp {
 namespace pc {
 hp_status precond_apply(HpPrecond* h, const uint8_t* label, const float* invd, const float* r,
                         float* z, int use_net, cudaStream_t s);
+uint64_t precond_serial(const HpPrecond* h);
 }
 
 // q = A p (p in p0), partial p.q and p.r; last block: alpha = p.r / p.q.
@@ -1044,7 +1099,7 @@ __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
   if constexpr (PAIRS) spmv_lines(a, T, cell);
   else spmv_lines_single(a, T, cell);
   double tot[2];
-  if (block_reduce_last<2>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+  if (block_reduce_last<2>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_PAP] = tot[0];
     if (!(fabs(tot[0]) >= 1e-30) || !isfinite(tot[0])) {
       a.iscal[IS_BREAKDOWN] = isfinite(tot[0]) ? 1 : 0;
@@ -1083,7 +1138,7 @@ __global__ void __launch_bounds__(TB) fcg_update(TorsoArgs a) {
         acc[0] += (double)rb[u] * rb[u];
       });
   double tot[1];
-  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0) {
+  if (block_reduce_last<1>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_RR] = tot[0];
     const double stat = sqrt(tot[0] / fmax(a.scal[SC_BB], 1e-300));
     a.scal[SC_STAT] = stat;
@@ -1110,7 +1165,7 @@ __global__ void __launch_bounds__(TB) fcg_beta(TorsoArgs a) {
       a, [&](int u, int64_t g) { zb[u] = z[g]; qb[u] = Ap[g]; },
       [&](int u, int64_t) { acc[0] += (double)zb[u] * qb[u]; });
   double tot[1];
-  if (block_reduce_last<1>(acc, false, a.part, a.ticket, tot) && threadIdx.x == 0)
+  if (block_reduce_last<1>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0)
     a.scal[SC_BETA] = -tot[0] / a.scal[SC_PAP];
 }
 
@@ -1142,9 +1197,10 @@ constexpr int FCG_CHUNK = 4;
 // preconditioner that changes from one iteration to the next.
 static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s) {
   const int q = use_net == 0 ? 0 : (use_net == 1 ? 1 : (use_net == 2 ? 2 : 3));
-  if (h->fcg_graph[q] && h->fcg_graph_stream == s && h->fcg_graph_pc == (const void*)p)
+  const uint64_t serial = pc::precond_serial(p);
+  if (h->fcg_graph[q] && h->fcg_graph_stream == s && h->fcg_graph_pc == serial)
     return HP_OK;
-  if (h->fcg_graph_stream != s || h->fcg_graph_pc != (const void*)p) {
+  if (h->fcg_graph_stream != s || h->fcg_graph_pc != serial) {
     for (int k = 0; k < 4; ++k)
       if (h->fcg_graph[k]) { cudaGraphExecDestroy(h->fcg_graph[k]); h->fcg_graph[k] = nullptr; }
   }
@@ -1166,7 +1222,7 @@ static hp_status fcg_graph(HpTorso* h, HpPrecond* p, int use_net, cudaStream_t s
   HP_CUDA_TRY(cudaGraphInstantiate(&h->fcg_graph[q], g, 0));
   cudaGraphDestroy(g);
   h->fcg_graph_stream = s;
-  h->fcg_graph_pc = (const void*)p;
+  h->fcg_graph_pc = serial;
   return HP_OK;
 }
 

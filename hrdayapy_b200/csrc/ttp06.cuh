@@ -25,9 +25,10 @@
 //     denominators (m, Xr1, Xr2), log(a/b) is log(a) - log(b) with the
 //     constant's logarithm folded, and buffer factors 1/(1 + B K/(c+K)^2)
 //     are (c+K)^2 / ((c+K)^2 + B K);
-//   * exp2V - 1 in I_CaL is evaluated with expm1f, which is the same
-//     quantity with less cancellation near V = 15 mV (the reference's FP64
-//     has the digits to spare; FP32 does not), and exp2V as that plus one;
+//   * exp2V - 1 in I_CaL is evaluated as expm1 (the Taylor series near 0,
+//     expm1_t), which is the same quantity with less cancellation near
+//     V = 15 mV (the reference's FP64 has the digits to spare; FP32 does
+//     not), and exp2V as that plus one;
 //   * the special-function unit (SFU) and the FMA pipe share the
 //     exponentials: those of the Rush-Larsen factors (unbounded arguments)
 //     and of the K1 current (arguments through E_K) use the SFU's base-2
@@ -230,7 +231,13 @@ template <class T> __device__ __forceinline__ T log_sfu(T x) {
 __device__ __forceinline__ float exp2_scale(float p, float t) {
   return __uint_as_float(__float_as_uint(p) + (__float_as_uint(t) << 23));
 }
+#ifndef HP_EXP_FMA
+#define HP_EXP_FMA 1
+#endif
 template <class T> __device__ __forceinline__ T exp_fma(T x) {
+#if !HP_EXP_FMA
+  return exp_sfu(x);
+#endif
   constexpr float SHIFT = 12582912.0f;  // 1.5 * 2^23
   const T y = x * LOG2E_F;
   const T t = y + SHIFT;
@@ -241,6 +248,25 @@ template <class T> __device__ __forceinline__ T exp_fma(T x) {
   p = fma(p, f, bc<T>(6.931469440460205e-1f));
   p = fma(p, f, bc<T>(1.0000001192092896f));
   return map2(p, t, exp2_scale);
+}
+
+// exp(x) - 1 without cancellation near 0: the Taylor series to x^8 for
+// |x| <= 1/2 (truncation below 1.1e-8 relative), exp(x) - 1 beyond (the
+// difference then loses at most a factor 2.6 of relative accuracy).
+template <class T> __device__ __forceinline__ T expm1_t(T x) {
+  T q = fma(x, bc<T>(1.0f / 40320.0f), bc<T>(1.0f / 5040.0f));
+  q = fma(q, x, bc<T>(1.0f / 720.0f));
+  q = fma(q, x, bc<T>(1.0f / 120.0f));
+  q = fma(q, x, bc<T>(1.0f / 24.0f));
+  q = fma(q, x, bc<T>(1.0f / 6.0f));
+  q = fma(q, x, bc<T>(0.5f));
+  const T small = fma(q * x, x, x);
+  const T big = exp_fma(x) - 1.0f;
+  T r;
+#pragma unroll
+  for (int l = 0; l < Lanes<T>::n; ++l)
+    set_lane(r, l, fabsf(lane(x, l)) <= 0.5f ? lane(small, l) : lane(big, l));
+  return r;
 }
 
 // Rush-Larsen update with the exponent given as dt/tau.
@@ -442,7 +468,7 @@ __device__ __forceinline__ T ttp06_step_t(T V, CellStateT<T>& c, float dt,
   const T dtr_fCass = div(dt * (1.0f + cq), 82.0f + 2.0f * cq);
 
   const T x2v = 2.0f * (V - 15.0f) * FRT;
-  T denom = map1(x2v, [](float x) { return expm1f(x); });
+  T denom = expm1_t(x2v);
   const T exp2V = denom + 1.0f;
   denom = map1(denom, [](float x) { return fabsf(x) < 1e-10f ? 1e-10f : x; });
   const T i_CaL = div(g_CaL * d * f * f2 * fCass * CaL_k * (V - 15.0f) *
@@ -509,6 +535,14 @@ __device__ __forceinline__ T ttp06_step_t(T V, CellStateT<T>& c, float dt,
   c.v[S_CASR] = vmax(fma(bc<T>(dt), dCaSR, CaSR), 1e-7f);
   c.v[S_CASS] = vmax(fma(bc<T>(dt), dCass, Cass), 1e-7f);
   return I_ion;
+}
+
+// W = V + dt/Cm (-I_ion Cm + I_stim), two explicit FMAs (every kernel forms
+// the ionic half's output with this one expression).
+__device__ __forceinline__ float w_update(float V, float Iion, float Istim, float dt_over_Cm,
+                                          float Cm) {
+  const F1 t = fma(F1{-Iion}, F1{Cm}, F1{Istim});
+  return fma(F1{dt_over_Cm}, t, F1{V}).x;
 }
 
 // One cell (the fused kernels, Purkinje nodes).

@@ -11,7 +11,7 @@ import numpy as np
 
 from .. import _lib
 
-RULES = {"rel": 0, "rms": 1, "linf": 2}
+RULES = {"rel": 0, "rms": 1, "linf": 2, "p99": 3}
 
 
 def heart_neighbours(vox_idx: np.ndarray) -> np.ndarray:

@@ -209,7 +209,8 @@ hp_status hp_mono_destroy(HpMono *h);
 typedef enum {
   HP_STOP_REL = 0,   /* FP64 true residual ||b - A x|| / ||b|| <= tol */
   HP_STOP_RMS = 1,   /* sqrt(mean(z^2)) < tol (z = M^-1 r, volts), reference 'rms' */
-  HP_STOP_LINF = 2   /* max |z| < tol, reference 'linf' */
+  HP_STOP_LINF = 2,  /* max |z| < tol, reference 'linf' */
+  HP_STOP_P99 = 3    /* 0.99 quantile of |z| (linear interpolation) < tol, reference 'p99' */
 } hp_stop_rule;
 
 /*

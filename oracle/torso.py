@@ -15,7 +15,7 @@ FP64 CPU restatement of HrdayaPy's torso forward solve, used only by tests/,
   solved to machine precision (sparse LU), the reference the GPU PCG is
   judged against
 * :func:`pcg_reference`      -- _pcg_gpu (compute_bspm.py:164-263) in FP64
-  numpy, with its rms / linf stopping statistics
+  numpy, with its rms / p99 / linf stopping statistics
 * :func:`pinned_csr`, :func:`pcg_fp64` -- the pinned system in CSR form
   without a LIL round trip, and _pcg_gpu's Jacobi-CG run in FP64 in C
   (torso_oracle.c, pthreads) to a relative true residual: the FP64
@@ -146,7 +146,11 @@ def pcg_reference(A_pinned, b, x0=None, tol_mV=0.01, max_iter=500, metric="rms")
     tol_v = tol_mV * 1e-3
 
     def stat(z):
-        return np.linalg.norm(z) / np.sqrt(N) if metric == "rms" else np.abs(z).max()
+        if metric == "rms":
+            return np.linalg.norm(z) / np.sqrt(N)
+        if metric == "p99":    # torch.quantile(|z|, 0.99), linear interpolation
+            return np.quantile(np.abs(z), 0.99)
+        return np.abs(z).max()
 
     x = np.zeros(N) if x0 is None else np.array(x0, np.float64)
     r = b - A_pinned @ x if x0 is not None else np.array(b, np.float64)

@@ -113,3 +113,49 @@ def test_theta_scheme_ensemble_matches_separate_runs():
         ok = np.isfinite(act_s)
         assert (np.isfinite(ae) == ok).all()
         assert np.max(np.abs(ae[ok] - act_s[ok])) <= 0.1
+
+
+@pytest.mark.gpu
+def test_ensemble_variants_vs_fp64_oracle():
+    """The batched ensemble's per-variant parameters (longitudinal
+    conductivity, g_Ks and g_Kr multipliers, its own geometry and tree)
+    against FP64 oracle runs of each variant with the same parameters: two
+    variants of uneven size advanced in one launch per step, Vm RMS <= 0.5 mV
+    over every frame and max activation-time error <= 0.1 ms at -20 mV."""
+    from hrdayapy_b200 import monodomain as M
+    from hrdayapy_b200.ensemble import build_ensemble
+    from oracle import mono as orc
+    spec = [dict(seed=11, shape=(28, 24, 18), sigma_l=0.25, gks=0.7, gkr=1.3),
+            dict(seed=12, shape=(24, 20, 16), sigma_l=0.38, gks=1.4, gkr=0.6)]
+    probs, inputs = [], []
+    for sp in spec:
+        args, fibre, kw = cases.ragged_aniso_case(seed=sp["seed"], shape=sp["shape"], T=25.0)
+        kw = dict(kw, sigma_l=sp["sigma_l"])
+        nodes, el, act, S, phi = args
+        prob, _ = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=True,
+                            vm_save_dt=kw["dt"], act_threshold=-20.0, deact_threshold=-20.0,
+                            brick=(4, 4, 8), **dict(kw, A_P=2.0 / kw["R_P"]))
+        probs.append(prob)
+        inputs.append((args, fibre, kw))
+    ens = build_ensemble(probs, gks=[s["gks"] for s in spec], gkr=[s["gkr"] for s in spec])
+    sim = M.MonoHandle(ens.problem)
+    sim.run(ens.problem.n_steps, graph_chunk=50)
+    vm_e = sim.vm_frames()
+    a_e, n_e, _, _ = sim.events()
+    sim.close()
+    for v, (sp, (args, fibre, kw)) in enumerate(zip(spec, inputs)):
+        nodes, el, act, S, phi = args
+        r = orc.run(nodes, el, act, S, phi, fibre_dir=fibre, anisotropic=True, vm_save_dt=kw["dt"],
+                    gks_scale=sp["gks"], gkr_scale=sp["gkr"], **kw)
+        vm = ens.split(vm_e)[v]
+        assert vm.shape == r["Vm"].shape
+        rms = float(np.sqrt(np.mean((vm.astype(np.float64) - r["Vm"]) ** 2)))
+        ra = orc.activation_maps(r["Vm"], r["time_vm"], -20.0, -20.0)["activation_times"][:, 0]
+        ok = np.isfinite(ra)
+        ae, ne = ens.split(a_e[0])[v], ens.split(n_e)[v]
+        assert ok.sum() > 0.5 * len(ok)
+        assert (ne[ok] >= 1).all() and (ne[~ok] == 0).all()
+        err = float(np.max(np.abs(ae[ok] - ra[ok])))
+        print(f"ensemble variant {v} ({len(ok)} voxels, sigma_l {sp['sigma_l']}, g_Ks x{sp['gks']}, "
+              f"g_Kr x{sp['gkr']}): Vm RMS {rms:.2e} mV, max |dLAT| {err:.2e} ms vs FP64")
+        assert rms <= 0.5 and err <= 0.1
