@@ -225,7 +225,7 @@ __device__ __forceinline__ void purkinje_ionic_state(const MonoArgs& a, int p, f
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p] = c.v[v];
   const float Is = stim_current(a, a.pk_stim[p], istep, var);
-  Wout[p] = w_update(Vn, Iion, Is, a.dt_over_Cm, a.Cm);
+  Wout[p] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
 __device__ __forceinline__ void purkinje_ionic(const MonoArgs& a, int p, float Vn, int64_t istep,
@@ -246,56 +246,59 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   }
 }
 
-// The values one voxel's 19-point sum reads: its W and its 18 neighbours',
-// the six face weights (own +i/+j/+k, the -i/-j/-k neighbours'), and the
-// off-diagonal tensor components at the voxel and at its 12 edge
-// neighbours (face order +i -i +j -j +k -k; edge order as the tag bits).
-struct StencilVals {
-  float Vc, Vf[6], V01[4], V02[4], V12[4];
-  float wf[6];
-  float T01c, T01[4], T02c, T02[4], T12c, T12[4];
-};
-
-// sum_j coef_ij (W_j - W_i) of one voxel from its values, including its
-// junction currents (Purkinje potentials from Wpk).  Every step kernel,
-// whatever its tiles or voxels per thread, forms the sum here, so the
-// arithmetic is one instruction sequence.  DIAG: every difference reads -1,
-// so the sum is the operator's diagonal.
-template <bool ANISO, bool DIAG = false>
-__device__ __forceinline__ float stencil_sum(const MonoArgs& a, const StencilVals& v,
-                                             uint32_t tag, int64_t slot,
+// Stencil sum of one voxel, sum_j coef_ij (W_j - W_i) including its junction
+// currents (Purkinje potentials from Wpk), from shared tiles with strides SI
+// (i), SJ (j), 1 (k); face weights and off-diagonal tensor components are
+// three tiles each, NS floats apart.
+template <int SI, int SJ, int NS, bool ANISO, bool DIAG = false>
+__device__ __forceinline__ float stencil_acc(const MonoArgs& a, const float* tV, const float* tW,
+                                             const float* tD, int c, uint32_t tag, int64_t slot,
                                              const float* __restrict__ Wpk) {
+  // DIAG: every difference reads -1, so the sum is the operator's diagonal
 #define HP_DV(x) (DIAG ? -1.0f : ((x) - Vc))
-  const float Vc = DIAG ? 0.0f : v.Vc;
+  const float Vc = DIAG ? 0.0f : tV[c];
   float acc = 0.0f;
   const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
   if constexpr (!ANISO) {
     float s = 0.0f;
-#pragma unroll
-    for (int f = 0; f < 6; ++f)
-      if (fb & (1u << f)) s += HP_DV(v.Vf[f]);
+    if (fb & 1u) s += HP_DV(tV[c + SI]);
+    if (fb & 2u) s += HP_DV(tV[c - SI]);
+    if (fb & 4u) s += HP_DV(tV[c + SJ]);
+    if (fb & 8u) s += HP_DV(tV[c - SJ]);
+    if (fb & 16u) s += HP_DV(tV[c + 1]);
+    if (fb & 32u) s += HP_DV(tV[c - 1]);
     acc = a.iso_coef * s;
   } else {
-#pragma unroll
-    for (int f = 0; f < 6; ++f)
-      if (fb & (1u << f)) acc += v.wf[f] * HP_DV(v.Vf[f]);
+    const float* tWx = tW;
+    const float* tWy = tW + NS;
+    const float* tWz = tW + 2 * NS;
+    if (fb & 1u) acc += tWx[c] * HP_DV(tV[c + SI]);
+    if (fb & 2u) acc += tWx[c - SI] * HP_DV(tV[c - SI]);
+    if (fb & 4u) acc += tWy[c] * HP_DV(tV[c + SJ]);
+    if (fb & 8u) acc += tWy[c - SJ] * HP_DV(tV[c - SJ]);
+    if (fb & 16u) acc += tWz[c] * HP_DV(tV[c + 1]);
+    if (fb & 32u) acc += tWz[c - 1] * HP_DV(tV[c - 1]);
     const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
+    const float* t01 = tD;
+    const float* t02 = tD + NS;
+    const float* t12 = tD + 2 * NS;
     // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float sg = q < 2 ? 1.0f : -1.0f;
-      if (db & (1u << q)) acc += sg * 0.25f * (v.T01c + v.T01[q]) * HP_DV(v.V01[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float sg = q < 2 ? 1.0f : -1.0f;
-      if (db & (1u << (4 + q))) acc += sg * 0.25f * (v.T02c + v.T02[q]) * HP_DV(v.V02[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float sg = q < 2 ? 1.0f : -1.0f;
-      if (db & (1u << (8 + q))) acc += sg * 0.25f * (v.T12c + v.T12[q]) * HP_DV(v.V12[q]);
-    }
+#define HP_DIAG(bit, T, OFF, SGN)                                            \
+  if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
+                                 HP_DV(tV[c + (OFF)]);
+    HP_DIAG(0, t01, SI + SJ, 1.0f)
+    HP_DIAG(1, t01, -SI - SJ, 1.0f)
+    HP_DIAG(2, t01, SI - SJ, -1.0f)
+    HP_DIAG(3, t01, -SI + SJ, -1.0f)
+    HP_DIAG(4, t02, SI + 1, 1.0f)
+    HP_DIAG(5, t02, -SI - 1, 1.0f)
+    HP_DIAG(6, t02, SI - 1, -1.0f)
+    HP_DIAG(7, t02, -SI + 1, -1.0f)
+    HP_DIAG(8, t12, SJ + 1, 1.0f)
+    HP_DIAG(9, t12, -SJ - 1, 1.0f)
+    HP_DIAG(10, t12, SJ - 1, -1.0f)
+    HP_DIAG(11, t12, -SJ + 1, -1.0f)
+#undef HP_DIAG
   }
   if (tag & HP_TAG_PMJ) {
     const int r = a.pmj_row[slot];
@@ -304,169 +307,6 @@ __device__ __forceinline__ float stencil_sum(const MonoArgs& a, const StencilVal
   }
 #undef HP_DV
   return acc;
-}
-
-// Gathers one voxel's stencil values from shared tiles with strides SI (i),
-// SJ (j), 1 (k); face weights and off-diagonal tensor components are three
-// tiles each, NS floats apart.
-template <int SI, int SJ, int NS, bool ANISO>
-__device__ __forceinline__ void gather_vals(StencilVals& v, const float* tV, const float* tW,
-                                            const float* tD, int c) {
-  if (tV) {
-    v.Vc = tV[c];
-    const int fo[6] = {SI, -SI, SJ, -SJ, 1, -1};
-#pragma unroll
-    for (int f = 0; f < 6; ++f) v.Vf[f] = tV[c + fo[f]];
-    if constexpr (ANISO) {
-      const int o01[4] = {SI + SJ, -SI - SJ, SI - SJ, -SI + SJ};
-      const int o02[4] = {SI + 1, -SI - 1, SI - 1, -SI + 1};
-      const int o12[4] = {SJ + 1, -SJ - 1, SJ - 1, -SJ + 1};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        v.V01[q] = tV[c + o01[q]];
-        v.V02[q] = tV[c + o02[q]];
-        v.V12[q] = tV[c + o12[q]];
-      }
-    }
-  }
-  if constexpr (ANISO) {
-    const float* tWx = tW;
-    const float* tWy = tW + NS;
-    const float* tWz = tW + 2 * NS;
-    v.wf[0] = tWx[c];
-    v.wf[1] = tWx[c - SI];
-    v.wf[2] = tWy[c];
-    v.wf[3] = tWy[c - SJ];
-    v.wf[4] = tWz[c];
-    v.wf[5] = tWz[c - 1];
-    const float* t01 = tD;
-    const float* t02 = tD + NS;
-    const float* t12 = tD + 2 * NS;
-    const int o01[4] = {SI + SJ, -SI - SJ, SI - SJ, -SI + SJ};
-    const int o02[4] = {SI + 1, -SI - 1, SI - 1, -SI + 1};
-    const int o12[4] = {SJ + 1, -SJ - 1, SJ - 1, -SJ + 1};
-    v.T01c = t01[c];
-    v.T02c = t02[c];
-    v.T12c = t12[c];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      v.T01[q] = t01[c + o01[q]];
-      v.T02[q] = t02[c + o02[q]];
-      v.T12[q] = t12[c + o12[q]];
-    }
-  }
-}
-
-// Stencil sum of one voxel from shared tiles (see gather_vals).
-template <int SI, int SJ, int NS, bool ANISO, bool DIAG = false>
-__device__ __forceinline__ float stencil_acc(const MonoArgs& a, const float* tV, const float* tW,
-                                             const float* tD, int c, uint32_t tag, int64_t slot,
-                                             const float* __restrict__ Wpk) {
-  StencilVals v;
-  gather_vals<SI, SJ, NS, ANISO>(v, DIAG ? nullptr : tV, tW, tD, c);
-  return stencil_sum<ANISO, DIAG>(a, v, tag, slot, Wpk);
-}
-
-// The stencil values of the two voxels at tile positions c (even) and c + 1
-// (consecutive k) from 8-byte pair loads: the k-column of the voxel pair and
-// of its four face neighbours (k - 1 .. k + 2, three aligned pairs), the
-// edge neighbours in ij (k, k + 1), and the weight tiles likewise -- about
-// 45 shared loads for both voxels against 80 for two one-voxel gathers.
-// Tile rows start on 16-byte boundaries, so c even is 8-byte aligned; the
-// pairs below the first and above the last k of a row read the row
-// padding, which only fills lanes that are not used.
-__device__ __forceinline__ float2 lds2(const float* t, int i) {
-  return *(const float2*)(t + i);
-}
-template <int SI, int SJ, int NS, bool ANISO>
-__device__ __forceinline__ void gather_vals_pair(StencilVals (&v)[2], const float* tV,
-                                                 const float* tW, const float* tD, int c) {
-  // column at offset o: values at k - 1, k, k + 1, k + 2 (relative to c)
-  auto col4 = [&](const float* t, int o, float (&x)[4]) {
-    const float2 lo = lds2(t, c + o - 2), mid = lds2(t, c + o), hi = lds2(t, c + o + 2);
-    x[0] = lo.y;
-    x[1] = mid.x;
-    x[2] = mid.y;
-    x[3] = hi.x;
-  };
-  float cc[4], ip[4], im[4], jp[4], jm[4];
-  col4(tV, 0, cc);
-  col4(tV, SI, ip);
-  col4(tV, -SI, im);
-  col4(tV, SJ, jp);
-  col4(tV, -SJ, jm);
-#pragma unroll
-  for (int e = 0; e < 2; ++e) {
-    // x[1 + e] is the voxel's own k, x[e] its k - 1, x[2 + e] its k + 1
-    v[e].Vc = cc[1 + e];
-    v[e].Vf[0] = ip[1 + e];
-    v[e].Vf[1] = im[1 + e];
-    v[e].Vf[2] = jp[1 + e];
-    v[e].Vf[3] = jm[1 + e];
-    v[e].Vf[4] = cc[2 + e];
-    v[e].Vf[5] = cc[e];
-  }
-  if constexpr (ANISO) {
-    const float2 d0 = lds2(tV, c + SI + SJ), d1 = lds2(tV, c - SI - SJ);
-    const float2 d2 = lds2(tV, c + SI - SJ), d3 = lds2(tV, c - SI + SJ);
-    v[0].V01[0] = d0.x; v[1].V01[0] = d0.y;
-    v[0].V01[1] = d1.x; v[1].V01[1] = d1.y;
-    v[0].V01[2] = d2.x; v[1].V01[2] = d2.y;
-    v[0].V01[3] = d3.x; v[1].V01[3] = d3.y;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      // (SI+1, -SI-1, SI-1, -SI+1) and the same in j
-      v[e].V02[0] = ip[2 + e];
-      v[e].V02[1] = im[e];
-      v[e].V02[2] = ip[e];
-      v[e].V02[3] = im[2 + e];
-      v[e].V12[0] = jp[2 + e];
-      v[e].V12[1] = jm[e];
-      v[e].V12[2] = jp[e];
-      v[e].V12[3] = jm[2 + e];
-    }
-    const float* tWx = tW;
-    const float* tWy = tW + NS;
-    const float* tWz = tW + 2 * NS;
-    const float2 wx = lds2(tWx, c), wxm = lds2(tWx, c - SI);
-    const float2 wy = lds2(tWy, c), wym = lds2(tWy, c - SJ);
-    const float2 wz = lds2(tWz, c), wzm = lds2(tWz, c - 2);
-    v[0].wf[0] = wx.x;  v[1].wf[0] = wx.y;
-    v[0].wf[1] = wxm.x; v[1].wf[1] = wxm.y;
-    v[0].wf[2] = wy.x;  v[1].wf[2] = wy.y;
-    v[0].wf[3] = wym.x; v[1].wf[3] = wym.y;
-    v[0].wf[4] = wz.x;  v[1].wf[4] = wz.y;
-    v[0].wf[5] = wzm.y; v[1].wf[5] = wz.x;
-    const float* t01 = tD;
-    const float* t02 = tD + NS;
-    const float* t12 = tD + 2 * NS;
-    const float2 a0 = lds2(t01, c), a1 = lds2(t01, c + SI + SJ), a2 = lds2(t01, c - SI - SJ);
-    const float2 a3 = lds2(t01, c + SI - SJ), a4 = lds2(t01, c - SI + SJ);
-    v[0].T01c = a0.x; v[1].T01c = a0.y;
-    v[0].T01[0] = a1.x; v[1].T01[0] = a1.y;
-    v[0].T01[1] = a2.x; v[1].T01[1] = a2.y;
-    v[0].T01[2] = a3.x; v[1].T01[2] = a3.y;
-    v[0].T01[3] = a4.x; v[1].T01[3] = a4.y;
-    float bp[4], bm[4], cp[4], cm[4];
-    col4(t02, SI, bp);
-    col4(t02, -SI, bm);
-    col4(t12, SJ, cp);
-    col4(t12, -SJ, cm);
-    const float2 b0 = lds2(t02, c), c0 = lds2(t12, c);
-    v[0].T02c = b0.x; v[1].T02c = b0.y;
-    v[0].T12c = c0.x; v[1].T12c = c0.y;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      v[e].T02[0] = bp[2 + e];
-      v[e].T02[1] = bm[e];
-      v[e].T02[2] = bp[e];
-      v[e].T02[3] = bm[2 + e];
-      v[e].T12[0] = cp[2 + e];
-      v[e].T12[1] = cm[e];
-      v[e].T12[2] = cp[e];
-      v[e].T12[3] = cm[2 + e];
-    }
-  }
 }
 
 // Diffusion half of one voxel (explicit step): V = clamp(W + sum coef (W_j - W)).
@@ -516,7 +356,7 @@ __device__ __forceinline__ void voxel_ionic(const MonoArgs& a, int64_t slot, uin
 #pragma unroll
   for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * a.n_slots + slot] = cs.v[v];
   const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
-  Wout[slot] = w_update(Vn, Iion, Is, a.dt_over_Cm, a.Cm);
+  Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
 }
 
 // Everything a tissue voxel does once V_{i+1} = Vn is known (mode 0):
@@ -961,15 +801,12 @@ __device__ __forceinline__ void cn_pass_scalars(const CnArgs& c, int op, const d
 // their sums).  OP_CN_APPLY: q = p - theta Lh p and <p, q>_w.  The CN
 // passes write tissue entries only: padding entries of the CG vectors are
 // zero from set-up and stay zero.
-template <int BI, int BJ, int BK, bool ANISO, int OP, int VPT = 1>
+template <int BI, int BJ, int BK, bool ANISO, int OP>
 __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, int step_off) {
   using G = PipeGeom<BI, BJ, BK>;
   using H = DiffHalo<BI, BJ, BK, ANISO>;
   using D = DiffStage<BI, BJ, BK, ANISO>;
-  static_assert(VPT == 1 || (VPT == 2 && OP == OP_STEP && BK % 2 == 0), "voxels per thread");
-  constexpr int BV = G::BV, NF = D::NF;
-  constexpr int NT = BV / VPT;                        // threads per CTA
-  constexpr int PT = (H::N + NT - 1) / NT;            // halo copies per thread
+  constexpr int BV = G::BV, NF = D::NF, PT = H::PER_THREAD;
   constexpr int QB = BV / 4;  // 16-byte chunks per brick row of one field
   // per-slot fields after the tiles: tag, then V_i (step) or Dinv (start)
   constexpr int NCHUNK = OP == OP_CN_APPLY ? (NF + 1) * BV / 4 : D::NCHUNK;
@@ -991,7 +828,7 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
   const float* hsrc[PT];
 #pragma unroll
   for (int q = 0; q < PT; ++q) {
-    const int e = tid + q * NT;
+    const int e = tid + q * BV;
     const uint32_t t = e < a.n_halo ? a.halo_tab[e] : 0u;
     const int f = (t >> 11) & 7;
     hpos[q] = e < a.n_halo ? (uint32_t)(f * G::NT + (int)(t & ((1u << HALO_POS_BITS) - 1)))
@@ -1004,8 +841,8 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
   auto issue = [&](float* st, const int* nb27, int b) {
     const int64_t base = (int64_t)b * BV;
 #pragma unroll
-    for (int k = 0; k < (NCHUNK + NT - 1) / NT; ++k) {
-      const int q = tid + k * NT;
+    for (int k = 0; k < (NCHUNK + BV - 1) / BV; ++k) {
+      const int q = tid + k * BV;
       if (q < NCHUNK) {
         const int f = q / QB, o = (q % QB) * 4;
         const float* src = f == 0    ? Win
@@ -1035,8 +872,7 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
       }
     }
   };
-  const int v0 = tid * VPT;                 // first voxel of this thread in the brick
-  const int li = v0 / (BJ * BK), lj = (v0 / BK) % BJ, lk = v0 % BK;
+  const int li = tid / (BJ * BK), lj = (tid / BK) % BJ, lk = tid % BK;
   const int c = G::pos(li, lj, lk);
   const int G_ = gridDim.x;
   const int n_items = a.n_bricks + (a.n_pk + BV - 1) / BV;
@@ -1064,36 +900,7 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
       if (nn < a.n_bricks && tid < 27) cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
     }
     cp_async_commit();
-    if (VPT == 2 && cur < a.n_bricks) {
-      // explicit step, two voxels (consecutive k) per thread
-      const float* st = stages + (n & 1) * D::FLOATS;
-      const uint2 tg = ((const uint2*)(st + D::TAG))[tid];
-      if ((tg.x | tg.y) & HP_TAG_PHENO_MASK) {
-        const int64_t slot = (int64_t)cur * BV + v0;
-        const float* tW = ANISO ? st + G::NT : st;
-        const float* tD = ANISO ? st + 4 * G::NT : st;
-        StencilVals vv[2];
-        gather_vals_pair<G::SI, G::SJ, G::NT, ANISO>(vv, st, tW, tD, c);
-        const float2 vp = ((const float2*)(st + D::VP))[tid];
-        const float* Wpk = odd ? a.pk_Vs1 : a.pk_Vs0;
-        const uint32_t tags[2] = {tg.x, tg.y};
-        const float vprev[2] = {vp.x, vp.y};
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (tags[e] & HP_TAG_PHENO_MASK) {
-            const float acc = stencil_sum<ANISO>(a, vv[e], tags[e], slot + e, Wpk);
-            const float Vn = fminf(fmaxf(vv[e].Vc + acc, -150.0f), 80.0f);
-            voxel_outputs(a, slot + e, tags[e], Vn, vprev[e], step, s_vm_frame, s_anim_frame);
-          }
-        }
-      }
-    } else if (VPT == 2) {
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int p = (cur - a.n_bricks) * BV + v0 + e;
-        if (p < a.n_pk) purkinje_diffuse(a, p, step);
-      }
-    } else if (cur < a.n_bricks) {
+    if (cur < a.n_bricks) {
       const float* st = stages + (n & 1) * D::FLOATS;
       const uint32_t tag = ((const uint32_t*)(st + D::TAG))[tid];
       if (tag & HP_TAG_PHENO_MASK) {
@@ -1154,17 +961,11 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
   }
 }
 
-// Explicit diffusion half of the split step: two voxels per thread (BV / 2
-// threads per CTA), 8-byte pair loads from the tiles.
-#ifndef HP_DIFF_VPT
-#define HP_DIFF_VPT 2
-#endif
-constexpr int DIFF_VPT = HP_DIFF_VPT;
 template <int BI, int BJ, int BK, bool ANISO>
-__global__ void __launch_bounds__(BI * BJ * BK / DIFF_VPT)
+__global__ void __launch_bounds__(BI * BJ * BK)
 mono_diffuse_kernel(MonoArgs a, int step_off) {
   CnArgs none{};
-  diffuse_pass<BI, BJ, BK, ANISO, OP_STEP, DIFF_VPT>(a, none, step_off);
+  diffuse_pass<BI, BJ, BK, ANISO, OP_STEP>(a, none, step_off);
 }
 
 // The two CN passes on the persistent diffusion kernel's tiles.
@@ -1174,30 +975,18 @@ __global__ void __launch_bounds__(BI * BJ * BK) cn_pass_kernel(MonoArgs a, CnArg
 }
 
 constexpr int ION_THREADS = 128;
-#ifndef HP_ION_PAIRS
-#define HP_ION_PAIRS 1
-#endif
-constexpr int ION_CPT = HP_ION_PAIRS ? 2 : 1;   // cells per thread of the ionic kernel
-
-// 8-byte access to two adjacent floats as one packed pair
-__device__ __forceinline__ F2 ld_pair(const float* p) {
-  return F2{*(const unsigned long long*)p};
-}
-__device__ __forceinline__ void st_pair(float* p, F2 v) { *(unsigned long long*)p = v.x; }
 
 // The split step keeps the 18 TTP06 states in compact tissue order (index
-// i of active_slot, not the slot; row stride n_active_pad, a multiple of 32),
-// so the ionic half's state loads and stores are fully coalesced; tag, V and
-// W stay per slot for the stencil.  Each thread advances two cells (compact
-// indices 2t, 2t + 1, or two Purkinje nodes) with the packed-FP32 TTP06: its
-// state moves as 8-byte pairs.
+// i of active_slot, not the slot), so the ionic half's state loads and
+// stores are fully coalesced; tag, V and W stay per slot for the stencil.
+// mode 1: the prologue, the ionic half of step 0 on V_0 into W_0.
 // mode 0: the ionic half of step i+1 on V_{i+1} = Vpost; mode 1: the
 // prologue, the ionic half of step 0 on V_0 into W_0; mode 2: the end of a
 // theta-scheme step, V_{i+1} = clamp(x) with the outputs of step i recorded
 // exactly as the explicit step records them, then the ionic half of step
 // i+1 on it.
 template <int mode>
-__global__ void __launch_bounds__(ION_THREADS, HP_ION_PAIRS ? 4 : 8) mono_ionic_kernel(MonoArgs a, int step_off) {
+__global__ void __launch_bounds__(ION_THREADS, 8) mono_ionic_kernel(MonoArgs a, int step_off) {
   __shared__ int64_t s_vm_frame, s_anim_frame;
   const int64_t step = *a.d_step + step_off;
   if constexpr (mode == 2) {
@@ -1209,10 +998,9 @@ __global__ void __launch_bounds__(ION_THREADS, HP_ION_PAIRS ? 4 : 8) mono_ionic_
   }
   const bool odd = step & 1;
   const int64_t istep = mode == 1 ? 0 : step + 1;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-#if !HP_ION_PAIRS
-  if (t < a.n_active) {
-    const int64_t slot = a.active_slot[t];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.n_active) {
+    const int64_t slot = a.active_slot[i];
     const uint32_t tag = a.tag[slot];
     float Vn;
     if constexpr (mode == 2) {
@@ -1221,20 +1009,20 @@ __global__ void __launch_bounds__(ION_THREADS, HP_ION_PAIRS ? 4 : 8) mono_ionic_
     } else {
       Vn = a.Vpost[slot];
     }
-    const int64_t na = a.n_active_pad;
+    const int64_t na = a.n_active;
     CellState cs;
 #pragma unroll
-    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + t];
+    for (int v = 0; v < N_STATE; ++v) cs.v[v] = a.state[(int64_t)v * na + i];
     const int var = a.brick_variant ? a.brick_variant[slot >> a.bv_shift] : 0;
     const CellParams cp = pheno_params(tag & HP_TAG_PHENO_MASK, a.var_gks[var], a.var_gkr[var]);
     const float Iion = ttp06_step(Vn, cs, a.dt, cp);
 #pragma unroll
-    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + t] = cs.v[v];
+    for (int v = 0; v < N_STATE; ++v) a.state[(int64_t)v * na + i] = cs.v[v];
     const float Is = stim_current(a, tag >> HP_TAG_STIM_SHIFT, istep, var);
     float* __restrict__ Wout = mode == 1 ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
-    Wout[slot] = w_update(Vn, Iion, Is, a.dt_over_Cm, a.Cm);
+    Wout[slot] = Vn + a.dt_over_Cm * (-(Iion * a.Cm) + Is);
   } else {
-    const int p = t - a.n_active_pad;
+    const int p = i - a.n_active_pad;
     if (p >= 0 && p < a.n_pk) {
       float Vn;
       if constexpr (mode == 2) {
@@ -1245,88 +1033,6 @@ __global__ void __launch_bounds__(ION_THREADS, HP_ION_PAIRS ? 4 : 8) mono_ionic_
         Vn = a.pk_Vpost[p];
       }
       purkinje_ionic(a, p, Vn, istep, mode == 1 ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1));
-    }
-  }
-  return;
-#endif
-  const int i0 = 2 * t;
-  if (i0 < a.n_active) {
-    const int nl = i0 + 1 < a.n_active ? 2 : 1;  // valid lanes
-    int64_t slot[2];
-    uint32_t tag[2];
-    float Vn[2];
-    int var[2];
-    CellParams cp[2];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      slot[l] = a.active_slot[l < nl ? i0 + l : i0];
-      tag[l] = a.tag[slot[l]];
-      if constexpr (mode == 2) {
-        Vn[l] = fminf(fmaxf(a.cn_x[slot[l]], -150.0f), 80.0f);
-        if (l < nl)
-          voxel_outputs(a, slot[l], tag[l], Vn[l], a.Vpost[slot[l]], step, s_vm_frame,
-                        s_anim_frame);
-      } else {
-        Vn[l] = a.Vpost[slot[l]];
-      }
-      var[l] = a.brick_variant ? a.brick_variant[slot[l] >> a.bv_shift] : 0;
-      cp[l] = pheno_params(tag[l] & HP_TAG_PHENO_MASK, a.var_gks[var[l]], a.var_gkr[var[l]]);
-    }
-    // a lone last cell fills lane 1 with itself; its state pair stays in the
-    // row's padding (i0 + 1 < n_active_pad)
-    const int64_t na = a.n_active_pad;
-    CellStateT<F2> cs;
-#pragma unroll
-    for (int v = 0; v < N_STATE; ++v) cs.v[v] = ld_pair(a.state + (int64_t)v * na + i0);
-    const F2 I = ttp06_step2(pack2(Vn[0], Vn[1]), cs, a.dt, cp[0], cp[1]);
-#pragma unroll
-    for (int v = 0; v < N_STATE; ++v) st_pair(a.state + (int64_t)v * na + i0, cs.v[v]);
-    float* __restrict__ Wout = mode == 1 ? a.Vs0 : (odd ? a.Vs0 : a.Vs1);
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      if (l < nl) {
-        const float Iion = lane(I, l);
-        const float Is = stim_current(a, tag[l] >> HP_TAG_STIM_SHIFT, istep, var[l]);
-        Wout[slot[l]] = w_update(Vn[l], Iion, Is, a.dt_over_Cm, a.Cm);
-      }
-    }
-  } else {
-    const int p0 = 2 * (t - a.n_active_pad / 2);
-    if (p0 >= 0 && p0 < a.n_pk) {
-      const int nl = p0 + 1 < a.n_pk ? 2 : 1;
-      int p[2] = {p0, nl == 2 ? p0 + 1 : p0};
-      float Vn[2];
-      int var[2];
-      CellParams cp[2];
-      CellStateT<F2> cs;
-#pragma unroll
-      for (int l = 0; l < 2; ++l) {
-        if constexpr (mode == 2) {
-          Vn[l] = fminf(fmaxf(a.cn_x[a.n_slots + p[l]], -150.0f), 80.0f);
-          if (l < nl) {
-            a.pk_Vpost[p[l]] = Vn[l];
-            if (s_anim_frame >= 0) a.pk_frames[s_anim_frame * (int64_t)a.n_pk + p[l]] = Vn[l];
-          }
-        } else {
-          Vn[l] = a.pk_Vpost[p[l]];
-        }
-        var[l] = a.pk_variant ? a.pk_variant[p[l]] : 0;
-        cp[l] = pheno_params(1, a.var_gks[var[l]], a.var_gkr[var[l]]);  // Purkinje -> endo
-      }
-#pragma unroll
-      for (int v = 0; v < N_STATE; ++v)
-        cs.v[v] = pack2(a.pk_state[(int64_t)v * a.n_pk + p[0]], a.pk_state[(int64_t)v * a.n_pk + p[1]]);
-      const F2 I = ttp06_step2(pack2(Vn[0], Vn[1]), cs, a.dt, cp[0], cp[1]);
-      float* __restrict__ Wout = mode == 1 ? a.pk_Vs0 : (odd ? a.pk_Vs0 : a.pk_Vs1);
-#pragma unroll
-      for (int l = 0; l < 2; ++l) {
-        if (l < nl) {
-#pragma unroll
-          for (int v = 0; v < N_STATE; ++v) a.pk_state[(int64_t)v * a.n_pk + p[l]] = lane(cs.v[v], l);
-          const float Is = stim_current(a, a.pk_stim[p[l]], istep, var[l]);
-          Wout[p[l]] = w_update(Vn[l], lane(I, l), Is, a.dt_over_Cm, a.Cm);
-        }
-      }
     }
   }
 }
@@ -1607,7 +1313,7 @@ static hp_status launch_step(HpMono* h, int step_off, int mode, cudaStream_t s) 
   const int grid = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   if (grid == 0) return HP_OK;
   if (mode == 0 && h->diff) {
-    h->diff<<<h->diff_grid, h->bv / DIFF_VPT, h->diff_smem, s>>>(h->a, step_off);
+    h->diff<<<h->diff_grid, h->bv, h->diff_smem, s>>>(h->a, step_off);
     if (h->ion_grid > 0) mono_ionic_kernel<0><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
   } else if (mode == 1 && h->diff) {
     if (h->ion_grid > 0) mono_ionic_kernel<1><<<h->ion_grid, ION_THREADS, 0, s>>>(h->a, step_off);
@@ -1680,8 +1386,7 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   h->diff = d->anisotropic ? se->diff_aniso : se->diff_iso;
   // states in compact tissue order (resting state, as for the slot order)
   if (!act.empty())
-    init_cells_kernel<<<1024, 256, 0, s>>>(h->a.state, h->a.Vpost, (int64_t)h->a.n_active_pad,
-                                           d->v0);
+    init_cells_kernel<<<1024, 256, 0, s>>>(h->a.state, h->a.Vpost, (int64_t)act.size(), d->v0);
   HP_CUDA_TRY(cudaGetLastError());
   // diffusion half: persistent CTAs over bricks, halo copy table per shape
   const std::vector<uint32_t> tab = se->halo(d->anisotropic != 0);
@@ -1702,15 +1407,11 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
   HP_CUDA_TRY(cudaFuncSetAttribute((const void*)h->diff, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
-  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->diff,
-                                                            h->bv / DIFF_VPT, smem));
+  HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)h->diff, h->bv, smem));
   h->diff_smem = smem;
   const int n_items = h->a.n_bricks + (h->a.n_pk + h->bv - 1) / h->bv;
   h->diff_grid = std::max(1, std::min(n_items, std::max(per_sm, 1) * n_sm));
-  // two cells per thread: n_active_pad / 2 threads for the tissue, then the
-  // Purkinje pairs
-  h->ion_grid = (h->a.n_active_pad / ION_CPT + (h->a.n_pk + ION_CPT - 1) / ION_CPT + ION_THREADS - 1) /
-                ION_THREADS;
+  h->ion_grid = (h->a.n_active_pad + h->a.n_pk + ION_THREADS - 1) / ION_THREADS;
   return HP_OK;
 }
 
@@ -2252,13 +1953,12 @@ extern "C" hp_status hp_mono_copy_state(HpMono* h, float* st_slots, float* st_pk
     if (h->diff) {
       // the split step stores states in compact tissue order: scatter to slots
       HP_CUDA_TRY(cudaStreamSynchronize(s));
-      // (rows of stride n_active_pad)
-      const int64_t ns = h->a.n_slots, na = h->a.n_active, nr = h->a.n_active_pad;
+      const int64_t ns = h->a.n_slots, na = h->a.n_active;
       std::vector<int32_t> act(na);
       if (na) HP_CUDA_TRY(cudaMemcpy(act.data(), h->a.active_slot, na * 4, cudaMemcpyDeviceToHost));
       std::vector<float> tmp((size_t)N_STATE * na);
       for (int v = 0; v < N_STATE; ++v)
-        std::copy(st_slots + (size_t)v * nr, st_slots + (size_t)v * nr + na, tmp.begin() + (size_t)v * na);
+        std::copy(st_slots + (size_t)v * na, st_slots + (size_t)(v + 1) * na, tmp.begin() + (size_t)v * na);
       for (int v = 0; v < N_STATE; ++v) {
         float* dst = st_slots + (size_t)v * ns;
         std::fill(dst, dst + ns, 0.0f);

@@ -1369,6 +1369,26 @@ extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const fl
   return finish(result, "hp_torso_solve_frame_fcg");
 }
 
+namespace hp {
+// n more iterations of the current CG recursion (no restart, no stopping
+// test), then the pending x update applied so that x is the n-th iterate.
+static hp_status pcg_continue(HpTorso* h, int n, cudaStream_t s) {
+  TorsoArgs& a = h->a;
+  const double never = 0.0;     // relative rule with tolerance 0: runs all n
+  HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_TOL, &never, 8, cudaMemcpyHostToDevice, s));
+  int32_t is_run[N_ISCAL] = {0, 0, HP_STOP_REL, n, 0, 0};
+  HP_CUDA_TRY(cudaMemcpyAsync(a.iscal, is_run, sizeof(is_run), cudaMemcpyHostToDevice, s));
+  hp_status st = run_iterations(h, n, false, s);
+  if (st != HP_OK) return st;
+  pcg_finish_x<<<h->nblk, TB, 0, s>>>(a);
+  HP_CUDA_TRY(cudaGetLastError());
+  const double zero = 0.0;      // the update is applied: nothing pending
+  HP_CUDA_TRY(cudaMemcpyAsync(a.scal + SC_ALPHA_PREV, &zero, 8, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));   // the host scalars above are stack temporaries
+  return HP_OK;
+}
+}  // namespace hp
+
 extern "C" hp_status hp_torso_train_precond(HpTorso* h, HpPrecond* p, const float* vm_frames,
                                             int64_t frame_stride, int32_t n_frames,
                                             const int32_t* ks, int32_t n_ks, int32_t repeats,
@@ -1376,6 +1396,9 @@ extern "C" hp_status hp_torso_train_precond(HpTorso* h, HpPrecond* p, const floa
                                             void* stream) {
   HP_REQUIRE(h && p && vm_frames && ks && n_frames >= 1 && n_ks >= 1 && repeats >= 1,
              "hp_torso_train_precond: bad arguments");
+  for (int q = 0; q < n_ks; ++q)
+    HP_REQUIRE(ks[q] >= 0 && (q == 0 || ks[q] >= ks[q - 1]),
+               "hp_torso_train_precond: ks must be non-negative and ascending");
   cudaStream_t s = (cudaStream_t)stream;
   TorsoArgs& a = h->a;
   double *xstar = nullptr, *x0 = nullptr;
@@ -1393,14 +1416,16 @@ extern "C" hp_status hp_torso_train_precond(HpTorso* h, HpPrecond* p, const floa
     ret = pcg_solve(h, tol_exact, HP_STOP_REL, 20000, nullptr, &res, s);
     if (ret != HP_OK) break;
     if (cudaMemcpyAsync(xstar, a.x, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
+    // one plain-PCG trajectory from the warm start; pairs at iterations ks
+    // (ascending): r_k (the recursion's residual) and e_k = x* - x_k
+    if (cudaMemcpyAsync(a.x, x0, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
+    true_residual<<<h->nblk, TB, 0, s>>>(a, 1);     // r = b - A x0, fresh recursion
+    int done = 0;
     for (int kq = 0; kq < n_ks && ret == HP_OK; ++kq) {
-      if (cudaMemcpyAsync(a.x, x0, a.ng * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) { ret = HP_ERR_CUDA; break; }
-      if (ks[kq] > 0) {
-        // exactly ks[kq] plain iterations; r ends as the true residual of x_k
-        ret = pcg_solve(h, 1e-300, HP_STOP_REL, ks[kq], nullptr, &res, s);
+      if (ks[kq] > done) {
+        ret = pcg_continue(h, ks[kq] - done, s);
         if (ret != HP_OK) break;
-      } else {
-        true_residual<<<h->nblk, TB, 0, s>>>(a, 1);
+        done = ks[kq];
       }
       error_kernel<<<h->nblk, TB, 0, s>>>(a, xstar, e);
       for (int rp = 0; rp < repeats && ret == HP_OK; ++rp) {

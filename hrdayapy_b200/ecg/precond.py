@@ -121,7 +121,7 @@ class LearnedPreconditioner:
     def train(self, vm_frames_dev, ks=(0, 2, 8, 32, 96), repeats=2, lr=1e-3, tol_exact=1e-8):
         """vm_frames_dev: CUDA tensor (n_frames, n_heart) float32 (mV)."""
         n_frames = int(vm_frames_dev.shape[0])
-        ks = np.ascontiguousarray(ks, np.int32)
+        ks = np.ascontiguousarray(np.sort(np.asarray(ks)), np.int32)
         hist = np.zeros(n_frames * len(ks) * repeats, np.float32)
         _lib.check(_lib.lib().hp_torso_train_precond(
             self.solver.h, self.h, C.c_void_p(vm_frames_dev.data_ptr()),
