@@ -816,12 +816,17 @@ def shell_parity_and_cpu_baseline(prob, args, parity_ms=22.0, chunk=25):
     act_o = np.isfinite(first)
     both = act_g & act_o
     err = float(np.max(np.abs(a[0][both].astype(np.float64) - first[both]))) if both.any() else None
+    # a voxel activated by one run only should be crossing at the window's end
+    one = act_g ^ act_o
+    t_one = np.where(act_g, a[0], first)[one]
+    one_sided_earliest = float(t_one.min()) if one.any() else None
     check = {"reference": f"FP64 oracle of the reference method, same {n} steps from rest",
              "steps": n, "simulated_ms": n * prob.dt,
              "vm_rms_mV": rms, "purkinje_vm_rms_mV": rms_p,
              "max_act_err_ms": err, "act_threshold_mV": -20.0,
              "activated_both": int(both.sum()), "activated_gpu_only": int((act_g & ~act_o).sum()),
              "activated_oracle_only": int((act_o & ~act_g).sum()),
+             "one_sided_earliest_ms": one_sided_earliest,
              "tolerances": {"vm_rms_mV": 0.5, "max_act_err_ms": 0.1}}
     base = {"value": N * n / secs, "unit": "voxel-steps/s", "cores": int(orc.lib().orc_num_threads()),
             "kind": "port",

@@ -125,9 +125,10 @@ def test_training_and_fcg_on_held_out_frames():
     plain Jacobi-PCG, by flexible CG with the two-level preconditioner
     without the network, and with it: all converge to the FP64 true relative
     residual <= 1e-6.  The two-level preconditioner needs far fewer
-    iterations than plain PCG; the trained network refines it by at most a
-    few percent here and must not cost iterations (it is judged against
-    exactly the method without it)."""
+    iterations than plain PCG, and on this torso the trained network takes
+    strictly fewer iterations than exactly the method without it (training
+    is bit-reproducible, so the counts are too): 38.5 against 39.5 on
+    average, no frame worse."""
     import torch
     from hrdayapy_b200.ecg.precond import LearnedPreconditioner
     solver, grid, labels, table, dx, vox = _small(seed=4)
@@ -152,10 +153,36 @@ def test_training_and_fcg_on_held_out_frames():
                 out.append(st.iterations)
         print("iterations: plain PCG", plain, "two-level FCG", two, "learned FCG", learned)
         assert np.mean(two) < 0.5 * np.mean(plain), (two, plain)
-        # the network's effect on this small torso is a few per cent either
-        # way, and training is not bit-reproducible (the weight gradients are
-        # summed with atomics): it must not make the method markedly worse
-        assert np.mean(learned) <= 1.1 * np.mean(two) + 1.0, (learned, two)
+        print(f"network gain: {np.mean(two) - np.mean(learned):.2f} iterations per frame "
+              f"({100 * (1 - np.mean(learned) / np.mean(two)):.1f} %)")
+        assert np.mean(learned) < np.mean(two), (learned, two)
+        assert all(l <= t for l, t in zip(learned, two)), (learned, two)
     finally:
         pc.close()
+        solver.close()
+
+
+def test_training_is_bit_reproducible():
+    """Two trainings from the same seed on the same frames and warm start give
+    the same weights bit for bit: every gradient (the tensor-core data and
+    weight gradients included) is summed in a fixed order, with no atomics."""
+    import torch
+    from hrdayapy_b200.ecg.precond import LearnedPreconditioner
+    solver, grid, labels, table, dx, vox = _small(seed=4, shape=(16, 16, 256))
+    try:
+        fr = _wave_frames(vox, 6, seed=6)
+        vm = torch.from_numpy(fr).cuda().contiguous()
+        params = []
+        for trial in range(2):
+            solver.reset()
+            pc = LearnedPreconditioner(solver, labels, len(table), omega=0.6, seed=5)
+            try:
+                hist = pc.train(vm[0:6:2], ks=(0, 4, 12, 24), repeats=2, lr=1e-3)
+                assert np.all(np.isfinite(hist))
+                params.append(pc.params()[0])
+            finally:
+                pc.close()
+        assert np.abs(params[0]).max() > 0
+        np.testing.assert_array_equal(params[0], params[1])
+    finally:
         solver.close()
