@@ -68,6 +68,10 @@ struct TorsoArgs {
   int32_t n_lines;
   const int64_t* line_g0;
   const int32_t* line_len;
+  // the 32-cell, 128-byte aligned chunks of the padded grid that hold a
+  // tissue-line cell (each once; vectors are allocated to a multiple of 32)
+  int32_t n_chunks;
+  const int32_t* chunk;
   // label | LAB_UNIFORM when all six neighbours carry the cell's own label
   const uint8_t* label_u;
 };
@@ -179,8 +183,35 @@ __device__ __forceinline__ void for_line_batches(const TorsoArgs& a, Load&& load
   }
 }
 
+// The same over the chunk list: a warp takes U whole 32-cell chunks at a
+// time, all loads issued before any arithmetic, every access a full
+// 128-byte row segment.  Cells of a chunk outside every tissue line (air,
+// the ends of the neighbouring rows) carry zeros in every vector and invd,
+// so the updates leave them zero and they add nothing to the sums.
+template <int U, class Load, class Apply>
+__device__ __forceinline__ void for_chunk_batches(const TorsoArgs& a, Load&& load, Apply&& apply) {
+  const int lane = threadIdx.x & 31;
+  const int n_warps = gridDim.x * (TB / 32);
+  const int w = blockIdx.x * (TB / 32) + (threadIdx.x >> 5);
+  for (int c0 = w * U; c0 < a.n_chunks; c0 += n_warps * U) {
+    int64_t g[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      g[u] = c0 + u < a.n_chunks ? (int64_t)a.chunk[c0 + u] * 32 + lane : -1;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (g[u] >= 0) load(u, g[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (g[u] >= 0) apply(u, g[u]);
+  }
+}
+
 // Iteration part 1a: pending x update and p <- M^-1 r + beta p, in place
-// (every thread reads and writes only its own cells).
+// (every thread reads and writes only its own cells), over the chunk list
+// (measured on the full torso: 28.7 us against 31.5 us over the tissue
+// lines; the r update, with its FP64 sums, keeps the line batches of 8,
+// which measured 24.2 us against 31.3 us over chunks).
 __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha_prev = a.scal[SC_ALPHA_PREV];
@@ -193,14 +224,14 @@ __global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
   float pv[LB], zv[LB];
   if (alpha_prev != 0.0) {
     double xv[LB];
-    for_line_batches<LB>(
+    for_chunk_batches<LB>(
         a, [&](int u, int64_t g) { pv[u] = p[g]; zv[u] = invd[g] * r[g]; xv[u] = x[g]; },
         [&](int u, int64_t g) {
           x[g] = xv[u] + alpha_prev * (double)pv[u];
           p[g] = zv[u] + betaf * pv[u];
         });
   } else {
-    for_line_batches<LB>(
+    for_chunk_batches<LB>(
         a, [&](int u, int64_t g) { pv[u] = p[g]; zv[u] = invd[g] * r[g]; },
         [&](int u, int64_t g) { p[g] = zv[u] + betaf * pv[u]; });
   }
@@ -717,20 +748,24 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   HP_CUDA_TRY(cudaMemcpyToSymbolAsync(c_T64, T64, sizeof(T64), 0, cudaMemcpyHostToDevice, s));
   TorsoArgs& a = h->a;
   a.ng = ng; a.pj = PJ; a.pk = PK; a.pin = pin_g; a.n_rows = n_rows;
+  // the vectors and invd extend to a multiple of 32 cells (whole chunks),
+  // zero past the grid
+  const int64_t ng32 = (ng + 31) / 32 * 32;
+  invd.resize(ng32, 0.0f);
   TT_TRY(tup(h, (uint8_t**)&a.label, lab.data(), ng, s));
-  TT_TRY(tup(h, (float**)&a.invd, invd.data(), ng, s));
-  TT_TRY(tal(h, &a.r, ng));
-  TT_TRY(tal(h, &a.p0, ng));
-  TT_TRY(tal(h, &a.p1, ng));
-  TT_TRY(tal(h, &a.Ap, ng));
-  TT_TRY(tal(h, &a.x, ng));
-  TT_TRY(tal(h, &a.b, ng));
-  HP_CUDA_TRY(cudaMemsetAsync(a.r, 0, ng * 4, s));
-  HP_CUDA_TRY(cudaMemsetAsync(a.p0, 0, ng * 4, s));
-  HP_CUDA_TRY(cudaMemsetAsync(a.p1, 0, ng * 4, s));
-  HP_CUDA_TRY(cudaMemsetAsync(a.Ap, 0, ng * 4, s));
-  HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, ng * 8, s));
-  HP_CUDA_TRY(cudaMemsetAsync(a.b, 0, ng * 4, s));
+  TT_TRY(tup(h, (float**)&a.invd, invd.data(), ng32, s));
+  TT_TRY(tal(h, &a.r, ng32));
+  TT_TRY(tal(h, &a.p0, ng32));
+  TT_TRY(tal(h, &a.p1, ng32));
+  TT_TRY(tal(h, &a.Ap, ng32));
+  TT_TRY(tal(h, &a.x, ng32));
+  TT_TRY(tal(h, &a.b, ng32));
+  HP_CUDA_TRY(cudaMemsetAsync(a.r, 0, ng32 * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.p0, 0, ng32 * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.p1, 0, ng32 * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.Ap, 0, ng32 * 4, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.x, 0, ng32 * 8, s));
+  HP_CUDA_TRY(cudaMemsetAsync(a.b, 0, ng32 * 4, s));
   int nsm = 148;
   {
     int dev = 0;
@@ -782,6 +817,14 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
         }
       }
     a.n_lines = (int32_t)g0.size();
+    // chunks: the 32-cell aligned blocks that a tissue line touches, each once
+    std::vector<int32_t> chunks;
+    for (size_t L = 0; L < g0.size(); ++L) {
+      const int64_t c0 = g0[L] >> 5, c1 = (g0[L] + len[L] - 1) >> 5;
+      for (int64_t c = c0; c <= c1; ++c)
+        if (chunks.empty() || chunks.back() < (int32_t)c) chunks.push_back((int32_t)c);
+    }
+    a.n_chunks = (int32_t)chunks.size();
     std::vector<uint8_t> lab_u(lab);
     for (int64_t r = 0; r < n_rows; ++r) {
       const int64_t g = grid_of_row[r];
@@ -794,7 +837,8 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
 
     TT_TRY(tup(h, (int64_t**)&a.line_g0, g0.data(), g0.size(), s));
     TT_TRY(tup(h, (int32_t**)&a.line_len, len.data(), len.size(), s));
-    HP_CUDA_TRY(cudaStreamSynchronize(s));  // g0 / len are stack temporaries
+    TT_TRY(tup(h, (int32_t**)&a.chunk, chunks.data(), chunks.size(), s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));  // g0 / len / chunks are stack temporaries
   }
   // heart sources: segments of heart voxels per receiving row
   SrcArgs& sa = h->s;
