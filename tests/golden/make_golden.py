@@ -29,6 +29,9 @@ Fixtures (all seeded, small enough to commit):
 * torso.npz         -- _assemble_stiffness / _find_surface_ids on a small
                        synthetic torso, build_heart_laplacian /
                        build_projection_map, and solve_frame on one Vm frame.
+* transmural.npz    -- generate_transmural_coordinate on a small truncated
+                       ellipsoidal shell (epicardium +1, endocardium -1,
+                       a Neumann base plane).
 * bspm_loop.npz     -- the upstream chain end to end: run_coupled (theta 0,
                        FP64) writes vm_snapshots.npz of a 24x24x8 slab at
                        0.5 mm (1 ms frames), run_bspm_loop solves every frame
@@ -342,6 +345,37 @@ def bspm_loop():
                         sigma_vals=np.array(list(sig_map.values())), **out)
 
 
+def transmural_case():
+    """Truncated ellipsoidal shell with its surface labels (restated in the
+    tests): +1 on myocardial voxels touching the exterior, -1 on those
+    touching the cavity, nothing on the cut base plane."""
+    from scipy import ndimage as ndi
+    n = (30, 26, 24)
+    ii, jj, kk = np.indices(n).astype(np.float64)
+    r = np.sqrt(((ii - 14.5) / 13.0) ** 2 + ((jj - 12.5) / 11.0) ** 2 + ((kk - 6.0) / 16.0) ** 2)
+    outer, inner = r <= 1.0, r <= 0.62
+    S = (outer & ~inner & (kk <= 19)).astype(np.uint8)
+    cav = inner & (kk <= 19)
+    ext = ~outer
+    st = ndi.generate_binary_structure(3, 1)
+    lab = np.zeros(n, np.int8)
+    lab[(S == 1) & ndi.binary_dilation(ext, st)] = 1
+    lab[(S == 1) & ndi.binary_dilation(cav, st)] = -1
+    return S, lab
+
+
+def transmural():
+    hp = _refload.REF_ROOT / "hrdayapy"
+    _refload._pkg("hrdayapy.coordinates", hp / "coordinates")
+    _refload._pkg("hrdayapy.coordinates.functions", hp / "coordinates" / "functions")
+    mod = _refload._load("hrdayapy.coordinates.functions.generate_transmural_coordinate",
+                         hp / "coordinates" / "functions" / "generate_transmural_coordinate.py")
+    S, lab = transmural_case()
+    phi = quiet(mod.generate_transmural_coordinate, S, lab, device="cpu", tol=1e-8,
+                maxiter=20000)
+    np.savez_compressed(HERE / "transmural.npz", S=S, surface_label=lab, phi=phi)
+
+
 def act_maps():
     """The upstream activation-map writer on upstream snapshots; keys are
     prefixed "slab_" (340 ms isotropic run, thresholds -20 / -60 mV) and
@@ -436,9 +470,10 @@ def pmj_exp4():
 
 if __name__ == "__main__":
     torch.set_num_threads(8)
-    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso", "bspm"]
+    which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso", "bspm",
+                             "transmural"]
     for w in which:
         print("generating", w, flush=True)
         {"cells": ttp06_cells, "pacing": ttp06_pacing, "iso": mono_iso,
          "aniso": mono_aniso, "maps": act_maps, "pmj": pmj_exp4, "torso": torso,
-         "bspm": bspm_loop}[w]()
+         "bspm": bspm_loop, "transmural": transmural}[w]()
