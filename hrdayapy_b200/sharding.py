@@ -53,3 +53,24 @@ def gather_to_all(obj):
     out = [None] * dist.get_world_size()
     dist.all_gather_object(out, obj)
     return out
+
+
+def shard_run_gather(sizes, run_share):
+    """Deals the variants (expected work `sizes`) to the ranks of the
+    default process group by longest-processing-time-first, runs
+    run_share(indices) on each rank -- it returns one result per index, in
+    the order given -- and returns every variant's result in variant order
+    on every rank.  Without a process group the one rank runs them all."""
+    import torch.distributed as dist
+    on = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size() if on else 1
+    rank = dist.get_rank() if on else 0
+    share = lpt_assign(sizes, world)[rank]
+    res = list(run_share(share))
+    if len(res) != len(share):
+        raise ValueError(f"run_share returned {len(res)} results for {len(share)} variants")
+    out = [None] * len(sizes)
+    for g in gather_to_all({"variants": share, "results": res}):
+        for v, r in zip(g["variants"], g["results"]):
+            out[v] = r
+    return out
