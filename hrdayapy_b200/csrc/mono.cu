@@ -246,6 +246,78 @@ __device__ __forceinline__ void purkinje_part(const MonoArgs& a, int p, int64_t 
   }
 }
 
+// Operator sum of one voxel from its operands, in one fixed order of
+// explicitly rounded operations, so every kernel that feeds it (shared-memory
+// tiles, registers) gets bit-identical results.  nv(q) is the value of
+// neighbour q: the faces +i, -i, +j, -j, +k, -k (q = 0..5), then the twelve
+// edge neighbours in diagonal-bit order (q = 6..17); wf(f) the weight of face
+// f; tc(e) and tn(e) the off-diagonal tensor component of edge term e at the
+// voxel and at its edge neighbour.  Face and diagonal bits of the tag gate
+// every term.  The co-signed edge pairs (+,+)/(-,-) carry +avg, the
+// counter-signed ones -avg (bit e has the minus sign when e & 2).
+// DIAG: every difference reads -1, so the sum is the operator's diagonal.
+template <bool ANISO, bool DIAG, class NV, class WF, class TC, class TN>
+__device__ __forceinline__ float stencil_sum(float iso_coef, uint32_t tag, float Vc, NV&& nv,
+                                             WF&& wf, TC&& tc, TN&& tn) {
+#define HP_DV(x) (DIAG ? -1.0f : __fsub_rn((x), Vc))
+  const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
+  float acc = 0.0f;
+  if constexpr (!ANISO) {
+    float s = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+      if (fb & (1u << f)) s = __fadd_rn(s, HP_DV(nv(f)));
+    acc = __fmul_rn(iso_coef, s);
+  } else {
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+      if (fb & (1u << f)) acc = __fmaf_rn(wf(f), HP_DV(nv(f)), acc);
+    const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
+#pragma unroll
+    for (int e = 0; e < 12; ++e)
+      if (db & (1u << e))
+        acc = __fmaf_rn(__fmul_rn((e & 2) ? -0.25f : 0.25f, __fadd_rn(tc(e), tn(e))),
+                        HP_DV(nv(6 + e)), acc);
+  }
+#undef HP_DV
+  return acc;
+}
+
+// Junction currents of a voxel tagged HP_TAG_PMJ (Purkinje potentials from
+// Wpk) added to acc; DIAG as in stencil_sum.
+template <bool DIAG>
+__device__ __forceinline__ float pmj_sum(const MonoArgs& a, float acc, float Vc, int64_t slot,
+                                         const float* __restrict__ Wpk) {
+  const int r = a.pmj_row[slot];
+  for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
+    acc = __fmaf_rn(a.pmj_coef[q], DIAG ? -1.0f : __fsub_rn(Wpk[a.pmj_pk[q]], Vc), acc);
+  return acc;
+}
+
+// Neighbour offset q (stencil_sum order) in a tile with strides SI (i), SJ
+// (j), 1 (k).
+template <int SI, int SJ>
+__host__ __device__ constexpr int stencil_off(int q) {
+  return q == 0    ? SI
+         : q == 1  ? -SI
+         : q == 2  ? SJ
+         : q == 3  ? -SJ
+         : q == 4  ? 1
+         : q == 5  ? -1
+         : q == 6  ? SI + SJ
+         : q == 7  ? -SI - SJ
+         : q == 8  ? SI - SJ
+         : q == 9  ? -SI + SJ
+         : q == 10 ? SI + 1
+         : q == 11 ? -SI - 1
+         : q == 12 ? SI - 1
+         : q == 13 ? -SI + 1
+         : q == 14 ? SJ + 1
+         : q == 15 ? -SJ - 1
+         : q == 16 ? SJ - 1
+                   : -SJ + 1;
+}
+
 // Stencil sum of one voxel, sum_j coef_ij (W_j - W_i) including its junction
 // currents (Purkinje potentials from Wpk), from shared tiles with strides SI
 // (i), SJ (j), 1 (k); face weights and off-diagonal tensor components are
@@ -254,58 +326,16 @@ template <int SI, int SJ, int NS, bool ANISO, bool DIAG = false>
 __device__ __forceinline__ float stencil_acc(const MonoArgs& a, const float* tV, const float* tW,
                                              const float* tD, int c, uint32_t tag, int64_t slot,
                                              const float* __restrict__ Wpk) {
-  // DIAG: every difference reads -1, so the sum is the operator's diagonal
-#define HP_DV(x) (DIAG ? -1.0f : ((x) - Vc))
   const float Vc = DIAG ? 0.0f : tV[c];
-  float acc = 0.0f;
-  const uint32_t fb = tag >> HP_TAG_FACE_SHIFT;
-  if constexpr (!ANISO) {
-    float s = 0.0f;
-    if (fb & 1u) s += HP_DV(tV[c + SI]);
-    if (fb & 2u) s += HP_DV(tV[c - SI]);
-    if (fb & 4u) s += HP_DV(tV[c + SJ]);
-    if (fb & 8u) s += HP_DV(tV[c - SJ]);
-    if (fb & 16u) s += HP_DV(tV[c + 1]);
-    if (fb & 32u) s += HP_DV(tV[c - 1]);
-    acc = a.iso_coef * s;
-  } else {
-    const float* tWx = tW;
-    const float* tWy = tW + NS;
-    const float* tWz = tW + 2 * NS;
-    if (fb & 1u) acc += tWx[c] * HP_DV(tV[c + SI]);
-    if (fb & 2u) acc += tWx[c - SI] * HP_DV(tV[c - SI]);
-    if (fb & 4u) acc += tWy[c] * HP_DV(tV[c + SJ]);
-    if (fb & 8u) acc += tWy[c - SJ] * HP_DV(tV[c - SJ]);
-    if (fb & 16u) acc += tWz[c] * HP_DV(tV[c + 1]);
-    if (fb & 32u) acc += tWz[c - 1] * HP_DV(tV[c - 1]);
-    const uint32_t db = tag >> HP_TAG_DIAG_SHIFT;
-    const float* t01 = tD;
-    const float* t02 = tD + NS;
-    const float* t12 = tD + 2 * NS;
-    // co-signed pairs (+,+)/(-,-) carry +avg, counter-signed (+,-)/(-,+) -avg
-#define HP_DIAG(bit, T, OFF, SGN)                                            \
-  if (db & (1u << (bit))) acc += (SGN) * 0.25f * (T[c] + T[c + (OFF)]) *      \
-                                 HP_DV(tV[c + (OFF)]);
-    HP_DIAG(0, t01, SI + SJ, 1.0f)
-    HP_DIAG(1, t01, -SI - SJ, 1.0f)
-    HP_DIAG(2, t01, SI - SJ, -1.0f)
-    HP_DIAG(3, t01, -SI + SJ, -1.0f)
-    HP_DIAG(4, t02, SI + 1, 1.0f)
-    HP_DIAG(5, t02, -SI - 1, 1.0f)
-    HP_DIAG(6, t02, SI - 1, -1.0f)
-    HP_DIAG(7, t02, -SI + 1, -1.0f)
-    HP_DIAG(8, t12, SJ + 1, 1.0f)
-    HP_DIAG(9, t12, -SJ - 1, 1.0f)
-    HP_DIAG(10, t12, SJ - 1, -1.0f)
-    HP_DIAG(11, t12, -SJ + 1, -1.0f)
-#undef HP_DIAG
-  }
-  if (tag & HP_TAG_PMJ) {
-    const int r = a.pmj_row[slot];
-    for (int q = a.pmj_ptr[r]; q < a.pmj_ptr[r + 1]; ++q)
-      acc += a.pmj_coef[q] * HP_DV(Wpk[a.pmj_pk[q]]);
-  }
-#undef HP_DV
+  float acc = stencil_sum<ANISO, DIAG>(
+      a.iso_coef, tag, Vc, [&](int q) { return tV[c + stencil_off<SI, SJ>(q)]; },
+      [&](int f) {
+        // face weights live on the lower voxel of each face
+        return tW[(f >> 1) * NS + c - ((f & 1) ? (f == 1 ? SI : (f == 3 ? SJ : 1)) : 0)];
+      },
+      [&](int e) { return tD[(e >> 2) * NS + c]; },
+      [&](int e) { return tD[(e >> 2) * NS + c + stencil_off<SI, SJ>(6 + e)]; });
+  if (tag & HP_TAG_PMJ) acc = pmj_sum<DIAG>(a, acc, Vc, slot, Wpk);
   return acc;
 }
 
@@ -316,7 +346,7 @@ __device__ __forceinline__ float diffuse(const MonoArgs& a, const float* tV, con
                                          bool odd) {
   const float acc = stencil_acc<SI, SJ, NS, ANISO>(a, tV, tW, tD, c, tag, slot,
                                                    odd ? a.pk_Vs1 : a.pk_Vs0);
-  return fminf(fmaxf(tV[c] + acc, -150.0f), 80.0f);
+  return fminf(fmaxf(__fadd_rn(tV[c], acc), -150.0f), 80.0f);
 }
 
 // Outputs of a tissue voxel once V_{i+1} = Vn is known: the
