@@ -35,6 +35,17 @@
 namespace hp {
 
 constexpr int TB = 256;            // threads per block
+// resident blocks per SM the register budgets of the iteration kernels are
+// sized for (1: the compiler's choice)
+#ifndef HP_AP_MINB
+#define HP_AP_MINB 4  // pcg_ap: 64 registers (86.2 us per iteration on the full torso, 89.4 at 80)
+#endif
+#ifndef HP_K2_MINB
+#define HP_K2_MINB 1
+#endif
+#ifndef HP_PU_MINB
+#define HP_PU_MINB 1
+#endif
 constexpr int NPART = 4;           // partial sums per block
 
 enum Scal : int {
@@ -72,11 +83,15 @@ struct TorsoArgs {
   // tissue-line cell (each once; vectors are allocated to a multiple of 32)
   int32_t n_chunks;
   const int32_t* chunk;
-  // label | LAB_UNIFORM when all six neighbours carry the cell's own label
+  // label | LAB_UNIFORM when all six neighbours carry the cell's own label,
+  // | LAB_PIN at the pinned voxel
   const uint8_t* label_u;
 };
 
 constexpr int LAB_UNIFORM = 0x80;
+constexpr int LAB_PIN = 0x40;
+constexpr int LAB_MASK = 0x3F;  // the material label (< HP_MAX_MATERIALS)
+static_assert(HP_MAX_MATERIALS <= LAB_MASK + 1, "material labels must fit under the flag bits");
 
 __constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
 __constant__ double c_T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
@@ -212,7 +227,7 @@ __device__ __forceinline__ void for_chunk_batches(const TorsoArgs& a, Load&& loa
 // (measured on the full torso: 28.7 us against 31.5 us over the tissue
 // lines; the r update, with its FP64 sums, keeps the line batches of 8,
 // which measured 24.2 us against 31.3 us over chunks).
-__global__ void __launch_bounds__(TB) pcg_p_update(TorsoArgs a) {
+__global__ void __launch_bounds__(TB, HP_PU_MINB) pcg_p_update(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha_prev = a.scal[SC_ALPHA_PREV];
   const float betaf = (float)a.scal[SC_BETA];
@@ -268,10 +283,9 @@ __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, C
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
   const int sj = a.pk, si = a.pj * a.pk;   // even; the padded plane fits in 32 bits
-  const int64_t pin = a.pin;
   const int lane = threadIdx.x & 31;
   const int n_warps = gridDim.x * (TB / 32);
-  constexpr int M = LAB_UNIFORM - 1;
+  constexpr int M = LAB_MASK;
   for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
     const int64_t g0 = a.line_g0[L];
     const int64_t ga = g0 & ~(int64_t)1;                  // even start
@@ -305,17 +319,22 @@ __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, C
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int l = lf[e] & M;
-        int ln[6] = {l, l, l, l, l, l};
-        if (!(lf[e] & LAB_UNIFORM)) {
+        // face conductances: one table entry inside a material region
+        float tf[6];
+        if (lf[e] & LAB_UNIFORM) {
+          const float t = T[l * (HP_MAX_MATERIALS + 1)];
+#pragma unroll
+          for (int f = 0; f < 6; ++f) tf[f] = t;
+        } else {
           const uint8_t* __restrict__ le = lab + c + e;
           const int off[6] = {si, -si, sj, -sj, 1, -1};
 #pragma unroll
-          for (int f = 0; f < 6; ++f) ln[f] = le[off[f]] & M;
+          for (int f = 0; f < 6; ++f) tf[f] = T[l * HP_MAX_MATERIALS + (le[off[f]] & M)];
         }
         float ap = 0.0f;
 #pragma unroll
-        for (int f = 0; f < 6; ++f) ap += T[l * HP_MAX_MATERIALS + ln[f]] * (pv[e] - pn0[e][f]);
-        if (l == 0 || c + e == pin) ap = 0.0f;
+        for (int f = 0; f < 6; ++f) ap += tf[f] * (pv[e] - pn0[e][f]);
+        if (l == 0 || (lf[e] & LAB_PIN)) ap = 0.0f;
         ap2[e] = ap;
       }
       *(float2*)(Ap + c) = make_float2(ap2[0], ap2[1]);
@@ -333,7 +352,6 @@ __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const floa
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
   const int sj = a.pk, si = a.pj * a.pk;   // the padded plane fits in 32 bits
-  const int64_t pin = a.pin;
   const int lane = threadIdx.x & 31;
   const int n_warps = gridDim.x * (TB / 32);
   for (int L = blockIdx.x * (TB / 32) + (threadIdx.x >> 5); L < a.n_lines; L += n_warps) {
@@ -345,22 +363,26 @@ __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const floa
       const float* __restrict__ pc = p + g;
       const int off[6] = {si, -si, sj, -sj, 1, -1};
       const int lf = lc[0];
-      const int l = lf & (LAB_UNIFORM - 1);
+      const int l = lf & LAB_MASK;
       const float pg = pc[0];
       float pn[6];
 #pragma unroll
       for (int f = 0; f < 6; ++f) pn[f] = pc[off[f]];
-      // inside a material region every face has the same conductance: the
-      // neighbours' labels are read only at material boundaries
-      int ln[6] = {l, l, l, l, l, l};
-      if (!(lf & LAB_UNIFORM)) {
+      // inside a material region every face has the same conductance: one
+      // table entry, and the neighbours' labels are read only at boundaries
+      float tf[6];
+      if (lf & LAB_UNIFORM) {
+        const float t = T[l * (HP_MAX_MATERIALS + 1)];
 #pragma unroll
-        for (int f = 0; f < 6; ++f) ln[f] = lc[off[f]] & (LAB_UNIFORM - 1);
+        for (int f = 0; f < 6; ++f) tf[f] = t;
+      } else {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) tf[f] = T[l * HP_MAX_MATERIALS + (lc[off[f]] & LAB_MASK)];
       }
       float ap = 0.0f;
 #pragma unroll
-      for (int f = 0; f < 6; ++f) ap += T[l * HP_MAX_MATERIALS + ln[f]] * (pg - pn[f]);
-      if (l == 0 || g == pin) ap = 0.0f;
+      for (int f = 0; f < 6; ++f) ap += tf[f] * (pg - pn[f]);
+      if (l == 0 || (lf & LAB_PIN)) ap = 0.0f;
       Ap[g] = ap;
       cell(g, pg, ap);
     }
@@ -368,7 +390,7 @@ __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const floa
 }
 
 template <bool PAIRS>
-__global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
+__global__ void __launch_bounds__(TB, HP_AP_MINB) pcg_ap(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
   for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
@@ -407,7 +429,7 @@ __global__ void __launch_bounds__(TB) pcg_ap(TorsoArgs a) {
 // m_lt (an upper bound of the quantile, below tol) or m_ge (a lower bound,
 // not below tol).
 template <bool P99>
-__global__ void __launch_bounds__(TB) pcg_k2(TorsoArgs a) {
+__global__ void __launch_bounds__(TB, HP_K2_MINB) pcg_k2(TorsoArgs a) {
   if (a.iscal[IS_DONE]) return;
   const double alpha = a.scal[SC_ALPHA];
   const float alphaf = (float)alpha;
@@ -833,6 +855,7 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
       for (int f = 0; f < 6; ++f) uni = uni && lab[nb[f]] == lab[g];
       if (uni) lab_u[g] |= (uint8_t)LAB_UNIFORM;
     }
+    lab_u[pin_g] |= (uint8_t)LAB_PIN;
     TT_TRY(tup(h, (uint8_t**)&a.label_u, lab_u.data(), lab_u.size(), s));
 
     TT_TRY(tup(h, (int64_t**)&a.line_g0, g0.data(), g0.size(), s));
