@@ -86,7 +86,7 @@ class HpTorsoDesc(C.Structure):
         ("ni", C.c_int32), ("nj", C.c_int32), ("nk", C.c_int32), ("h_m", C.c_double),
         ("label", P), ("n_materials", C.c_int32), ("sigma", P), ("pin_row", C.c_int64),
         ("n_heart", C.c_int32), ("heart_nbr", P), ("proj", P), ("coeff", C.c_double),
-        ("n_expected", C.c_double), ("n_read", C.c_int32), ("read_rows", P),
+        ("n_expected", C.c_double), ("n_read", C.c_int32), ("read_rows", P), ("psi", P),
     ]
 
 

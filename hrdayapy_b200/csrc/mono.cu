@@ -539,6 +539,11 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// waits until at most N of this thread's most recent groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_pending() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 template <int BI, int BJ, int BK, bool ANISO>
 __device__ __forceinline__ void pipe_issue(const MonoArgs& a, float* stage, const uint32_t* tab,
@@ -785,14 +790,22 @@ struct DiffHalo {
 };
 
 // Shared-memory stage of the diffusion kernel: the staged tiles, then the
-// brick's tags and V_i.
+// brick's tags and V_i.  NS stages are in flight or in use per CTA (the
+// bricks of NS - 1 stages stream in while one is computed), and the
+// neighbour lists of the next RING bricks ride along in the same groups.
+#ifndef HP_DIFF_STAGES
+#define HP_DIFF_STAGES 2
+#endif
 template <int BI, int BJ, int BK, bool ANISO>
 struct DiffStage {
   using G = PipeGeom<BI, BJ, BK>;
+  static constexpr int NS = HP_DIFF_STAGES;
+  static constexpr int RING = 2 * NS;
   static constexpr int NF = ANISO ? 7 : 1;
   static constexpr int TAG = NF * G::NT;
   static constexpr int VP = TAG + G::BV;
   static constexpr int FLOATS = VP + G::BV;
+  static constexpr int SMEM_FLOATS = NS * FLOATS + 27 * RING;  // + the neighbour-list ring
   static constexpr int NCHUNK = (NF + 2) * G::BV / 4;  // 16-byte own-brick copies
 };
 
@@ -840,9 +853,10 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
   constexpr int QB = BV / 4;  // 16-byte chunks per brick row of one field
   // per-slot fields after the tiles: tag, then V_i (step) or Dinv (start)
   constexpr int NCHUNK = OP == OP_CN_APPLY ? (NF + 1) * BV / 4 : D::NCHUNK;
+  constexpr int NS = D::NS, RS = D::RING;
   extern __shared__ __align__(16) float smem[];
-  float* stages = smem;                     // 2 x FLOATS
-  int* ring = (int*)(smem + 2 * D::FLOATS);  // 2 x 27 neighbour lists
+  float* stages = smem;                       // NS x FLOATS
+  int* ring = (int*)(smem + NS * D::FLOATS);  // RS x 27 neighbour lists
   __shared__ int64_t s_vm_frame, s_anim_frame;
   if (OP == OP_CN_APPLY && cn.iscal[CI_DONE]) return;
   const int64_t step = *a.d_step + step_off;
@@ -911,27 +925,42 @@ __device__ __forceinline__ void diffuse_pass(const MonoArgs a, const CnArgs cn, 
     s_anim_frame = (a.frame_every > 0 && step % a.frame_every == 0) ? step / a.frame_every : -1;
   }
   double v[3] = {0.0, 0.0, 0.0};  // CN sums
+  // item m of this CTA is blockIdx.x + m G_, staged in stage m % NS; its
+  // neighbour list sits in ring slot m % RS, fetched together with item
+  // m - (NS - 1) (the first NS - 1 lists are loaded directly), so it is
+  // complete by the time item m is issued
   int cur = blockIdx.x;
-  if (cur < a.n_bricks && tid < 27) ring[tid] = a.nbr[(int64_t)cur * 27 + tid];
-  __syncthreads();
-  if (cur < a.n_bricks) {
-    issue(stages, ring, cur);
-    const int nx = cur + G_;
-    if (nx < a.n_bricks && tid < 27) cp_async4(ring + 27 + tid, a.nbr + (int64_t)nx * 27 + tid);
+#pragma unroll
+  for (int m = 0; m < NS - 1; ++m) {
+    const int it = cur + m * G_;
+    if (it < a.n_bricks && tid < 27) ring[(m % RS) * 27 + tid] = a.nbr[(int64_t)it * 27 + tid];
   }
-  cp_async_commit();
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < NS - 1; ++m) {
+    const int it = cur + m * G_;
+    if (it < a.n_bricks) {
+      issue(stages + m * D::FLOATS, ring + (m % RS) * 27, it);
+      const int ahead = it + (NS - 1) * G_;
+      if (ahead < a.n_bricks && tid < 27)
+        cp_async4(ring + ((m + NS - 1) % RS) * 27 + tid, a.nbr + (int64_t)ahead * 27 + tid);
+    }
+    cp_async_commit();
+  }
   for (int n = 0; cur < n_items; ++n, cur += G_) {
-    cp_async_wait_all();
+    cp_async_wait_pending<NS - 2>();  // item n has landed
     __syncthreads();
-    const int nxt = cur + G_;
-    if (nxt < a.n_bricks) {
-      issue(stages + ((n + 1) & 1) * D::FLOATS, ring + ((n + 1) & 1) * 27, nxt);
-      const int nn = nxt + G_;
-      if (nn < a.n_bricks && tid < 27) cp_async4(ring + (n & 1) * 27 + tid, a.nbr + (int64_t)nn * 27 + tid);
+    const int m = n + NS - 1;
+    const int it = cur + (NS - 1) * G_;
+    if (it < a.n_bricks) {
+      issue(stages + (m % NS) * D::FLOATS, ring + (m % RS) * 27, it);
+      const int ahead = it + (NS - 1) * G_;
+      if (ahead < a.n_bricks && tid < 27)
+        cp_async4(ring + ((m + NS - 1) % RS) * 27 + tid, a.nbr + (int64_t)ahead * 27 + tid);
     }
     cp_async_commit();
     if (cur < a.n_bricks) {
-      const float* st = stages + (n & 1) * D::FLOATS;
+      const float* st = stages + (n % NS) * D::FLOATS;
       const uint32_t tag = ((const uint32_t*)(st + D::TAG))[tid];
       if (tag & HP_TAG_PHENO_MASK) {
         const int64_t slot = (int64_t)cur * BV + tid;
@@ -1254,7 +1283,7 @@ struct ShapeEntry {
   HaloFn halo;
   int stage_floats_iso, stage_floats_aniso;
   int diff_cap_iso, diff_cap_aniso;  // halo entries the diffusion kernel holds
-  int diff_floats_iso, diff_floats_aniso;
+  int diff_floats_iso, diff_floats_aniso;  // dynamic shared memory of the diffusion kernel
   CnFn cn_iso, cn_aniso;
   CnPassFn start_iso, start_aniso, apply_iso, apply_aniso;
 };
@@ -1265,7 +1294,7 @@ struct ShapeEntry {
    mono_diffuse_kernel<I, J, K, false>, mono_diffuse_kernel<I, J, K, true>, pipe_halo_table<I, J, K>, \
    PipeStage<I, J, K, false>::FLOATS, PipeStage<I, J, K, true>::FLOATS,                      \
    DiffHalo<I, J, K, false>::PER_THREAD * I * J * K, DiffHalo<I, J, K, true>::PER_THREAD * I * J * K, \
-   DiffStage<I, J, K, false>::FLOATS, DiffStage<I, J, K, true>::FLOATS,                      \
+   DiffStage<I, J, K, false>::SMEM_FLOATS, DiffStage<I, J, K, true>::SMEM_FLOATS,            \
    cn_diag_kernel<I, J, K, false>, cn_diag_kernel<I, J, K, true>,                            \
    cn_pass_kernel<I, J, K, false, OP_CN_START>, cn_pass_kernel<I, J, K, true, OP_CN_START>,  \
    cn_pass_kernel<I, J, K, false, OP_CN_APPLY>, cn_pass_kernel<I, J, K, true, OP_CN_APPLY>}
@@ -1430,8 +1459,8 @@ static hp_status setup_split(HpMono* h, const ShapeEntry* se, const HpMonoDesc* 
   HP_CUDA_TRY(cudaStreamSynchronize(s));  // tab is a stack temporary
   h->a.halo_tab = dtab;
   h->a.n_halo = (int32_t)tab.size();
-  const size_t smem = (2 * (size_t)(d->anisotropic ? se->diff_floats_aniso : se->diff_floats_iso) +
-                       54) * sizeof(float);
+  const size_t smem =
+      (size_t)(d->anisotropic ? se->diff_floats_aniso : se->diff_floats_iso) * sizeof(float);
   int dev = 0, n_sm = 0, per_sm = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
   HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));

@@ -83,9 +83,13 @@ struct TorsoArgs {
   // tissue-line cell (each once; vectors are allocated to a multiple of 32)
   int32_t n_chunks;
   const int32_t* chunk;
-  // label | LAB_UNIFORM when all six neighbours carry the cell's own label,
+  // label | LAB_UNIFORM when all six neighbours carry the cell's own label
+  // (and, with a smoothed boundary, psi is 1 at the cell and all six),
   // | LAB_PIN at the pinned voxel
   const uint8_t* label_u;
+  // smoothed-boundary domain function per padded cell (0 off the rows), or
+  // null for the sharp boundary
+  const float* psi;
 };
 
 constexpr int LAB_UNIFORM = 0x80;
@@ -95,6 +99,17 @@ static_assert(HP_MAX_MATERIALS <= LAB_MASK + 1, "material labels must fit under 
 
 __constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
 __constant__ double c_T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
+
+// Smoothed-boundary factor of a face: the harmonic mean of the two cells'
+// domain function, 0 when both are 0 (build_torso_grid.py:350-375).
+__device__ __forceinline__ float psi_face(float pa, float pb) {
+  const float s = pa + pb;
+  return s < 1e-30f ? 0.0f : __fdiv_rn(2.0f * pa * pb, s);
+}
+__host__ __device__ inline double psi_face64(double pa, double pb) {
+  const double s = pa + pb;
+  return s < 1e-30 ? 0.0 : (2.0 * pa * pb) / s;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -277,11 +292,12 @@ __global__ void __launch_bounds__(TB, HP_PU_MINB) pcg_p_update(TorsoArgs a) {
 // labels are read only where a cell's six neighbours do not all share its
 // label.  Per-cell arithmetic is the same sum of face fluxes in the same
 // face order as before.
-template <class Cell>
+template <bool PSI, class Cell>
 __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, Cell&& cell) {
   const uint8_t* __restrict__ lab = a.label_u;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
+  const float* __restrict__ psi = a.psi;
   const int sj = a.pk, si = a.pj * a.pk;   // even; the padded plane fits in 32 bits
   const int lane = threadIdx.x & 31;
   const int n_warps = gridDim.x * (TB / 32);
@@ -330,6 +346,12 @@ __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, C
           const int off[6] = {si, -si, sj, -sj, 1, -1};
 #pragma unroll
           for (int f = 0; f < 6; ++f) tf[f] = T[l * HP_MAX_MATERIALS + (le[off[f]] & M)];
+          if constexpr (PSI) {
+            const float* __restrict__ pe = psi + c + e;
+            const float pself = pe[0];
+#pragma unroll
+            for (int f = 0; f < 6; ++f) tf[f] *= psi_face(pself, pe[off[f]]);
+          }
         }
         float ap = 0.0f;
 #pragma unroll
@@ -346,11 +368,12 @@ __device__ __forceinline__ void spmv_lines(const TorsoArgs& a, const float* T, C
 
 // The same with one cell per lane, for a padded row of odd length (the
 // pair accesses need even strides).
-template <class Cell>
+template <bool PSI, class Cell>
 __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const float* T, Cell&& cell) {
   const uint8_t* __restrict__ lab = a.label_u;
   const float* __restrict__ p = a.p0;
   float* __restrict__ Ap = a.Ap;
+  const float* __restrict__ psi = a.psi;
   const int sj = a.pk, si = a.pj * a.pk;   // the padded plane fits in 32 bits
   const int lane = threadIdx.x & 31;
   const int n_warps = gridDim.x * (TB / 32);
@@ -378,6 +401,11 @@ __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const floa
       } else {
 #pragma unroll
         for (int f = 0; f < 6; ++f) tf[f] = T[l * HP_MAX_MATERIALS + (lc[off[f]] & LAB_MASK)];
+        if constexpr (PSI) {
+          const float pself = psi[g];
+#pragma unroll
+          for (int f = 0; f < 6; ++f) tf[f] *= psi_face(pself, psi[g + off[f]]);
+        }
       }
       float ap = 0.0f;
 #pragma unroll
@@ -389,7 +417,7 @@ __device__ __forceinline__ void spmv_lines_single(const TorsoArgs& a, const floa
   }
 }
 
-template <bool PAIRS>
+template <bool PAIRS, bool PSI>
 __global__ void __launch_bounds__(TB, HP_AP_MINB) pcg_ap(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
@@ -397,8 +425,8 @@ __global__ void __launch_bounds__(TB, HP_AP_MINB) pcg_ap(TorsoArgs a) {
   __syncthreads();
   double acc[1] = {0.0};
   auto cell = [&](int64_t, float pg, float ap) { acc[0] += (double)pg * (double)ap; };
-  if constexpr (PAIRS) spmv_lines(a, T, cell);
-  else spmv_lines_single(a, T, cell);
+  if constexpr (PAIRS) spmv_lines<PSI>(a, T, cell);
+  else spmv_lines_single<PSI>(a, T, cell);
   double tot[1];
   if (block_reduce_last<1>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     const double pAp = tot[0];
@@ -527,7 +555,8 @@ __global__ void __launch_bounds__(TB) true_residual(TorsoArgs a, int reset) {
     double ax = 0.0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      const double t = c_T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
+      double t = c_T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
+      if (a.psi) t *= psi_face64(a.psi[g], a.psi[nb[f]]);
       ax += t * (xg - a.x[nb[f]]);   // x is 0 on air and at the pinned voxel
     }
     const double bb = (double)a.b[g];
@@ -595,14 +624,17 @@ __global__ void __launch_bounds__(TB) src_laplacian(SrcArgs s) {
 __global__ void __launch_bounds__(TB) src_scatter(const float* iv, const int32_t* seg_ptr,
                                                   const int32_t* seg_vox, const int64_t* seg_grid,
                                                   int32_t n_seg, const double* scal,
-                                                  double inv_nexp, float* b, int64_t pin) {
+                                                  double inv_nexp, float* b, int64_t pin,
+                                                  const float* psi) {
   const int q = blockIdx.x * TB + threadIdx.x;
   if (q >= n_seg) return;
   const float mean = (float)scal[SC_SRC_MEAN];
   float s = 0.0f;
   for (int t = seg_ptr[q]; t < seg_ptr[q + 1]; ++t) s += iv[seg_vox[t]] - mean;
   const int64_t g = seg_grid[q];
-  b[g] = g == pin ? 0.0f : (float)(s * inv_nexp);
+  float bg = (float)(s * inv_nexp);
+  if (psi) bg *= psi[g];   // smoothed boundary: psi b (compute_bspm.py:413-414)
+  b[g] = g == pin ? 0.0f : bg;
 }
 
 __global__ void gather_out(const double* x, const int64_t* grid_of_read, int32_t n, float* out) {
@@ -707,8 +739,10 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   const int ni = d->ni, nj = d->nj, nk = d->nk;
   const int PI = ni + 2, PJ = nj + 2, PK = nk + 2;
   const int64_t ng = (int64_t)PI * PJ * PK;
-  // padded labels, row <-> grid maps (rows in flat active order)
+  // padded labels (and smoothed-boundary psi), row <-> grid maps (rows in
+  // flat active order)
   std::vector<uint8_t> lab(ng, 0);
+  std::vector<float> psi(d->psi ? ng : 0, 0.0f);
   std::vector<int64_t> grid_of_row;
   grid_of_row.reserve((size_t)ni * nj * nk);
   for (int i = 0; i < ni; ++i)
@@ -722,6 +756,15 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
         const int64_t g = ((int64_t)(i + 1) * PJ + (j + 1)) * PK + (k + 1);
         lab[g] = l;
         if (l != 0) grid_of_row.push_back(g);
+        if (d->psi) {
+          const float pv = d->psi[((int64_t)i * nj + j) * nk + k];
+          if (!(pv >= 0.0f && pv <= 1.0f) || (pv > 0.0f) != (l != 0)) {
+            hp::set_error("hp_torso_create: psi %g at (%d,%d,%d) must be in (0, 1] exactly where "
+                          "the label is non-zero (label %d)", (double)pv, i, j, k, l);
+            return HP_ERR_INVALID;
+          }
+          psi[g] = pv;
+        }
       }
   const int64_t n_rows = (int64_t)grid_of_row.size();
   HP_REQUIRE(d->pin_row >= 0 && d->pin_row < n_rows, "hp_torso_create: pin_row out of range");
@@ -750,7 +793,9 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     const int l = lab[g];
     const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
     double dg = 0.0;
-    for (int f = 0; f < 6; ++f) dg += T64[l * HP_MAX_MATERIALS + lab[nb[f]]];
+    for (int f = 0; f < 6; ++f)
+      dg += T64[l * HP_MAX_MATERIALS + lab[nb[f]]] *
+            (d->psi ? psi_face64(psi[g], psi[nb[f]]) : 1.0);
     invd[g] = dg > 1e-30 ? (float)(1.0 / dg) : 1.0f;
   }
   HpTorso* h = new HpTorso();
@@ -776,6 +821,8 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   invd.resize(ng32, 0.0f);
   TT_TRY(tup(h, (uint8_t**)&a.label, lab.data(), ng, s));
   TT_TRY(tup(h, (float**)&a.invd, invd.data(), ng32, s));
+  a.psi = nullptr;
+  if (d->psi) TT_TRY(tup(h, (float**)&a.psi, psi.data(), ng, s));
   TT_TRY(tal(h, &a.r, ng32));
   TT_TRY(tal(h, &a.p0, ng32));
   TT_TRY(tal(h, &a.p1, ng32));
@@ -801,7 +848,10 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     int o = 0;
     // cell pairs need even padded strides (an even padded row)
     h->pairs = (PK % 2) == 0;
-    h->ap_fn = h->pairs ? pcg_ap<true> : pcg_ap<false>;
+    // the smoothed-boundary face weights are a separate instantiation, so
+    // the sharp operator carries no psi code
+    h->ap_fn = a.psi ? (h->pairs ? pcg_ap<true, true> : pcg_ap<false, true>)
+                     : (h->pairs ? pcg_ap<true, false> : pcg_ap<false, false>);
     h->fspmv_fn = h->pairs ? fcg_spmv<true> : fcg_spmv<false>;
     const void* fs[N_LINE_KERNELS] = {(const void*)pcg_p_update, (const void*)h->ap_fn,
                                       (const void*)pcg_k2<false>, (const void*)h->fspmv_fn,
@@ -851,8 +901,9 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
     for (int64_t r = 0; r < n_rows; ++r) {
       const int64_t g = grid_of_row[r];
       const int64_t nb[6] = {g + SI, g - SI, g + SJ, g - SJ, g + 1, g - 1};
-      bool uni = true;
-      for (int f = 0; f < 6; ++f) uni = uni && lab[nb[f]] == lab[g];
+      bool uni = !d->psi || psi[g] == 1.0f;
+      for (int f = 0; f < 6; ++f)
+        uni = uni && lab[nb[f]] == lab[g] && (!d->psi || psi[nb[f]] == 1.0f);
       if (uni) lab_u[g] |= (uint8_t)LAB_UNIFORM;
     }
     lab_u[pin_g] |= (uint8_t)LAB_PIN;
@@ -1001,7 +1052,7 @@ static hp_status build_rhs(HpTorso* h, const float* vm, int vm_on_device, cudaSt
     if (h->n_seg > 0)
       src_scatter<<<(h->n_seg + TB - 1) / TB, TB, 0, s>>>(sa.iv, h->seg_ptr, h->seg_vox,
                                                            h->seg_grid, h->n_seg, a.scal,
-                                                           h->inv_nexp, a.b, a.pin);
+                                                           h->inv_nexp, a.b, a.pin, a.psi);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -1163,8 +1214,8 @@ __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
     acc[0] += (double)pv * q;
     acc[1] += (double)pv * rv[g];
   };
-  if constexpr (PAIRS) spmv_lines(a, T, cell);
-  else spmv_lines_single(a, T, cell);
+  if constexpr (PAIRS) spmv_lines<false>(a, T, cell);
+  else spmv_lines_single<false>(a, T, cell);
   double tot[2];
   if (block_reduce_last<2>(acc, 0u, a.part, a.ticket, tot) && threadIdx.x == 0) {
     a.scal[SC_PAP] = tot[0];
@@ -1419,7 +1470,11 @@ extern "C" hp_status hp_torso_solve_frame_fcg(HpTorso* h, HpPrecond* p, const fl
                                               int32_t out_on_device, double tol, int32_t max_iter,
                                               int32_t fallback_iter, int32_t use_net,
                                               HpSolveStats* stats, void* stream) {
-  HP_REQUIRE(h && p, "hp_torso_solve_frame_fcg: null handle");
+  HP_REQUIRE(h, "hp_torso_solve_frame_fcg: null torso handle");
+  HP_REQUIRE(!h->a.psi, "hp_torso_solve_frame_fcg: the flexible-CG preconditioners are built for "
+                        "the sharp-boundary operator; a smoothed-boundary (psi) handle solves "
+                        "with hp_torso_solve_frame");
+  HP_REQUIRE(p, "hp_torso_solve_frame_fcg: null preconditioner");
   HP_REQUIRE(max_iter >= 1 && fallback_iter >= 1, "hp_torso_solve_frame_fcg: bad iteration limits");
   HP_REQUIRE(use_net == 0 || use_net == 1 || use_net == 2 || use_net == 4,
              "hp_torso_solve_frame_fcg: use_net must be 0, 1, 2 or 4");
@@ -1461,6 +1516,8 @@ extern "C" hp_status hp_torso_train_precond(HpTorso* h, HpPrecond* p, const floa
                                             const int32_t* ks, int32_t n_ks, int32_t repeats,
                                             float lr, double tol_exact, float* loss_hist,
                                             void* stream) {
+  HP_REQUIRE(h && !h->a.psi, "hp_torso_train_precond: the preconditioners are built for the "
+                            "sharp-boundary operator (this handle has psi)");
   HP_REQUIRE(h && p && vm_frames && ks && n_frames >= 1 && n_ks >= 1 && repeats >= 1,
              "hp_torso_train_precond: bad arguments");
   for (int q = 0; q < n_ks; ++q)

@@ -8,7 +8,9 @@ the previous frame -- all on the GPU (hp_torso_solve_frame).  cg_metric
 'rms' / 'p99' / 'linf' keep the reference's absolute-mV stop on z = M^-1 r
 (p99: the 0.99 quantile of |z| with torch.quantile's linear
 interpolation, decided exactly on the device); the extra metric 'rel' stops
-on the FP64 true relative residual (cg_tol_rel).
+on the FP64 true relative residual (cg_tol_rel).  A grid built with
+use_sbm=True solves the smoothed-boundary system (psi-weighted faces and
+right-hand side, compute_bspm.py:413-414, :542-546).
 """
 from __future__ import annotations
 
@@ -59,7 +61,7 @@ def run_bspm_loop(vm_snapshots_path, grid, registration, sigma_i, h_fine_mm, out
         raise ValueError("full_field_frames contains indices outside the frame range")
     solver = T.TorsoSolver(labels, table, grid["dx_mm"], grid["pin_row"],
                            T.heart_neighbours(vox), proj, sigma_i, h_fine_mm,
-                           np.concatenate(read))
+                           np.concatenate(read), psi=T.psi_from_grid(grid))
     tol = cg_tol_rel if cg_metric == "rel" else cg_tol_mV
     try:
         solver.solve_frame(Vm_all[0], tol, cg_metric, cg_max_iter)   # warm-up, as the reference

@@ -78,11 +78,20 @@ def labels_from_grid(grid):
     return lab, np.concatenate([[0.0], vals])
 
 
+def psi_from_grid(grid):
+    """The smoothed-boundary domain function of a grid built with
+    use_sbm=True (float32, grid shape), else None."""
+    if bool(grid.get("use_sbm", False)) and "psi_vol" in grid:
+        return np.ascontiguousarray(grid["psi_vol"], np.float32)
+    return None
+
+
 class TorsoSolver:
-    """Owns one hp_torso handle."""
+    """Owns one hp_torso handle.  psi: the smoothed-boundary domain function
+    (labels' shape, > 0 exactly on the labelled cells) or None."""
 
     def __init__(self, labels, sigma_table, dx_mm, pin, heart_nbr, proj, sigma_i, h_fine_mm,
-                 read_rows, stream=None):
+                 read_rows, stream=None, psi=None):
         torch = _lib.require_cuda()
         L = _lib.lib()
         labels = np.ascontiguousarray(labels, np.uint8)
@@ -105,6 +114,11 @@ class TorsoSolver:
         d.n_expected = float((float(dx_mm) / float(h_fine_mm)) ** 3)
         d.n_read = len(read)
         d.read_rows = _lib.ptr(read)
+        if psi is not None:
+            psi = np.ascontiguousarray(psi, np.float32)
+            if psi.shape != labels.shape:
+                raise ValueError(f"psi {psi.shape} and labels {labels.shape} differ in shape")
+            d.psi = _lib.ptr(psi)
         if stream is None:
             self._torch_stream = torch.cuda.Stream()
             stream = C.c_void_p(self._torch_stream.cuda_stream)

@@ -243,6 +243,13 @@ typedef struct {
   double n_expected;            /* fine voxels per coarse voxel */
   int32_t n_read;               /* read-out rows (surface nodes, electrodes) */
   const int64_t *read_rows;     /* n_read */
+  /* Smoothed boundary method (build_torso_grid.py:130-186, :276-386;
+   * compute_bspm.py:413-414): NULL for the sharp boundary, else the domain
+   * function psi (ni * nj * nk, > 0 exactly where label != 0).  Every face
+   * conductance is multiplied by the harmonic mean 2 psi_k psi_n /
+   * (psi_k + psi_n) and the right-hand side by psi.  Jacobi-PCG only: the
+   * flexible-CG preconditioners refuse such a handle. */
+  const float *psi;
 } HpTorsoDesc;
 
 typedef struct {

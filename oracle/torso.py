@@ -4,7 +4,9 @@ FP64 CPU restatement of HrdayaPy's torso forward solve, used only by tests/,
 ``__graft_entry__.smoke()`` (as the checker) and bench.py's CPU-baseline leg.
 
 * :func:`assemble_stiffness` -- ecg/functions/build_torso_grid.py:276-397
-  (sharp-boundary path: harmonic-mean face conductance / h^2, air skipped)
+  (harmonic-mean face conductance / h^2, air skipped; with psi_vol the
+  smoothed-boundary path, the face conductance times the harmonic mean of
+  psi)
 * :func:`surface_ids`        -- build_torso_grid.py:469-488
 * :func:`pin_row`            -- build_torso_grid.py:616-623
 * :func:`heart_laplacian`    -- ecg/functions/compute_bspm.py:88-119
@@ -32,13 +34,17 @@ from scipy import ndimage as ndi
 from scipy.sparse.linalg import splu
 
 
-def assemble_stiffness(sigma_vol, h_m, active_mask):
+def assemble_stiffness(sigma_vol, h_m, active_mask, psi_vol=None):
+    """psi_vol: the smoothed-boundary domain function, or None (sharp).
+    With psi every face conductance is (psi_face * sigma_face) / h^2, psi_face
+    the harmonic mean of the two cells' psi (build_torso_grid.py:340-378)."""
     ni, nj, nk = sigma_vol.shape
     flat = np.where(active_mask.ravel())[0]
     N = len(flat)
     id_map = np.full(sigma_vol.size, -1, np.int64)
     id_map[flat] = np.arange(N)
     sig = sigma_vol.ravel().astype(np.float64)
+    psi = None if psi_vol is None else np.asarray(psi_vol, np.float64).ravel()
     i, j, k = np.unravel_index(flat, sigma_vol.shape)
     rows, cols, vals = [], [], []
     diag = np.zeros(N)
@@ -49,8 +55,17 @@ def assemble_stiffness(sigma_vol, h_m, active_mask):
         fn = (a[r] * nj + b[r]) * nk + c[r]
         sk, sn = sig[flat[r]], sig[fn]
         ok = sk + sn >= 1e-30
+        if psi_vol is not None:
+            pk_, pn_ = psi[flat[r]], psi[fn]
+            ok &= ~((pk_ <= 0.0) & (pn_ <= 0.0))
         r, fn, sk, sn = r[ok], fn[ok], sk[ok], sn[ok]
-        g = (2.0 * sk * sn) / (sk + sn) / (h_m ** 2)
+        if psi_vol is None:
+            g = (2.0 * sk * sn) / (sk + sn) / (h_m ** 2)
+        else:
+            pk_, pn_ = psi[flat[r]], psi[fn]
+            ps = pk_ + pn_
+            pf = np.where(ps < 1e-30, 0.0, (2.0 * pk_ * pn_) / np.where(ps < 1e-30, 1.0, ps))
+            g = pf * ((2.0 * sk * sn) / (sk + sn)) / (h_m ** 2)
         np.add.at(diag, r, g)
         act = active_mask.ravel()[fn]
         rows.append(r[act]); cols.append(id_map[fn[act]]); vals.append(-g[act])
@@ -105,14 +120,17 @@ def projection_map(coords_mm, R, t, scale, origin, dx, active_id_map, shape):
     return proj, proj >= 0
 
 
-def frame_rhs(K, Vm_mV, proj, valid, n_rows, pin, sigma_i, h_fine_m, dx_mm):
-    """FP64 restatement of solve_frame's b (compute_bspm.py:381-419)."""
+def frame_rhs(K, Vm_mV, proj, valid, n_rows, pin, sigma_i, h_fine_m, dx_mm, psi_row=None):
+    """FP64 restatement of solve_frame's b (compute_bspm.py:381-419); with a
+    smoothed boundary b is weighted by psi per row (:413-414)."""
     V = np.asarray(Vm_mV, np.float64) * 1e-3
     Iv = (K @ V)[valid] * (sigma_i / h_fine_m ** 2)
     src = Iv - Iv.mean()
     b = np.zeros(n_rows)
     np.add.at(b, proj[valid], src)
     b /= (dx_mm / (h_fine_m * 1e3)) ** 3
+    if psi_row is not None:
+        b *= np.asarray(psi_row, np.float64)
     b[pin] = 0.0
     return b
 

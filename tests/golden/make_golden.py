@@ -279,6 +279,85 @@ def torso():
         phi_full_ref=phi_full, ref_iters=n_it)
 
 
+def sbm_case():
+    """Fine (0.75 mm) segmentation of a small torso for the smoothed-boundary
+    method: elliptic cylinder with two lungs and a blood pool, boundaries
+    placed off the coarse (1.5 mm) grid.  Labels: 0 air, 1 bulk, 2 lung,
+    3 blood."""
+    ni, nj, nk = 44, 36, 48
+    x, y, z = (np.indices((ni, nj, nk)).astype(np.float64) + 0.5) * 0.75
+    cx, cy = ni * 0.75 / 2, nj * 0.75 / 2
+    lab = np.zeros((ni, nj, nk), np.int32)
+    body = ((x - cx) / 14.6) ** 2 + ((y - cy) / 11.3) ** 2 <= 1.0
+    body &= (z >= 2.2) & (z <= 33.4)
+    lab[body] = 1
+    for sgn in (-1, 1):
+        lung = (((x - cx - sgn * 7.6) / 5.1) ** 2 + ((y - cy) / 6.4) ** 2
+                + ((z - 19.0) / 10.2) ** 2 <= 1)
+        lab[lung & body] = 2
+    blood = ((x - cx) / 3.1) ** 2 + ((y - cy - 1.4) / 2.9) ** 2 + ((z - 15.2) / 3.6) ** 2 <= 1
+    lab[blood & body] = 3
+    return lab, 0.75
+
+
+def sbm():
+    """The upstream smoothed-boundary set-up and stiffness on sbm_case, and a
+    frame solved by the upstream GPU solver loop (on the CPU) with its
+    psi-weighted right-hand side."""
+    btg = ref.build_torso_grid
+    cb = ref.compute_bspm
+    fine, sp_f = sbm_case()
+    spacing = np.full(3, sp_f)
+    dx = 1.5
+    sig_map = {1: 0.2, 2: 0.05, 3: 0.7}
+    coarse = btg._resample_labels(fine, spacing, dx)
+    sigma = np.zeros(coarse.shape)
+    for k, v in sig_map.items():
+        sigma[coarse == k] = v
+    tissue = coarse != 0
+    psi = btg.compute_smoothed_domain(fine, spacing, dx, coarse.shape, interface_width_mm=3.0,
+                                      psi_cutoff=1e-3)
+    active = psi > 0.0
+    sigma_ext = btg.extend_conductivity(sigma, tissue, active)
+    active_flat = np.where(active.ravel())[0].astype(np.int32)
+    id_map = np.full(coarse.size, -1, np.int32)
+    id_map[active_flat] = np.arange(len(active_flat), dtype=np.int32)
+    A = btg._assemble_stiffness(sigma_ext, dx * 1e-3, active, active_flat, id_map, psi_vol=psi)
+    interior = np.where(tissue.ravel())[0]
+    pin_row = int(id_map[int(interior[len(interior) // 2])])
+    surf_flat, surf_rows = btg._find_surface_ids(coarse, tissue, id_map)
+    # heart shell and wavefront as in torso(), registered into this torso
+    h_f = 0.5
+    gi, gj, gk = np.indices((36, 30, 36))
+    cen = np.array([17.5, 14.5, 17.5])
+    r = np.sqrt((gi - cen[0]) ** 2 + (gj - cen[1]) ** 2 + (gk - cen[2]) ** 2)
+    vox = np.argwhere((r >= 9) & (r <= 14)).astype(np.int32)
+    coords = (vox[:, [1, 0, 2]].astype(np.float64)) * h_f
+    R = np.eye(3)
+    t = np.array([8.0, 6.0, 9.0])
+    K = cb.build_heart_laplacian(vox, len(vox), h_f)
+    proj, valid = quiet(cb.build_projection_map, coords, R, t, 1.0, np.zeros(3), dx,
+                        id_map, coarse.shape)
+    rng = np.random.default_rng(5)
+    xv = vox[:, 0].astype(np.float64)
+    Vm = (-85.0 + 110.0 / (1.0 + np.exp(-(xv - 17.0) / 1.5)) + rng.normal(0, 0.5, len(vox)))
+    Vm = Vm.astype(np.float32)
+    psi_row = psi.ravel()[active_flat]
+    solve, iters = quiet(cb.make_gpu_solver, A, pin_row, proj, valid, cb._scipy_csr_to_torch(
+        K, torch.device("cpu"), torch.float32), 0.2625, h_f * 1e-3, dx, surf_rows,
+        len(active_flat), torch.device("cpu"), cg_tol_mV=1e-7, cg_max=20000, cg_metric="linf",
+        psi_row=psi_row)
+    phi_s, n_it, res_mV, phi_full = quiet(solve, Vm, capture_full=True)
+    A = A.tocsr()
+    np.savez_compressed(
+        HERE / "sbm.npz", fine=fine.astype(np.uint8), spacing=spacing, dx=dx, coarse=coarse,
+        sigma_keys=np.array(list(sig_map)), sigma_vals=np.array(list(sig_map.values())),
+        psi=psi, sigma_ext=sigma_ext, active_ids=active_flat, A_indptr=A.indptr,
+        A_indices=A.indices, A_data=A.data, pin_row=pin_row, surf_flat=surf_flat,
+        surf_rows=surf_rows, heart_vox=vox, h_fine=h_f, reg_t=t, proj=proj, valid=valid, Vm=Vm,
+        phi_surf_ref=phi_s, phi_full_ref=phi_full, ref_iters=n_it)
+
+
 def bspm_case():
     """Slab, stimulus and registration of bspm_loop (restated in the tests)."""
     nx, ny, nz = 24, 24, 8
@@ -471,9 +550,9 @@ def pmj_exp4():
 if __name__ == "__main__":
     torch.set_num_threads(8)
     which = sys.argv[1:] or ["cells", "pacing", "iso", "aniso", "maps", "pmj", "torso", "bspm",
-                             "transmural"]
+                             "transmural", "sbm"]
     for w in which:
         print("generating", w, flush=True)
         {"cells": ttp06_cells, "pacing": ttp06_pacing, "iso": mono_iso,
          "aniso": mono_aniso, "maps": act_maps, "pmj": pmj_exp4, "torso": torso,
-         "bspm": bspm_loop, "transmural": transmural}[w]()
+         "bspm": bspm_loop, "transmural": transmural, "sbm": sbm}[w]()
