@@ -559,8 +559,12 @@ def run_ours(args):
                         f"algorithmic {bpv * n_vox / 1e6:.0f} MB")
     # end to end through the C-ABI handle: host buffers in, Vm frames out;
     # three repetitions, the median reported (the first one also pays
-    # first-use costs of the process: pinned buffers, module loads)
-    reps = sorted((e2e_run(prob, args, fs) for _ in range(3)), key=lambda r: r["value"])
+    # first-use costs of the process: module loads)
+    import torch
+    k_e2e = max(1, int(round(args.e2e_ms)))
+    out_e2e = torch.empty((k_e2e, prob.n_myo), dtype=torch.float32, pin_memory=True)
+    reps = sorted((e2e_run(prob, args, fs, out_e2e) for _ in range(3)), key=lambda r: r["value"])
+    del out_e2e
     e2e = dict(reps[1], repetitions=[r["value"] for r in reps])
     if rank == 0:
         line = {
@@ -744,37 +748,41 @@ def torso_leg(prob, n_train=8, n_test=5, net_every=1, net_iters=25, parity=True,
             **extra}
 
 
-def e2e_run(prob, args, fs):
-    """hp_mono_create from host arrays + K frames + D2H of each frame."""
+def e2e_run(prob, args, fs, out):
+    """One whole run as a user makes it: hp_mono_create from host arrays
+    (the problem upload), then K frames of fs steps, each frame's Vm read
+    back into pinned host memory (out, K x n_myo).  K = the run's length in
+    ms (--e2e-ms, by default the configuration's 400 ms), so the upload is
+    paid once per run as in the configuration."""
     import torch
     from hrdayapy_b200 import monodomain as M
     import dataclasses
-    # 40 frames (40 ms of simulated time) at the default 20 bench steps: the
-    # handle's creation (problem upload) is paid once per run, as in a user's
-    # run of hundreds of frames
-    k = max(1, min(2 * args.steps, 40))
+    k = out.shape[0]
     p2 = dataclasses.replace(prob, n_steps=k * fs, site_on=np.resize(prob.site_on, k * fs + 1),
                              vm_every=fs)
     h2d = (p2.tag.nbytes + (p2.wface.nbytes + p2.doff.nbytes if p2.anisotropic else 0) +
            p2.layout.brick_nbr.nbytes + p2.pk_ptr.nbytes + p2.pk_idx.nbytes +
            p2.pk_coef.nbytes + p2.pmj_row.nbytes + p2.surf_of_slot.nbytes +
            p2.site_on.nbytes + p2.layout.slot_of_node.nbytes)
-    out = torch.empty((k, p2.n_myo), dtype=torch.float32, pin_memory=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim = M.MonoHandle(p2)
     t1 = time.perf_counter()
+    # each frame's D2H (pinned) runs on the handle's copy stream while the
+    # next frame's steps run
     for f in range(k):
         sim.run(fs, graph_chunk=fs)
-        sim.vm_frames(f, 1, out=out[f].numpy())
+        sim.vm_frames_async(f, 1, out[f])
+    sim.wait_copies()
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     dt_s = t2 - t0
     sim.close()
     return {"value": p2.n_myo * fs * k / dt_s, "unit": "voxel-steps/s",
             "h2d_bytes_per_step": int(h2d // k), "d2h_bytes_per_step": int(p2.n_myo * 4),
-            "steps": k, "includes": "hp_mono_create upload + run + per-frame Vm D2H "
-                                    "(frames of 1 ms, one per bench step)",
+            "steps": k, "includes": f"one {k}-ms run: hp_mono_create upload + {k * fs} steps "
+                                    f"+ {k} Vm frames D2H (one per ms, each copy overlapping "
+                                    "the next frame's steps)",
             "create_s": t1 - t0, "run_and_d2h_s": t2 - t1}
 
 
@@ -973,6 +981,9 @@ def main():
                     help="skip the torso ms/frame leg (plain PCG vs learned FCG)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default brick shape and kernel instead of timing candidates")
+    ap.add_argument("--e2e-ms", type=float, default=400.0,
+                    help="simulated length of the end-to-end run (one Vm frame per ms); the "
+                         "configuration's 400 ms by default")
     ap.add_argument("--kernel", type=int, default=0,
                     help="monodomain step kernel: 0 auto, 1 per-brick, 2 pipelined, 3 split")
     args = ap.parse_args()

@@ -261,6 +261,42 @@ class MonoHandle:
         self.sync()
         return out
 
+    def vm_frames_async(self, f0, nf, out):
+        """Starts the device-to-host copy of snapshots [f0, f0 + nf) into out
+        ((nf, n_myo) float32 in pinned host memory: a torch tensor made with
+        pin_memory=True, or a numpy view of one) and returns at once.  The
+        copy runs on a copy stream of this handle, ordered after every step
+        enqueued so far, so the steps enqueued next overlap it; each frame
+        has its own device slot, which later steps never overwrite.  out
+        holds the frames once wait_copies() returns.  A handle made on a
+        caller's stream queues the copy on that stream instead (no overlap)."""
+        import torch
+        nf = int(nf)
+        ptr = C.c_void_p(out.data_ptr()) if hasattr(out, "data_ptr") else _lib.ptr(out)
+        if tuple(out.shape) != (nf, self.prob.n_myo) and not (nf == 1 and tuple(out.shape) ==
+                                                              (self.prob.n_myo,)):
+            raise ValueError(f"out has shape {tuple(out.shape)}, expected ({nf}, "
+                             f"{self.prob.n_myo})")
+        stream = self.stream
+        own = getattr(self, "_torch_stream", None)
+        if own is not None:
+            if getattr(self, "_copy_stream", None) is None:
+                self._copy_stream = torch.cuda.Stream()
+            ev = torch.cuda.Event()
+            ev.record(own)
+            self._copy_stream.wait_event(ev)
+            stream = C.c_void_p(self._copy_stream.cuda_stream)
+        _lib.check(_lib.lib().hp_mono_copy_vm(self.h, int(f0), nf, ptr, 0, stream),
+                   "hp_mono_copy_vm")
+
+    def wait_copies(self):
+        """Blocks until every copy started by vm_frames_async has landed."""
+        cs = getattr(self, "_copy_stream", None)
+        if cs is not None:
+            cs.synchronize()
+        elif getattr(self, "_torch_stream", None) is None:
+            self.sync()
+
     def vm_frames_device(self, dst_ptr: int, f0: int, nf: int):
         _lib.check(_lib.lib().hp_mono_copy_vm(self.h, f0, nf, C.c_void_p(dst_ptr), 1, self.stream),
                    "hp_mono_copy_vm")
@@ -306,6 +342,7 @@ class MonoHandle:
 
     def close(self):
         if getattr(self, "h", None):
+            self.wait_copies()   # no copy may read the snapshots once they are freed
             _lib.lib().hp_mono_destroy(self.h)
             self.h = None
 
@@ -567,10 +604,30 @@ def run(nodes, elements, activation_times, S, Z, phi, *, fibre_dir=None, anisotr
                          save_every=save_every, **cn, **kw)
     sim = MonoHandle(prob)
     try:
-        sim.run(n_steps, graph_chunk)
+        vm = None
+        if run_vm and sim.n_vm_frames > 0:
+            # the snapshots stream into pinned host memory chunk by chunk,
+            # each chunk's copy overlapping the next chunk's steps
+            import torch
+            ve = prob.vm_every
+            nvf = sim.n_vm_frames
+            buf = torch.empty((nvf, prob.n_myo), dtype=torch.float32, pin_memory=True)
+            per = max(1, min(nvf, 64))
+            f0 = 0
+            while f0 < nvf:
+                nf_ = min(per, nvf - f0)
+                end = n_steps if f0 + nf_ == nvf else (f0 + nf_) * ve
+                sim.run(end - sim.steps_done, graph_chunk)
+                sim.vm_frames_async(f0, nf_, buf[f0:f0 + nf_])
+                f0 += nf_
+            if sim.steps_done < n_steps:
+                sim.run(n_steps - sim.steps_done, graph_chunk)
+            sim.wait_copies()
+            vm = buf.numpy()
+        else:
+            sim.run(n_steps, graph_chunk)
         surf, pk = sim.anim_frames()
         act, nact, dea, ndea = sim.events()
-        vm = sim.vm_frames() if run_vm else None
     finally:
         sim.close()
     Np = info["Np"]

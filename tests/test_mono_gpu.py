@@ -204,3 +204,27 @@ def test_activation_map_file_from_gpu_events(golden, tmp_path):
     np.testing.assert_array_equal(m.vox_idx, g["vox_idx"])
     assert np.max(np.abs(m.activation_map(1) - g["act"][:, 0])) <= ACT_TOL
     assert (m.n_activations == 1).all()
+
+
+def test_async_frame_copies_match_synchronous():
+    """vm_frames_async (copy stream, overlapping the following steps) lands
+    the same frames as the synchronous read-out, frame by frame while the
+    run continues."""
+    import torch
+    from hrdayapy_b200 import monodomain as M
+    args, fibre, kw = cases.aniso_case()
+    nodes, el, act, S, phi = args
+    prob, _ = M.prepare(nodes, el, act, S, S, phi, fibre_dir=fibre, anisotropic=True,
+                        vm_save_dt=0.5, **dict(kw, A_P=2.0 / kw["R_P"], T=6.0))
+    sim = M.MonoHandle(prob)
+    try:
+        per = prob.vm_every
+        nf = sim.n_vm_frames
+        out = torch.empty((nf, prob.n_myo), dtype=torch.float32, pin_memory=True)
+        for f in range(nf):
+            sim.run(min(per, prob.n_steps - sim.steps_done), graph_chunk=per)
+            sim.vm_frames_async(f, 1, out[f])
+        sim.wait_copies()
+        np.testing.assert_array_equal(out.numpy(), sim.vm_frames())
+    finally:
+        sim.close()
