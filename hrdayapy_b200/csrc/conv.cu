@@ -83,13 +83,14 @@ conv3_tc_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat16* __
       }
       tc_fence_after();
       const uint32_t a0 = smem_u32(smem + buf * C::STAGE);
-      const uint32_t b0 = a0 + C::A_BYTES;
+      const uint64_t a_d = smem_desc(a0, CHUNK, 128);
+      const uint64_t b_d = smem_desc(a0 + C::A_BYTES, COUT * 16, 128);
 #pragma unroll
       for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
         for (int k = 0; k < CIN / 16; ++k) {
-          const uint64_t ad = smem_desc(a0 + 2 * k * CHUNK + dx * 16, CHUNK, 128);
-          const uint64_t bd = smem_desc(b0 + (dx * C::G + 2 * k) * COUT * 16, COUT * 16, 128);
+          const uint64_t ad = desc_add(a_d, 2 * k * CHUNK + dx * 16);
+          const uint64_t bd = desc_add(b_d, (dx * C::G + 2 * k) * COUT * 16);
           mma_bf16(tmem, ad, bd, C::IDESC, (s | dx | k) != 0);
         }
       }
@@ -269,8 +270,8 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
       }
       tc_fence_after();
       const int zi = s / (R + 2), ri = s % (R + 2);
-      const uint32_t a0 = smem_u32(smem + buf * C::A_BYTES);
-      const uint32_t b0 = smem_u32(Bbase + (zi & 1) * C::B_BYTES);
+      const uint64_t a_d = smem_desc(smem_u32(smem + buf * C::A_BYTES), CHUNK, 128);
+      const uint64_t b_d = smem_desc(smem_u32(Bbase + (zi & 1) * C::B_BYTES), COUT * 16, 128);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int dy = ri - 1 - r;   // input line h0-1+ri feeds output line h0+r
@@ -280,9 +281,9 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
         for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
           for (int k = 0; k < CIN / 16; ++k) {
-            const uint64_t ad = smem_desc(a0 + 2 * k * CHUNK + dx * 16, CHUNK, 128);
+            const uint64_t ad = desc_add(a_d, 2 * k * CHUNK + dx * 16);
             const uint64_t bd =
-                smem_desc(b0 + ((3 * (dy + 1) + dx) * C::G + 2 * k) * COUT * 16, COUT * 16, 128);
+                desc_add(b_d, ((3 * (dy + 1) + dx) * C::G + 2 * k) * COUT * 16);
             // the first product into line r (zi 0, dy -1, dx 0, k 0) overwrites
             const uint32_t acc = (zi != 0 || dy != -1 || dx != 0 || k != 0) ? 1u : 0u;
             mma_bf16(td, ad, bd, C::IDESC, acc);
@@ -351,6 +352,244 @@ conv3_tc_rows_kernel(const __grid_constant__ CUtensorMap tmX, const __nv_bfloat1
 }
 
 // -------------------------------------------------------------------------
+// Persistent warp-specialised variant.  One CTA per SM walks the tiles
+// (128 voxels along W x R output lines x one depth) t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... with three roles:
+//   warp 0, lane 0: producer -- the line stages of every tile in one
+//     continuous sequence (dz-major, R + 2 input lines per depth slice,
+//     TMA line loads plus the slice's 9-tap weight block on the slice's
+//     first line) into an NS-stage ring, refilling a stage once the
+//     products that read it completed;
+//   warp 1, lane 0: MMA issuer -- the products of tile j into one of two
+//     TMEM accumulator sets (R lines x ACC columns each, set j & 1), then a
+//     commit that hands the set to the epilogue;
+//   warps 2-5: epilogue -- each thread owns TMEM lane (warp & 3) * 32 +
+//     lane, i.e. one voxel of the tile: it reads the R lines' accumulators,
+//     applies the epilogue, stores, and releases the set, while the products
+//     of the next tile run in the other set.
+// The weight block of a depth slice is double-buffered by global slice
+// index; a buffer is rewritten at the first stage of the slice two later,
+// whose ring wait (NS <= R + 2 stages back) already covers every product of
+// the slice that read it.  Every wait is bounded; on a timeout the role
+// records the location in *err and sets a shared flag that makes the other
+// roles stop, the CTA waits (bounded) for its copies and products in
+// flight, frees its TMEM and returns.
+template <int CIN, int COUT, int RR>
+struct PersistCfg {
+  static constexpr int G = CIN / 8;
+  static constexpr int A_BYTES = G * CHUNK;
+  static constexpr int A_TX = G * LINE * 16;
+  static constexpr int B_BYTES = 9 * CIN * COUT * 2;
+  static constexpr int ACC = (COUT + 31) / 32 * 32;          // TMEM columns per output line
+  static constexpr int R = RR;                                // output lines per tile
+  static constexpr int NSTG = 3 * (R + 2);                   // line stages per tile
+  static constexpr uint32_t COLS = 2 * R * ACC <= 128 ? 128 : (2 * R * ACC <= 256 ? 256 : 512);
+  static constexpr int NS_FIT = (200 * 1024 - 2 * B_BYTES - 128) / A_BYTES;
+  static constexpr int NS = NS_FIT > R + 2 ? R + 2 : NS_FIT;
+  static constexpr int SMEM = NS * A_BYTES + 2 * B_BYTES + 128;
+  static constexpr uint32_t IDESC = idesc_bf16(TILE_M, COUT);
+  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "channel counts");
+  static_assert(NS >= 2 && NS <= R + 2, "ring depth (the weight-buffer reuse needs NS <= R + 2)");
+  static_assert(2 * R * ACC <= 512, "TMEM columns");
+  static_assert(B_BYTES % 128 == 0 && A_BYTES % 128 == 0, "stage alignment");
+};
+
+constexpr int PERSIST_THREADS = 192;
+
+template <int CIN, int COUT, int RR>
+__global__ void __launch_bounds__(PERSIST_THREADS, 1)
+conv3_tc_persist_kernel(const __grid_constant__ CUtensorMap tmX,
+                        const __nv_bfloat16* __restrict__ Wp, const float* __restrict__ bias,
+                        void* __restrict__ Yv, const __nv_bfloat16* __restrict__ mask, int D,
+                        int H, int W, int epi, int* err) {
+  using C = PersistCfg<CIN, COUT, RR>;
+  constexpr int NS = C::NS, R = C::R, NSTG = C::NSTG, ACC = C::ACC;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  __shared__ __align__(8) uint64_t full[NS];
+  __shared__ __align__(8) uint64_t empty[NS];
+  __shared__ __align__(8) uint64_t acc_full[2];
+  __shared__ __align__(8) uint64_t acc_empty[2];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int failed;
+  __shared__ int issued_s, consumed_s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int n_wt = W / TILE_M, n_hb = (H + R - 1) / R;
+  const int n_tiles = n_wt * n_hb * D;
+
+  if (tid == 0) {
+    for (int b = 0; b < NS; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
+    mbar_init(&done, 1);
+    failed = 0;
+    issued_s = 0;
+    consumed_s = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0) tmem_alloc(&tmem_base, C::COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  uint8_t* const Bbase = smem + NS * C::A_BYTES;
+  auto fail = [&](int code) {
+    atomicOr(err, code);
+    failed = 1;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      int s = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const int w0 = (t % n_wt) * TILE_M, q = t / n_wt;
+        const int h0 = (q % n_hb) * R, d = q / n_hb;
+        for (int st = 0; st < NSTG; ++st, ++s) {
+          const int buf = s % NS;
+          if (s >= NS && !mbar_wait_f(&empty[buf], ((s / NS) - 1) & 1, &failed)) {
+            fail(2);
+            ok = false;
+            break;
+          }
+          const int zi = st / (R + 2), ri = st % (R + 2);
+          uint8_t* A = smem + buf * C::A_BYTES;
+          const bool new_slice = ri == 0;
+          mbar_expect_tx(&full[buf], C::A_TX + (new_slice ? C::B_BYTES : 0));
+#pragma unroll
+          for (int g = 0; g < C::G; ++g)
+            tma_load_4d(A + g * CHUNK, &tmX, g * 8, w0 - 1, h0 - 1 + ri, d + zi - 1, &full[buf]);
+          if (new_slice)
+            bulk_load(Bbase + ((s / (R + 2)) & 1) * C::B_BYTES, Wp + (size_t)9 * zi * CIN * COUT,
+                      C::B_BYTES, &full[buf]);
+        }
+      }
+      issued_s = s;
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      int s = 0, j = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++j) {
+        const int b = j & 1;
+        if (j >= 2 && !mbar_wait_f(&acc_empty[b], ((j >> 1) - 1) & 1, &failed)) {
+          fail(8);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t accb = tmem + (uint32_t)(b * R * ACC);
+        for (int st = 0; st < NSTG; ++st, ++s) {
+          const int buf = s % NS;
+          if (!mbar_wait_f(&full[buf], (s / NS) & 1, &failed)) {
+            fail(1);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int zi = st / (R + 2), ri = st % (R + 2);
+          const uint64_t a_d = smem_desc(smem_u32(smem + buf * C::A_BYTES), CHUNK, 128);
+          const uint64_t b_d =
+              smem_desc(smem_u32(Bbase + ((s / (R + 2)) & 1) * C::B_BYTES), COUT * 16, 128);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int dy = ri - 1 - r;  // input line h0-1+ri feeds output line h0+r
+            if (dy < -1 || dy > 1) continue;
+            const uint32_t td = accb + (uint32_t)(r * ACC);
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+              for (int k = 0; k < CIN / 16; ++k) {
+                const uint64_t ad = desc_add(a_d, 2 * k * CHUNK + dx * 16);
+                const uint64_t bd =
+                    desc_add(b_d, ((3 * (dy + 1) + dx) * C::G + 2 * k) * COUT * 16);
+                // the first product into line r (zi 0, dy -1, dx 0, k 0) overwrites
+                const uint32_t acc = (zi != 0 || dy != -1 || dx != 0 || k != 0) ? 1u : 0u;
+                mma_bf16(td, ad, bd, C::IDESC, acc);
+              }
+            }
+          }
+          mma_commit(&empty[buf]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[b]);
+      }
+      consumed_s = s;
+      // every product issued has completed before the CTA releases TMEM
+      mma_commit(&done);
+      if (!mbar_wait(&done, 0)) atomicOr(err, 4);
+    }
+  } else {  // epilogue: warps 2-5, TMEM lane quarter warp & 3
+    const int row = (warp & 3) * 32 + lane;
+    const uint32_t tlane = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    int j = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++j) {
+      const int b = j & 1;
+      if (!mbar_wait_sleep(&acc_full[b], (j >> 1) & 1, &failed)) {
+        if (lane == 0) fail(16);
+        break;
+      }
+      tc_fence_after();
+      const int w0 = (t % n_wt) * TILE_M, q = t / n_wt;
+      const int h0 = (q % n_hb) * R, d = q / n_hb;
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) {
+        if (h0 + r >= H) break;
+        const uint32_t tl = tlane + (uint32_t)(b * R * ACC + r * ACC);
+        const int64_t vox = ((int64_t)d * H + h0 + r) * W + w0 + row;
+        if (epi == EPI_F32_C0) {
+          float v[16];
+          tmem_ld16(tl, v);
+          ((float*)Yv)[vox] = v[0] + bias[0];
+        } else {
+          __nv_bfloat16* Y = (__nv_bfloat16*)Yv;
+#pragma unroll
+          for (int c0 = 0; c0 < COUT; c0 += 16) {
+            float v[16];
+            tmem_ld16(tl + c0, v);
+            __align__(16) __nv_bfloat16 o[16];
+            if (epi == EPI_MASK) {
+              const uint4* mp = (const uint4*)(mask + vox * COUT + c0);
+              __align__(16) __nv_bfloat16 m[16];
+              *(uint4*)&m[0] = mp[0];
+              *(uint4*)&m[8] = mp[1];
+#pragma unroll
+              for (int qq = 0; qq < 16; ++qq)
+                o[qq] = __float2bfloat16(__bfloat162float(m[qq]) > 0.0f ? v[qq] : 0.0f);
+            } else {
+#pragma unroll
+              for (int qq = 0; qq < 16; ++qq) {
+                float y = v[qq] + bias[c0 + qq];
+                if (epi == EPI_RELU) y = fmaxf(y, 0.0f);
+                o[qq] = __float2bfloat16(y);
+              }
+            }
+            uint4* yp = (uint4*)(Y + vox * COUT + c0);
+            yp[0] = *(uint4*)&o[0];
+            yp[1] = *(uint4*)&o[8];
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[b]);
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && failed) {
+    // let the copies already issued land before the CTA releases its smem
+    for (int s = consumed_s; s < issued_s; ++s) (void)mbar_wait(&full[s % NS], (s / NS) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, C::COLS);
+}
+
+// -------------------------------------------------------------------------
 // host side: tensor maps and dispatch
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
@@ -403,17 +642,34 @@ struct ConvEntry {
   ConvFn fn;
   int rows_smem;
   ConvFn rows_fn;   // CONV_ROWS output lines per CTA
+  int persist_smem;
+  ConvFn persist_fn;   // persistent warp-specialised kernel, or null
+  int persist_rows;
+  uint32_t persist_cols;
 };
 
+// Kernel per layer shape, from per-shape timings on B200 (network level
+// sizes, hp_conv3_forward, CUDA events): the persistent kernel with two
+// output lines per tile wins on the wide layers (96 -> 32 95 against
+// 134 us, 32 -> 96 55 against 73, 64 -> 64 29 against 35, 64 -> 32 25
+// against 31) and loses on the narrow ones (16 -> 16 108-118 against 54,
+// 48 -> 16 195 against 125, 32 -> 32 49 against 35): one CTA per SM
+// pair of copy and MMA threads keeps fewer small products in flight than
+// four row-blocked CTAs.
 #define HP_CONV(ci, co)                                                                     \
   {ci, co, ConvCfg<ci, co>::SMEM, conv3_tc_kernel<ci, co>, RowsCfg<ci, co, CONV_ROWS>::SMEM, \
-   conv3_tc_rows_kernel<ci, co, CONV_ROWS>}
+   conv3_tc_rows_kernel<ci, co, CONV_ROWS>, 0, nullptr, 0, 0}
+#define HP_CONV_P(ci, co)                                                                   \
+  {ci, co, ConvCfg<ci, co>::SMEM, conv3_tc_kernel<ci, co>, RowsCfg<ci, co, CONV_ROWS>::SMEM, \
+   conv3_tc_rows_kernel<ci, co, CONV_ROWS>, PersistCfg<ci, co, 2>::SMEM,                    \
+   conv3_tc_persist_kernel<ci, co, 2>, 2, PersistCfg<ci, co, 2>::COLS}
 static const ConvEntry kConv[] = {
-    HP_CONV(16, 16), HP_CONV(16, 32), HP_CONV(32, 16), HP_CONV(32, 32), HP_CONV(32, 64),
-    HP_CONV(64, 32), HP_CONV(64, 64), HP_CONV(48, 16), HP_CONV(96, 32), HP_CONV(16, 48),
-    HP_CONV(32, 96),
+    HP_CONV(16, 16),   HP_CONV(16, 32),   HP_CONV(32, 16),   HP_CONV(32, 32), HP_CONV(32, 64),
+    HP_CONV_P(64, 32), HP_CONV_P(64, 64), HP_CONV(48, 16),   HP_CONV_P(96, 32), HP_CONV(16, 48),
+    HP_CONV_P(32, 96),
 };
 #undef HP_CONV
+#undef HP_CONV_P
 
 hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y,
                        const void* mask, int D, int H, int W, int cin, int cout, int epi,
@@ -437,13 +693,35 @@ hp_status conv3_launch(const void* X, const void* Wp, const float* bias, void* Y
   hp_status st = make_line_map(&map, X, D, H, W, cin);
   if (st != HP_OK) return st;
   static bool attr_set[sizeof(kConv) / sizeof(kConv[0])] = {false};
+  static int persist_grid[sizeof(kConv) / sizeof(kConv[0])] = {0};
   const int idx = (int)(e - kConv);
   if (!attr_set[idx]) {
     HP_CUDA_TRY(cudaFuncSetAttribute((const void*)e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      e->smem));
     HP_CUDA_TRY(cudaFuncSetAttribute((const void*)e->rows_fn,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, e->rows_smem));
+    if (e->persist_fn) {
+      HP_CUDA_TRY(cudaFuncSetAttribute((const void*)e->persist_fn,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       e->persist_smem));
+      // resident CTAs of the persistent kernel: shared memory and TMEM columns
+      int dev = 0, n_sm = 0, per_sm = 0;
+      HP_CUDA_TRY(cudaGetDevice(&dev));
+      HP_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+      HP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, (const void*)e->persist_fn, PERSIST_THREADS, e->persist_smem));
+      per_sm = std::min(per_sm, (int)(512 / e->persist_cols));
+      persist_grid[idx] = std::max(1, per_sm) * n_sm;
+    }
     attr_set[idx] = true;
+  }
+  if (e->persist_fn) {
+    const int n_tiles = (W / TILE_M) * ((H + e->persist_rows - 1) / e->persist_rows) * D;
+    const int grid = std::min(n_tiles, persist_grid[idx]);
+    e->persist_fn<<<grid, PERSIST_THREADS, e->persist_smem, s>>>(
+        map, (const __nv_bfloat16*)Wp, bias, Y, (const __nv_bfloat16*)mask, D, H, W, epi, err);
+    HP_CUDA_TRY(cudaGetLastError());
+    return HP_OK;
   }
   // Row-blocked CTAs where their two line stages and two weight slices stay
   // small enough for several CTAs per SM; the wide layers (64+ input or

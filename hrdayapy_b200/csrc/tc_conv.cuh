@@ -71,6 +71,53 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait that also gives up once another role of the CTA has set
+// *failed (checked every 256 polls).  Returns false on timeout or failure.
+__device__ __forceinline__ bool mbar_wait_f(uint64_t* bar, uint32_t parity,
+                                            const volatile int* failed) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < SPIN_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255u) == 255u && *failed) return false;
+  }
+  return false;
+}
+
+// The same for waiters that are not on the critical path (epilogue warps
+// waiting for a finished accumulator): a short sleep between polls keeps
+// them from taking issue slots from the copy and MMA threads.  Bounded at
+// about 2^22 polls (about a second).
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity,
+                                                const volatile int* failed) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < (1u << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (*failed) return false;
+    __nanosleep(200);
+  }
+  return false;
+}
+
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -110,6 +157,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
   d |= (uint64_t)1 << 46;  // descriptor version for sm100
   return d;
+}
+
+// The descriptor of the same layout at saddr + off: the start field holds
+// (address >> 4) in 14 bits and shared-memory addresses stay below 2^18, so
+// adding (off >> 4) never carries into the stride fields.  Lets an MMA loop
+// build each operand's descriptor once per stage.
+__device__ __forceinline__ uint64_t desc_add(uint64_t desc, uint32_t off) {
+  return desc + (uint64_t)(off >> 4);
 }
 
 // Instruction descriptor, kind::f16: BF16 x BF16 -> FP32, both K-major.

@@ -50,10 +50,11 @@ def _run(D, H, W, cin, cout, epi, seed=0):
     return y, ref
 
 
-# (16, 16), (16, 32), (48, 16), (32, 32) run row-blocked CTAs, the others one
-# line per CTA; H = 5 leaves a partial block of output lines
+# (16, 16), (16, 32), (48, 16), (32, 32) run row-blocked CTAs, (64, 32),
+# (64, 64), (96, 32), (32, 96) the persistent warp-specialised kernel, the
+# others one line per CTA; H = 5 leaves a partial block of output lines
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32),
-                                      (48, 16)])
+                                      (48, 16), (64, 32), (32, 96)])
 def test_conv_forward(cin, cout):
     y, ref = _run(3, 5, 256, cin, cout, epi=1)
     scale = ref.abs().max().item()
@@ -63,5 +64,14 @@ def test_conv_forward(cin, cout):
 @pytest.mark.parametrize("epi", [0, 2, 3])
 def test_conv_epilogues(epi):
     y, ref = _run(2, 3, 128, 32, 16, epi=epi, seed=1)
+    scale = max(ref.abs().max().item(), 1e-6)
+    assert (y - ref).abs().max().item() <= 1e-2 * scale
+
+
+@pytest.mark.parametrize("epi", [0, 2])
+def test_persistent_kernel_epilogues(epi):
+    """The persistent kernel's epilogue warps (ReLU, ReLU-backward mask) on
+    more tiles than CTAs (the tile loop and both accumulator sets)."""
+    y, ref = _run(4, 9, 384, 64, 64, epi=epi, seed=2)
     scale = max(ref.abs().max().item(), 1e-6)
     assert (y - ref).abs().max().item() <= 1e-2 * scale
