@@ -133,6 +133,8 @@ def _declare_optional(L):
                                            C.POINTER(HpSolveStats), P]
     L.hp_torso_train_precond.argtypes = [P, P, P, C.c_int64, C.c_int32, P, C.c_int32, C.c_int32,
                                          C.c_float, C.c_double, P, P]
+    L.hp_mono_w_gather.argtypes = [P, P, C.c_int64, P, P]
+    L.hp_mono_w_scatter.argtypes = [P, P, C.c_int64, P, P]
     L.hp_conv3_forward.argtypes = [P, P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, P, P]
     L.hp_conv3_wgrad_workspace.argtypes = [C.c_int32] * 5

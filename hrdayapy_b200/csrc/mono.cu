@@ -1985,6 +1985,48 @@ extern "C" hp_status hp_mono_copy_events(HpMono* h, float* act, int32_t* n_act, 
   return HP_OK;
 }
 
+namespace hp {
+__global__ void w_gather_kernel(const float* __restrict__ W, const int32_t* __restrict__ slots,
+                                int64_t n, float* __restrict__ out) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    out[q] = W[slots[q]];
+}
+__global__ void w_scatter_kernel(float* __restrict__ W, const int32_t* __restrict__ slots,
+                                 int64_t n, const float* __restrict__ in) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    W[slots[q]] = in[q];
+}
+}  // namespace hp
+
+// The W buffer the next step's diffusion half reads (step steps_done).
+static float* next_w(HpMono* h) { return (h->steps_done & 1) ? h->a.Vs1 : h->a.Vs0; }
+
+extern "C" hp_status hp_mono_w_gather(HpMono* h, const int32_t* slots, int64_t n, float* out,
+                                      void* stream) {
+  HP_REQUIRE(h && (n == 0 || (slots && out)), "hp_mono_w_gather: null argument");
+  HP_REQUIRE(n >= 0, "hp_mono_w_gather: negative count");
+  HP_REQUIRE(!h->cn, "hp_mono_w_gather: the slab exchange runs the explicit step (theta = 0)");
+  if (n == 0) return HP_OK;
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+  w_gather_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(next_w(h), slots, n, out);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+extern "C" hp_status hp_mono_w_scatter(HpMono* h, const int32_t* slots, int64_t n,
+                                       const float* in, void* stream) {
+  HP_REQUIRE(h && (n == 0 || (slots && in)), "hp_mono_w_scatter: null argument");
+  HP_REQUIRE(n >= 0, "hp_mono_w_scatter: negative count");
+  HP_REQUIRE(!h->cn, "hp_mono_w_scatter: the slab exchange runs the explicit step (theta = 0)");
+  if (n == 0) return HP_OK;
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+  w_scatter_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(next_w(h), slots, n, in);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 extern "C" hp_status hp_mono_copy_v(HpMono* h, float* v_myo, float* v_pk, void* stream) {
   HP_REQUIRE(h, "hp_mono_copy_v: null handle");
   cudaStream_t s = (cudaStream_t)stream;

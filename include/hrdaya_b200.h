@@ -197,6 +197,15 @@ hp_status hp_mono_copy_v(HpMono *h, float *v_myo, float *v_pk, void *stream);
 /* Raw state access for checkpointing: the 18 TTP06 variables of every slot
  * (18 x n_slots) and Purkinje node (18 x n_pk) as last written. */
 hp_status hp_mono_copy_state(HpMono *h, float *state_slots, float *state_pk, void *stream);
+/* Halo exchange of a heart split into slabs over several handles (one per
+ * GPU; hrdayapy_b200.slab): the post-ionic potential W that the next step's
+ * diffusion half reads, at n slots listed in device memory.  gather copies
+ * W[slots[q]] to out[q], scatter writes in[q] to W[slots[q]] (device
+ * buffers, both on `stream`).  No counterpart in the reference, which runs
+ * one heart on one device (pipeline.py:1347-1420). */
+hp_status hp_mono_w_gather(HpMono *h, const int32_t *slots, int64_t n, float *out, void *stream);
+hp_status hp_mono_w_scatter(HpMono *h, const int32_t *slots, int64_t n, const float *in,
+                            void *stream);
 hp_status hp_mono_destroy(HpMono *h);
 
 /* ------------------------------------------------------------------ */
