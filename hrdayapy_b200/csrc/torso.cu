@@ -90,15 +90,18 @@ struct TorsoArgs {
   // smoothed-boundary domain function per padded cell (0 off the rows), or
   // null for the sharp boundary
   const float* psi;
+  // this handle's conductance tables (harmonic-mean face conductance / h^2,
+  // HP_MAX_MATERIALS x HP_MAX_MATERIALS, FP32 for the iteration, FP64 for
+  // the true residual): per handle, so that handles with different
+  // conductivities can live side by side on one device
+  const float* T32;
+  const double* T64;
 };
 
 constexpr int LAB_UNIFORM = 0x80;
 constexpr int LAB_PIN = 0x40;
 constexpr int LAB_MASK = 0x3F;  // the material label (< HP_MAX_MATERIALS)
 static_assert(HP_MAX_MATERIALS <= LAB_MASK + 1, "material labels must fit under the flag bits");
-
-__constant__ float c_T32[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
-__constant__ double c_T64[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
 
 // Smoothed-boundary factor of a face: the harmonic mean of the two cells'
 // domain function, 0 when both are 0 (build_torso_grid.py:350-375).
@@ -421,7 +424,7 @@ template <bool PAIRS, bool PSI>
 __global__ void __launch_bounds__(TB, HP_AP_MINB) pcg_ap(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
-  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = a.T32[q];
   __syncthreads();
   double acc[1] = {0.0};
   auto cell = [&](int64_t, float pg, float ap) { acc[0] += (double)pg * (double)ap; };
@@ -555,7 +558,7 @@ __global__ void __launch_bounds__(TB) true_residual(TorsoArgs a, int reset) {
     double ax = 0.0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      double t = c_T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
+      double t = a.T64[l * HP_MAX_MATERIALS + a.label[nb[f]]];
       if (a.psi) t *= psi_face64(a.psi[g], a.psi[nb[f]]);
       ax += t * (xg - a.x[nb[f]]);   // x is 0 on air and at the pinned voxel
     }
@@ -811,9 +814,9 @@ extern "C" hp_status hp_torso_create(const HpTorsoDesc* d, HpTorso** out, void* 
   h->n_rows = n_rows;
   h->parity = 0;
   h->have_x = false;
-  HP_CUDA_TRY(cudaMemcpyToSymbolAsync(c_T32, T32, sizeof(T32), 0, cudaMemcpyHostToDevice, s));
-  HP_CUDA_TRY(cudaMemcpyToSymbolAsync(c_T64, T64, sizeof(T64), 0, cudaMemcpyHostToDevice, s));
   TorsoArgs& a = h->a;
+  TT_TRY(tup(h, (float**)&a.T32, T32, HP_MAX_MATERIALS * HP_MAX_MATERIALS, s));
+  TT_TRY(tup(h, (double**)&a.T64, T64, HP_MAX_MATERIALS * HP_MAX_MATERIALS, s));
   a.ng = ng; a.pj = PJ; a.pk = PK; a.pin = pin_g; a.n_rows = n_rows;
   // the vectors and invd extend to a multiple of 32 cells (whole chunks),
   // zero past the grid
@@ -1206,7 +1209,7 @@ template <bool PAIRS>
 __global__ void __launch_bounds__(TB) fcg_spmv(TorsoArgs a) {
   __shared__ float T[HP_MAX_MATERIALS * HP_MAX_MATERIALS];
   if (a.iscal[IS_DONE]) return;
-  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = c_T32[q];
+  for (int q = threadIdx.x; q < HP_MAX_MATERIALS * HP_MAX_MATERIALS; q += TB) T[q] = a.T32[q];
   __syncthreads();
   const float* __restrict__ rv = a.r;
   double acc[2] = {0.0, 0.0};

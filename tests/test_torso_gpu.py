@@ -125,3 +125,33 @@ def test_leads_vs_oracle():
     for k in range(12):
         rel = np.linalg.norm(Lg[k] - Lo[k]) / max(np.linalg.norm(Lo[k]), 1e-12)
         assert rel <= LEAD_TOL, (T.LEADS[k], rel)
+
+
+def test_handles_with_different_conductivities_coexist():
+    """Each handle keeps its own conductance tables: a handle solves the
+    same frame bit for bit whether or not a handle with other conductivities
+    was created after it on the same device."""
+    case = torso_cases.random_case()
+    lab, sigma_map, dx, vox, coords, reg, h, frames = case
+    vm = frames if frames.ndim == 1 else frames[0]
+    other = (lab, {k: v * (1.5 + 0.25 * i) for i, (k, v) in enumerate(sigma_map.items())},
+             dx, vox, coords, reg, h, frames)
+    ref, _, _, _ = _setup(case)
+    try:
+        out_ref, st = ref.solve_frame(vm, 1e-6, "rel", 5000)
+        assert st.status == 0
+        x_ref = ref.solution()
+    finally:
+        ref.close()
+    first, _, _, _ = _setup(case)
+    second, _, _, _ = _setup(other)
+    try:
+        out, st = first.solve_frame(vm, 1e-6, "rel", 5000)
+        assert st.status == 0
+        assert np.array_equal(first.solution(), x_ref)
+        assert np.array_equal(out, out_ref)
+        out2, st2 = second.solve_frame(vm, 1e-6, "rel", 5000)
+        assert st2.status == 0 and not np.allclose(out2, out_ref)
+    finally:
+        first.close()
+        second.close()
