@@ -18,6 +18,10 @@
 //     denominators (m, Xr1, Xr2), log(a/b) is log(a) - log(b) with the
 //     constant's logarithm folded, and buffer factors 1/(1 + B K/(c+K)^2)
 //     are (c+K)^2 / ((c+K)^2 + B K);
+//   * exponentials of V with a common slope a share one exp(a V):
+//     exp(a (V + c)) = exp(a c) exp(a V) for the slopes 1/5, +-1/10,
+//     +-1/20, 1/7 and -1/6 (seven exponentials instead of eighteen), and a
+//     logistic 1 / (1 + exp(a c) / E) is E / (E + exp(a c));
 //   * exp2V - 1 in I_CaL is evaluated with expm1f, which is the same
 //     quantity with less cancellation near V = 15 mV (the reference's FP64
 //     has the digits to spare; FP32 does not), and exp2V as that plus one.
@@ -101,6 +105,16 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   constexpr float LN_KS = 2.2617630984737906f, LN_CAO = 0.6931471805599453f;
   // sqrt(Ko / 5.4) == 1 for Ko = 5.4
   constexpr float sqko = 1.0f;
+  // exp(c) for the offsets of the exponentials that share a slope (below)
+  constexpr float X_M12 = (float)6.14421235332821e-06, X_7 = (float)1096.6331584284585;
+  constexpr float X_1 = (float)2.718281828459045, X_56 = (float)270.42640742615254;
+  constexpr float X_4 = (float)54.598150033144236, X_M4 = (float)0.01831563888873418;
+  constexpr float X_M45 = (float)0.011108996538242306, X_3 = (float)20.085536923187668;
+  constexpr float X_13 = (float)3.6692966676192444, X_25 = (float)12.182493960703473;
+  constexpr float X_M32 = (float)0.04076220397836621, X_M3 = (float)0.049787068367863944;
+  constexpr float X_M26_7 = (float)0.0243728440732796, X_20_7 = (float)17.41170806332765;
+  constexpr float X_5 = (float)148.4131591025766, X_5_6 = (float)2.300975890892825;
+  constexpr float X_10_3 = (float)28.03162489452614;
 
   const float Ki = c.v[S_KI], Nai = c.v[S_NAI], Cai = c.v[S_CAI], Cass = c.v[S_CASS];
   const float CaSR = c.v[S_CASR], Xr1 = c.v[S_XR1], Xr2 = c.v[S_XR2], Xs = c.v[S_XS];
@@ -114,15 +128,26 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   const float E_Ks = RTF * (LN_KS - hlog(Ki + P_kna * Nai));
   const float E_Ca = (0.5f * RTF) * (LN_CAO - hlog(Cai));
 
+  // Exponentials of V that share a slope a are formed once:
+  // exp(a (V + c)) = exp(a c) exp(a V), with exp(a c) a constant.  A logistic
+  // 1 / (1 + K / E) is written E / (E + K), inside its one reciprocal.
+  const float P2 = hexp(0.2f * V);              // exp(V / 5)
+  const float Em1 = hexp(-0.1f * V);            // exp(-V / 10)
+  const float Ep1 = hexp(0.1f * V);             // exp(V / 10)
+  const float P05 = hexp(0.05f * V);            // exp(V / 20)
+  const float M05 = hexp(-0.05f * V);           // exp(-V / 20)
+  const float P7 = hexp(V * (1.0f / 7.0f));     // exp(V / 7)
+  const float M6 = hexp(V * (-1.0f / 6.0f));    // exp(-V / 6)
+
   // INa.  tau_m = alpha_m beta_m with alpha_m = 1/(1+e_am) and
-  // beta_m = 0.1/(1+e_b1) + 0.1/(1+e_b2) = 0.1 (2+e_b1+e_b2) / ((1+e_b1)(1+e_b2))
+  // beta_m = 0.1/(1+e_b1) + 0.1/(1+e_b2) = 0.1 (2+e_b1+e_b2) / ((1+e_b1)(1+e_b2));
+  // 1 + e_am = 1 + exp(-12) / P2 = (P2 + exp(-12)) / P2
   float t1 = sig((-56.86f - V) * (1.0f / 9.03f));
   const float m_inf = t1 * t1;
-  const float e_am = hexp((-60.0f - V) * 0.2f);
-  const float e_b1 = hexp((V + 35.0f) * 0.2f);
+  const float e_b1 = X_7 * P2;                  // exp((V + 35) / 5)
   const float e_b2 = hexp((V - 50.0f) * 0.005f);
-  const float dtr_m = dt * (1.0f + e_am) * (1.0f + e_b1) * (1.0f + e_b2) /
-                      (0.1f * (2.0f + e_b1 + e_b2));
+  const float dtr_m = dt * (P2 + X_M12) * (1.0f + e_b1) * (1.0f + e_b2) /
+                      (0.1f * (2.0f + e_b1 + e_b2) * P2);
   t1 = sig((V + 71.55f) * (1.0f / 7.43f));
   const float h_inf = t1 * t1;
   // 1/tau_h = alpha_h + beta_h, 1/tau_j = alpha_j + beta_j (+1e-30)
@@ -138,26 +163,25 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
     rate_j = (Aj * (1.0f + eb) + Bj * (1.0f + ea)) / ((1.0f + ea) * (1.0f + eb));
   } else {
     rate_h = (0.77f / 0.13f) / (1.0f + hexp((V + 10.66f) * (-1.0f / 11.1f)));
-    rate_j = 0.6f * hexp(0.057f * V) / (1.0f + hexp(-0.1f * (V + 32.0f)));
+    rate_j = 0.6f * hexp(0.057f * V) / (1.0f + X_M32 * Em1);
   }
   const float dtr_h = dt * (rate_h + 1e-30f);
   const float dtr_j = dt * (rate_j + 1e-30f);
   const float i_Na = g_Na * m * m * m * h * j * (V - E_Na);
 
   // IKr.  tau_xr1 = 2700 / ((1+e_m45)(1+e_x1)), tau_xr2 = 3.36 / ((1+e_x2)(1+e_x3))
-  const float xr1_inf = sig((-26.0f - V) * (1.0f / 7.0f));
-  const float e_m45 = hexp((-45.0f - V) * 0.1f);
-  const float e_p30 = hexp((V + 30.0f) * 0.1f);  // shared by tau_f, tau_f2
+  const float xr1_inf = P7 / (P7 + X_M26_7);    // 1 / (1 + exp((-26 - V) / 7))
+  const float e_m45 = X_M45 * Em1;               // exp((-45 - V) / 10)
+  const float e_p30 = X_3 * Ep1;                 // exp((V + 30) / 10), shared by tau_f, tau_f2
   const float dtr_xr1 = dt * (1.0f + e_m45) * (1.0f + hexp((V + 30.0f) * (1.0f / 11.5f))) *
                         (1.0f / 2700.0f);
   const float xr2_inf = sig((V + 88.0f) * (1.0f / 24.0f));
-  const float dtr_xr2 = dt * (1.0f + hexp((-60.0f - V) * 0.05f)) *
-                        (1.0f + hexp((V - 60.0f) * 0.05f)) * (1.0f / 3.36f);
+  const float dtr_xr2 = dt * (1.0f + X_M3 * M05) * (1.0f + X_M3 * P05) * (1.0f / 3.36f);
   const float i_Kr = p.g_Kr * sqko * Xr1 * Xr2 * (V - E_K);
 
   // IKs.  tau_xs = 1400 q / (1+e) + 80 = (1400 q + 80 (1+e)) / (1+e)
   const float xs_inf = sig((-5.0f - V) * (1.0f / 14.0f));
-  const float q_xs = rsqrtf(1.0f + hexp((5.0f - V) * (1.0f / 6.0f)));
+  const float q_xs = rsqrtf(1.0f + X_5_6 * M6);  // exp((5 - V) / 6)
   const float e_xs = hexp((V - 35.0f) * (1.0f / 15.0f));
   const float dtr_xs = dt * (1.0f + e_xs) / (1400.0f * q_xs + 80.0f * (1.0f + e_xs));
   const float i_Ks = p.g_Ks * Xs * Xs * (V - E_Ks);
@@ -176,18 +200,18 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   // Ito
   float s_inf, dtr_s;
   if (p.endo_s) {
-    s_inf = sig((V + 28.0f) * 0.2f);
+    s_inf = 1.0f / (1.0f + X_56 * P2);           // sig((V + 28) / 5)
     const float a = V + 67.0f;
     dtr_s = dt / (1000.0f * hexp(-a * a * 0.001f) + 8.0f);
   } else {
     // tau_s = g + 5/(1+e) + 3 = ((g+3)(1+e) + 5) / (1+e)
-    s_inf = sig((V + 20.0f) * 0.2f);
+    s_inf = 1.0f / (1.0f + X_4 * P2);            // sig((V + 20) / 5)
     const float a = V + 45.0f;
     const float g = 85.0f * hexp(-a * a * (1.0f / 320.0f));
-    const float e = hexp((V - 20.0f) * 0.2f);
+    const float e = X_M4 * P2;                     // exp((V - 20) / 5)
     dtr_s = dt * (1.0f + e) / ((g + 3.0f) * (1.0f + e) + 5.0f);
   }
-  const float r_inf = sig((20.0f - V) * (1.0f / 6.0f));
+  const float r_inf = 1.0f / (1.0f + X_10_3 * M6);   // sig((20 - V) / 6)
   const float a40 = V + 40.0f;
   const float dtr_r = dt / (9.5f * hexp(-a40 * a40 * (1.0f / 1800.0f)) + 0.8f);
   const float i_to = p.g_to * r * s * VmEK;
@@ -196,22 +220,22 @@ __device__ __forceinline__ float ttp06_step(float V, CellState& c, float dt,
   //        = (1.4 (1.4 + 0.25 (1+ea)) (1+ec) + (1+ea)(1+eb)) / ((1+ea)(1+eb)(1+ec))
   const float d_inf = sig((-8.0f - V) * (1.0f / 7.5f));
   const float ea_d = 1.0f + hexp((-35.0f - V) * (1.0f / 13.0f));
-  const float eb_d = 1.0f + hexp((V + 5.0f) * 0.2f);
-  const float ec_d = 1.0f + hexp((50.0f - V) * 0.05f);
+  const float eb_d = 1.0f + X_1 * P2;            // 1 + exp((V + 5) / 5)
+  const float ec_d = 1.0f + X_25 * M05;          // 1 + exp((50 - V) / 20)
   const float P_d = ea_d * eb_d;
   const float dtr_d = dt * P_d * ec_d / (1.4f * (1.4f + 0.25f * ea_d) * ec_d + P_d);
   // tau_f = G + 200/(1+eA) + 180/(1+eB) + 20, over the denominator (1+eA)(1+eB)
-  const float f_inf = sig((V + 20.0f) * (1.0f / 7.0f));
+  const float f_inf = 1.0f / (1.0f + X_20_7 * P7);  // sig((V + 20) / 7)
   const float a27 = V + 27.0f;
   const float eB = 1.0f + e_p30;
-  const float eA = 1.0f + hexp((13.0f - V) * 0.1f);
+  const float eA = 1.0f + X_13 * Em1;            // 1 + exp((13 - V) / 10)
   const float D_f = eA * eB;
   const float dtr_f = dt * D_f /
                       ((1102.5f * hexp(-a27 * a27 * (1.0f / 225.0f)) + 20.0f) * D_f +
                        200.0f * eB + 180.0f * eA);
   // tau_f2 = G2 + 31/(1+eC) + 80/(1+eB)
-  const float f2_inf = 0.67f * sig((V + 35.0f) * (1.0f / 7.0f)) + 0.33f;
-  const float eC = 1.0f + hexp((25.0f - V) * 0.1f);
+  const float f2_inf = 0.67f / (1.0f + X_5 * P7) + 0.33f;   // 0.67 sig((V + 35) / 7) + 0.33
+  const float eC = 1.0f + X_25 * Em1;            // 1 + exp((25 - V) / 10)
   const float D_f2 = eC * eB;
   const float dtr_f2 = dt * D_f2 /
                        (562.0f * hexp(-a27 * a27 * (1.0f / 240.0f)) * D_f2 + 31.0f * eB +
