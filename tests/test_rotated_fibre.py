@@ -23,10 +23,10 @@ and 0.6 mm from the z walls:
   5 % (rotated_fiber_values.py:35).
 
 The reference runs the experiment at dx 0.1 mm; the GPU test does too,
-through compute_anisotropic_coupled, and applies the reference's verdict.
+through compute_anisotropic_coupled, and applies the reference's pass rule.
 The oracle runs the same experiment at dx 0.25 mm on the CPU, where the
 axial fronts are checked for planarity (the oblique pointwise error is
-about 11 % at that spacing, so no verdict is taken there), and on the
+about 11 % at that spacing, so the pass rule is not applied there), and on the
 45-degree case the GPU run at that size is compared with it node by node."""
 import numpy as np
 import pytest
@@ -140,7 +140,7 @@ def _gpu_run(dx, name, T):
 def _check_ellipse(runs, dx, pointwise_oblique):
     """Planar velocities and the pointwise eikonal errors.  The axial fronts
     must be planar (their own pointwise error below the tolerance); the
-    verdict on the oblique run is its pointwise error, as the reference's
+    pass rule on the oblique run is its pointwise error, as the reference's
     (run_experiment5_rotated_fiber.py:80-86).  The planar fit of the oblique
     run against sqrt((v_l^2 + v_t^2) / 2) is reported only: the z walls bend
     that front, so the fit's assumption of a normal along x fails
